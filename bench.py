@@ -1,0 +1,329 @@
+"""Benchmark: converged Kohn–Sham SCF on one B200 (or N replicas, one per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload h2_48] [--impl ours|reference]
+
+A step is one full SCF solve of the workload, from the nuclei to |dE| < 1e-6 Ha (the
+BASELINE metric's stop rule; the reference's own three-criterion stop is exercised by the
+parity tests).  Inputs are synthetic (the workload's molecule and grid); nothing is read
+from a dataset.  One JSON line is printed by rank 0.
+
+Timing: W untimed warm-up steps, then K steps bracketed by a barrier and device
+synchronisation, each timed with CUDA events on the library's stream; L2 is flushed
+(a 512 MiB write) between steps; the max over ranks is reported.  `e2e` times the same
+solve through the host-buffer C-ABI call (dft_scf_molecule) by wall clock, including the
+copy of both spin densities back to host memory.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SCF time-to-1e-6 Ha, learned+mixed vs plain FP64 on 1 B200; H·ψ HBM GB/s"
+
+WORKLOADS = {
+    # H2, Z=1 at +-0.7 bohr on x, 48^3 grid, h = 0.3 bohr, centred box, PZ81, multiplicity 1,
+    # 4 bands per spin (1 occupied + 3 buffer bands)
+    "h2_48": dict(n=(48, 48, 48), bounds=(-7.05, 7.05) * 3, Z=[1, 1],
+                  xyz=[[-0.7, 0.0, 0.0], [0.7, 0.0, 0.0]], multiplicity=1, functional="PZ81", extra_bands=3,
+                  desc="H2 PZ81 48^3 h=0.3, 1a+1b (multiplicity 1), 4 bands/spin, Jacobi tol 1e-8, stop |dE|<1e-6"),
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            c = [x.strip() for x in l.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                mx = float(c[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def molecule(w):
+    import dft_b200
+    m = dft_b200.Molecule(0)
+    for z, p in zip(w["Z"], w["xyz"]):
+        m.addNucleus(z, *p)
+    return m
+
+
+def scf_options(w):
+    import dft_b200
+    return dft_b200.default_scf_options(stop_abs_de=1e-6, extra_bands=w["extra_bands"])
+
+
+def measure_jacobi(eng, torch, stream, w):
+    """Roofline of the dominant kernel (jacobi_sweep_kernel): one cold Poisson solve on the
+    workload's grid with the reference stop rule; algorithmic bytes per sweep = 24 B per
+    interior point (read V, read rho, write V')."""
+    import dft_b200
+    g = dft_b200.CartesianGrid(*w["n"], *w["bounds"])
+    N = g.getSize()
+    x = np.linspace(w["bounds"][0], w["bounds"][1], w["n"][0])
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    rho = np.zeros(N)
+    for (px, py, pz) in w["xyz"]:
+        rho += np.exp(-((X - px) ** 2 + (Y - py) ** 2 + (Z - pz) ** 2)).ravel() / np.pi ** 1.5
+    d_rho, d_vh = eng.upload(rho), eng.array(N)
+    eng.hartree(g, d_rho, d_vh)  # warm
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        sweeps, _ = eng.hartree(g, d_rho, d_vh)
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    nx, ny, nz = w["n"]
+    interior = (nx - 2) * (ny - 2) * (nz - 2)
+    bytes_per_sweep = 24.0 * interior
+    return {"sweeps": sweeps, "ms_per_sweep": ms / sweeps, "bytes_per_sweep": bytes_per_sweep,
+            "gbs": bytes_per_sweep / (ms / sweeps * 1e-3) / 1e9}
+
+
+def measure_hpsi(eng, torch, stream, n=(192, 192, 192), bands=16, reps=5):
+    """H psi block at the 192^3 grid: algorithmic bytes per band-point = 8 (read psi) +
+    8 (write H psi) + 8/bands (read V)."""
+    import dft_b200
+    g = dft_b200.CartesianGrid(*n, -19.1, 19.1, -19.1, 19.1, -19.1, 19.1)
+    N = g.getSize()
+    V = eng.array(N)
+    psi = eng.array(N * bands)
+    hp = eng.array(N * bands)
+    tV = torch.empty(0)  # noqa: F841 (torch imported for events only)
+    eng.apply_hamiltonian(g, V, psi, hp, bands, N)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    times = []
+    for _ in range(reps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.apply_hamiltonian(g, V, psi, hp, bands, N)
+            e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    byts = (16.0 + 8.0 / bands) * N * bands
+    return {"grid": list(n), "bands": bands, "ms": ms, "bytes": byts, "gbs": byts / (ms * 1e-3) / 1e9}
+
+
+def cpu_baseline(w, sample_iterations=1):
+    """The reference's own CPU code on this host: initial densities + `sample_iterations`
+    SCF iterations of the workload, scaled to one SCF to |dE| < 1e-6 by the reference's own
+    iteration count for that stop (tests/golden fixture), single-threaded as the reference is."""
+    from oracle.bindings import PBE96, PZ81, Port, Ref, ref_available
+    kind = PBE96 if w["functional"] == "PBE96" else PZ81
+    lib, k = (Ref(), "reference") if ref_available() else (Port(), "port")
+    xyz = np.ravel(w["xyz"])
+    t_init, t_iter = lib.scf_sample(w["n"], w["bounds"], w["Z"], xyz, w["multiplicity"], kind, sample_iterations)
+    iters = None
+    gpath = os.path.join(ROOT, "tests", "golden", "scf_h2_48_ref.json")
+    if os.path.exists(gpath):
+        iters = json.load(open(gpath)).get("h2_48_pz81", {}).get("first_iteration_abs_de_below_1e-6")
+    iters = iters or 10
+    seconds = t_init + iters * t_iter
+    return {"value": 1.0 / seconds, "unit": "SCF/s", "cores": 1, "kind": k,
+            "seconds_to_1e-6": seconds,
+            "sample": f"initial densities ({t_init:.2f} s) + {sample_iterations} SCF iteration(s) "
+                      f"({t_iter:.2f} s each) of the workload, scaled by the reference's {iters} iterations "
+                      f"to |dE|<1e-6"}
+
+
+def run_reference_arm(args, w, rank, world):
+    if rank != 0:
+        return
+    steps = []
+    for s in range(args.warmup + args.steps):
+        cb = cpu_baseline(w, 1)
+        if s >= args.warmup:
+            steps.append(cb)
+    secs = statistics.median(c["seconds_to_1e-6"] for c in steps)
+    val = 1.0 / secs
+    out = {"metric": METRIC, "value": val, "unit": "SCF/s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": args.workload, "desc": w["desc"]},
+           "cpu_baseline": {"value": val, "unit": "SCF/s", "cores": 1, "kind": steps[0]["kind"],
+                            "sample": steps[0]["sample"]},
+           "e2e": {"value": val, "unit": "SCF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="h2_48", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference_arm(args, w, rank, world)
+
+    import torch
+    import dft_b200
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    eng = dft_b200.Engine(local)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    g = dft_b200.CartesianGrid(*w["n"], *w["bounds"])
+    mol = molecule(w)
+    opts = scf_options(w)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        return eng.scf_molecule(g, mol, 0, w["multiplicity"], w["functional"], opts)
+
+    for _ in range(args.warmup):
+        r = step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = []
+    launches0 = eng.launches
+    results = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            r = step()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            results.append(r)
+        torch.cuda.synchronize()
+    launches = eng.launches - launches0
+    total_ms = sum(ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms * 1e-3)
+
+    # e2e through the host C-ABI call, with both spin densities returned to host memory
+    e2e_ms = []
+    for _ in range(max(1, min(3, args.steps))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.scf_molecule(g, mol, 0, w["multiplicity"], w["functional"], opts, want_density=True)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_val = world / (statistics.median(e2e_ms) * 1e-3)
+    N = g.getSize()
+    h2d = len(w["Z"]) * (4 + 24)
+    d2h = 2 * N * 8
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks = load_peaks()
+    jac = measure_jacobi(eng, torch, stream, w)
+    hp = measure_hpsi(eng, torch, stream)
+    last = results[-1]
+    out = {
+        "metric": METRIC, "value": value, "unit": "SCF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"], "grid": list(w["n"]),
+                   "l2": "512 MiB write between steps", "parallelism": f"replicas{world}",
+                   "scf_iterations": last.iterations, "energy": last.total,
+                   "seconds_to_1e-6": ms_per_step / 1e3},
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_val, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "kernel": "jacobi_sweep_kernel", "achieved": jac["gbs"],
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": jac["gbs"] / peaks["hbm_gbs"],
+                     "peak_source": peaks["source"], "traffic": None,
+                     "bytes_per_launch": jac["bytes_per_sweep"], "ms_per_launch": jac["ms_per_sweep"]},
+        "hpsi": {"achieved": hp["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": hp["gbs"] / peaks["hbm_gbs"],
+                 "grid": hp["grid"], "bands": hp["bands"], "ms": hp["ms"]},
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(w)
+    print(json.dumps(out), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,291 @@
+// extern "C" boundary of libdft_b200 (declared in include/dft_b200.h): argument checks,
+// context and workspace management, and the translation of dftb::Error into status codes.
+#include <cstring>
+#include <string>
+
+#include "ops.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+template <class F>
+dft_status_t guard(dft_context* ctx, F&& f) {
+    try {
+        if (ctx) {
+            cudaError_t e = cudaSetDevice(ctx->device);
+            if (e != cudaSuccess) {
+                g_error = std::string("cudaSetDevice failed: ") + cudaGetErrorString(e);
+                return DFT_CUDA_ERROR;
+            }
+        }
+        f();
+        return DFT_OK;
+    } catch (const dftb::Error& e) {
+        g_error = e.what();
+        return e.status;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return DFT_INVALID_ARGUMENT;
+    }
+}
+
+#define NEED(cond, msg)                                               \
+    do {                                                              \
+        if (!(cond)) ::dftb::fail(DFT_INVALID_ARGUMENT, "%s", msg);   \
+    } while (0)
+
+}  // namespace
+
+namespace dftb {
+
+void* ws_get(dft_context* ctx, int slot, size_t bytes) {
+    Workspace& w = ctx->ws[slot];
+    if (w.bytes >= bytes && w.ptr) return w.ptr;
+    if (w.ptr) {
+        // kernels queued on the stream may still read the old buffer
+        DFT_CUDA(cudaStreamSynchronize(ctx->stream));
+        DFT_CUDA(cudaFree(w.ptr));
+        w.ptr = nullptr;
+        w.bytes = 0;
+    }
+    const size_t want = std::max<size_t>(bytes, 256);
+    DFT_CUDA(cudaMalloc(&w.ptr, want));
+    w.bytes = want;
+    return w.ptr;
+}
+
+double* pinned(dft_context* ctx, size_t count) {
+    const size_t bytes = std::max<size_t>(count, 8) * sizeof(double);
+    if (ctx->host_pinned_bytes < bytes) {
+        DFT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (ctx->host_pinned) DFT_CUDA(cudaFreeHost(ctx->host_pinned));
+        ctx->host_pinned = nullptr;
+        DFT_CUDA(cudaMallocHost(&ctx->host_pinned, bytes));
+        ctx->host_pinned_bytes = bytes;
+    }
+    return ctx->host_pinned;
+}
+
+void sync(dft_context* ctx) { DFT_CUDA(cudaStreamSynchronize(ctx->stream)); }
+
+}  // namespace dftb
+
+extern "C" {
+
+const char* dft_last_error_message(void) { return g_error.c_str(); }
+const char* dft_version(void) { return "dft_b200 0.1 (sm_100a)"; }
+
+dft_status_t dft_context_create(int device, dft_context** out) {
+    return guard(nullptr, [&] {
+        NEED(out, "out is NULL");
+        int n = 0;
+        DFT_CUDA(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) dftb::fail(DFT_INVALID_ARGUMENT, "device %d out of range (%d devices)", device, n);
+        DFT_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        DFT_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10)
+            dftb::fail(DFT_CUDA_ERROR, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+        auto* c = new dft_context();
+        c->device = device;
+        c->num_sms = prop.multiProcessorCount;
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete c;
+            dftb::fail(DFT_CUDA_ERROR, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
+        }
+        *out = c;
+    });
+}
+
+dft_status_t dft_context_destroy(dft_context* ctx) {
+    if (!ctx) return DFT_OK;
+    dft_status_t s = guard(ctx, [&] {
+        DFT_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (auto& w : ctx->ws)
+            if (w.ptr) cudaFree(w.ptr);
+        if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+        cudaStreamDestroy(ctx->stream);
+    });
+    delete ctx;
+    return s;
+}
+
+dft_status_t dft_context_synchronize(dft_context* ctx) {
+    return guard(ctx, [&] {
+        NEED(ctx, "context is NULL");
+        dftb::sync(ctx);
+    });
+}
+
+void* dft_context_stream(dft_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+long long dft_context_launch_count(dft_context* ctx) { return ctx ? ctx->launches : 0; }
+
+dft_status_t dft_device_alloc(dft_context* ctx, size_t bytes, void** out) {
+    return guard(ctx, [&] {
+        NEED(ctx && out, "NULL argument");
+        DFT_CUDA(cudaMalloc(out, std::max<size_t>(bytes, 1)));
+    });
+}
+dft_status_t dft_device_free(dft_context* ctx, void* ptr) {
+    return guard(ctx, [&] {
+        NEED(ctx, "context is NULL");
+        if (ptr) {
+            DFT_CUDA(cudaStreamSynchronize(ctx->stream));
+            DFT_CUDA(cudaFree(ptr));
+        }
+    });
+}
+dft_status_t dft_copy_h2d(dft_context* ctx, void* dst, const void* src, size_t bytes) {
+    return guard(ctx, [&] {
+        NEED(ctx && dst && src, "NULL argument");
+        DFT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        dftb::sync(ctx);
+    });
+}
+dft_status_t dft_copy_d2h(dft_context* ctx, void* dst, const void* src, size_t bytes) {
+    return guard(ctx, [&] {
+        NEED(ctx && dst && src, "NULL argument");
+        DFT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        dftb::sync(ctx);
+    });
+}
+
+dft_status_t dft_apply_hamiltonian_dev(dft_context* ctx, const dft_grid* g, const double* V, const double* psi,
+                                       double* hpsi, int nbands, long ld) {
+    return guard(ctx, [&] {
+        NEED(ctx && V && psi && hpsi, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        NEED(nbands >= 0, "nbands must be >= 0");
+        NEED(ld >= G.N, "ld must be >= nx*ny*nz");
+        dftb::apply_hamiltonian(ctx, G, V, psi, hpsi, nbands, ld);
+    });
+}
+
+dft_status_t dft_hartree_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
+                             long max_sweeps, long* sweeps_out, double* last_diff_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && rho && vh, "NULL argument");
+        NEED(rho != vh, "rho and vh must not alias");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::JacobiResult r = dftb::hartree(ctx, G, rho, vh, tol, max_sweeps);
+        dftb::sync(ctx);
+        if (sweeps_out) *sweeps_out = r.sweeps;
+        if (last_diff_out) *last_diff_out = r.last_diff;
+    });
+}
+
+dft_status_t dft_hartree_energy_dev(dft_context* ctx, const dft_grid* g, const double* rho, const double* vh,
+                                    double* energy_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && rho && vh && energy_out, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        *energy_out = 0.5 * dftb::dot(ctx, G.N, rho, vh) * G.dV;
+    });
+}
+
+dft_status_t dft_xc_dev(dft_context* ctx, const dft_grid* g, dft_xc_kind kind, const double* na, const double* nb,
+                        double* va, double* vb, double* exc_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && na && nb, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        const double e = dftb::xc(ctx, G, (int)kind, na, nb, va, vb, exc_out != nullptr);
+        dftb::sync(ctx);
+        if (exc_out) *exc_out = e;
+    });
+}
+
+dft_status_t dft_xc_evaluate_dev(dft_context* ctx, dft_xc_kind kind, long m, const double* na, const double* nb,
+                                 const double* ga, const double* gb, double* out5) {
+    return guard(ctx, [&] {
+        NEED(ctx && na && nb && ga && gb && out5, "NULL argument");
+        NEED(m >= 0, "m must be >= 0");
+        dftb::xc_evaluate(ctx, (int)kind, m, na, nb, ga, gb, out5);
+    });
+}
+
+dft_status_t dft_spin_density_dev(dft_context* ctx, long npoints, const double* psi, int nbands, long ld,
+                                  const double* occ, double* out) {
+    return guard(ctx, [&] {
+        NEED(ctx && psi && occ && out, "NULL argument");
+        NEED(nbands > 0, "La lista de orbitales moleculares no puede estar vacia.");
+        NEED(npoints > 0 && ld >= npoints, "bad sizes");
+        dftb::spin_density(ctx, npoints, psi, nbands, ld, occ, out);
+    });
+}
+
+dft_status_t dft_kinetic_energy_dev(dft_context* ctx, const dft_grid* g, const double* psi, int nbands, long ld,
+                                    const double* occ, double* energy_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && psi && occ && energy_out, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        NEED(ld >= G.N, "ld must be >= nx*ny*nz");
+        *energy_out = dftb::kinetic_energy(ctx, G, psi, nbands, ld, occ);
+    });
+}
+
+dft_status_t dft_nuclear_potential_dev(dft_context* ctx, const dft_grid* g, int nnuc, const int* Z,
+                                       const double* xyz, double* vext) {
+    return guard(ctx, [&] {
+        NEED(ctx && Z && xyz && vext, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::nuclear_potential(ctx, G, nnuc, Z, xyz, vext);
+    });
+}
+
+dft_status_t dft_solve_orbitals_dev(dft_context* ctx, const dft_grid* g, const double* V, int nocc, int nbands,
+                                    double* psi, long ld, int init, double* eig, const dft_eig_opts* opts,
+                                    int* iterations_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && V && psi && eig, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::EigOpts o;
+        if (opts) {
+            if (opts->tol > 0) o.tol = opts->tol;
+            if (opts->max_iterations > 0) o.max_iterations = opts->max_iterations;
+            if (opts->max_subspace >= 2) o.max_subspace = opts->max_subspace;
+            o.verbose = opts->verbose;
+        }
+        const int it = dftb::solve_orbitals(ctx, G, V, nocc, nbands, psi, ld, init != 0, eig, nullptr, o);
+        if (iterations_out) *iterations_out = it;
+    });
+}
+
+void dft_scf_default_options(dft_scf_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->max_iterations = 250;        // DFTConstants.h:13
+    o->energy_tol = 1.0e-11;        // DFTConstants.h:16
+    o->density_tol = 1.0e-9;        // DFTConstants.h:15
+    o->ks_tol = 1.0e-7;             // DFTConstants.h:17
+    o->stop_abs_de = 0.0;
+    o->poisson_tol = 1.0e-8;        // HartreePotentialMolecule.cpp:15
+    o->poisson_max_sweeps = 10000;  // HartreePotentialMolecule.cpp:14
+    o->extra_bands = 3;
+    o->eig.tol = 1.0e-7;            // EigenvalueSolverMolecule.cpp:19
+    o->eig.max_iterations = 2000;
+    o->eig.max_subspace = 3;
+    o->eig.verbose = 0;
+    o->verbose = 0;
+}
+
+dft_status_t dft_scf_molecule(dft_context* ctx, const dft_grid* g, int nnuc, const int* Z, const double* xyz,
+                              int charge, int multiplicity, dft_xc_kind kind, const dft_scf_opts* opts,
+                              dft_scf_result* result) {
+    return guard(ctx, [&] {
+        NEED(ctx && Z && xyz && result, "NULL argument");
+        dftb::scf_molecule(ctx, g, nnuc, Z, xyz, charge, multiplicity, (int)kind, opts, result);
+    });
+}
+
+dft_status_t dft_solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, long points, double rmax,
+                             dft_atom_result* results) {
+    return guard(ctx, [&] {
+        NEED(ctx && Z && kinds && results, "NULL argument");
+        NEED(nruns > 0, "nruns must be > 0");
+        dftb::solve_atoms(ctx, nruns, Z, kinds, points, rmax, results);
+    });
+}
+
+}  // extern "C"

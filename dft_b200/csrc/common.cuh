@@ -1,0 +1,161 @@
+// Shared host/device plumbing for the dft_b200 kernels: status handling, the context,
+// the device grid descriptor and deterministic block reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/dft_b200.h"
+
+namespace dftb {
+
+// ---------------------------------------------------------------- status -----
+// Internal code throws dftb::Error; the C ABI converts it into a status + message.
+struct Error : std::runtime_error {
+    dft_status_t status;
+    Error(dft_status_t s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] inline void fail(dft_status_t s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    throw Error(s, buf);
+}
+
+#define DFT_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            ::dftb::fail(DFT_CUDA_ERROR, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),    \
+                         __FILE__, __LINE__);                                                       \
+    } while (0)
+
+#define DFT_LAUNCH_CHECK() DFT_CUDA(cudaGetLastError())
+
+// ---------------------------------------------------------------- grid -------
+// Device-side grid descriptor.  Spacing and inverse squares are derived on the host in
+// the reference's operation order (CartesianGrid.cpp:45-47, KohnShamHamiltonianMolecule.cpp:45-55).
+struct Grid {
+    int nx, ny, nz;
+    long long N;
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    double dx, dy, dz;
+    double ix2, iy2, iz2;  // 1/(d*d)
+    double dV;             // dx*dy*dz
+};
+
+inline Grid make_grid(const dft_grid* g) {
+    if (!g) fail(DFT_INVALID_ARGUMENT, "grid is NULL");
+    if (g->nx < 2 || g->ny < 2 || g->nz < 2)
+        fail(DFT_INVALID_ARGUMENT, "CartesianGrid requires at least two points per dimension.");
+    if (g->xmax <= g->xmin || g->ymax <= g->ymin || g->zmax <= g->zmin)
+        fail(DFT_INVALID_ARGUMENT, "CartesianGrid requires valid spatial bounds.");
+    if (g->nx > (1 << 20) || g->ny > (1 << 20) || g->nz > (1 << 20))
+        fail(DFT_INVALID_ARGUMENT, "grid dimension too large");
+    Grid d;
+    d.nx = (int)g->nx;
+    d.ny = (int)g->ny;
+    d.nz = (int)g->nz;
+    d.N = (long long)g->nx * g->ny * g->nz;
+    d.xmin = g->xmin; d.xmax = g->xmax;
+    d.ymin = g->ymin; d.ymax = g->ymax;
+    d.zmin = g->zmin; d.zmax = g->zmax;
+    d.dx = (g->xmax - g->xmin) / (double)(g->nx - 1);
+    d.dy = (g->ymax - g->ymin) / (double)(g->ny - 1);
+    d.dz = (g->zmax - g->zmin) / (double)(g->nz - 1);
+    d.ix2 = 1.0 / (d.dx * d.dx);
+    d.iy2 = 1.0 / (d.dy * d.dy);
+    d.iz2 = 1.0 / (d.dz * d.dz);
+    d.dV = d.dx * d.dy * d.dz;
+    return d;
+}
+
+// ---------------------------------------------------------------- context ----
+// Device workspace that grows on demand and is reused across calls.
+struct Workspace {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace dftb
+
+struct dft_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    long long launches = 0;
+    int num_sms = 148;
+    // named scratch buffers (reductions, Jacobi ping-pong, XC intermediates, Davidson)
+    dftb::Workspace ws[24];
+    double* host_pinned = nullptr;  // small pinned staging area for scalars
+    size_t host_pinned_bytes = 0;
+};
+
+namespace dftb {
+
+enum WsSlot {
+    WS_REDUCE = 0,   // block partial sums
+    WS_CTRL = 1,     // small control words (Jacobi state, flags)
+    WS_JACOBI = 2,   // Jacobi ping-pong buffer
+    WS_XC = 3,       // XC intermediates (4N)
+    WS_DAV0 = 4,     // Davidson workspaces
+    WS_DAV1 = 5,
+    WS_DAV2 = 6,
+    WS_DAV3 = 7,
+    WS_DAV4 = 8,
+    WS_DAV5 = 9,
+    WS_SMALL = 10,   // small dense matrices on device
+    WS_SCF0 = 11,
+    WS_SCF1 = 12,
+    WS_RADIAL = 13,
+    WS_TMP = 14,
+    WS_TMP2 = 15,
+    WS_DAV6 = 16,    // Davidson per-band scalars on device
+    WS_SCF2 = 17,
+    WS_SCF3 = 18,
+    WS_NUM = 24,
+};
+
+void* ws_get(dft_context* ctx, int slot, size_t bytes);
+double* pinned(dft_context* ctx, size_t count);
+void sync(dft_context* ctx);
+
+// Counts a launch on the context (bench reports how many kernels ran in a timed region).
+inline void count_launch(dft_context* ctx, long long n = 1) { ctx->launches += n; }
+
+// ---------------------------------------------------------------- device helpers --
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum in a fixed order (deterministic for a fixed launch shape).
+// `sh` must hold blockDim/32 doubles.  Result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < nw; ++w) s += sh[w];
+    __syncthreads();
+    return s;
+}
+
+}  // namespace dftb

@@ -1,0 +1,457 @@
+// Block Davidson eigensolver for H = -1/2 lap_h + V on the device.
+//
+// The reference solves one orbital at a time with a single-vector Davidson, deflating each
+// new orbital against all previous ones (EigenvalueSolverMolecule.cpp:666-1300).  That
+// costs O(i N) vector passes per step for orbital i and runs one H psi at a time.  Here all
+// nbands bands advance together:
+//
+//   basis V (orthonormal, dV-weighted), AV = H V
+//   G = dV V^T AV  -> eigh(G) -> Ritz pairs (theta, Y) for the lowest nbands
+//   X = V Y, AX = AV Y, R = AX - X theta, |r_b| = sqrt(dV sum R_b^2)
+//   occupied bands converge at |r_b| < tol (reference MO_RESIDUAL_TOLERANCE = 1e-7)
+//   T = R_b / (theta_b - diag) for unconverged bands (the reference's davidsonCorrection,
+//       :521-555, with the same 1e-10 guard), projected out of V twice and orthonormalised
+//       by the symmetric (SVQB) scheme, then appended; thick restart to [X] when full.
+//
+// Tall-skinny products (Gram V^T W, rotation V Y) are FP64 kernels with warp/block
+// reductions; the k x k eigenproblems are solved on the host (eigh.cpp).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "eigh.h"
+#include "ops.h"
+
+namespace dftb {
+
+namespace {
+
+// ------------------------------------------------------------------ kernels ----------
+
+// buildInitialVector (reference EigenvalueSolverMolecule.cpp:177-283) for seeds seed0+b.
+__global__ void seed_kernel(Grid g, double* psi, long long ld, int nb, int seed0) {
+    const int b = blockIdx.y;
+    const int idx = seed0 + b;
+    const double cx = 0.5 * (g.xmin + g.xmax), cy = 0.5 * (g.ymin + g.ymax), cz = 0.5 * (g.zmin + g.zmax);
+    const double sigma = 0.8 + 0.18 * (double)idx;
+    const double factor = 1.0 / (2.0 * sigma * sigma);
+    const int mode = idx % 9;
+    double* out = psi + (long long)b * ld;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx);
+        const int j = (int)((p / g.nx) % g.ny);
+        const int k = (int)(p / ((long long)g.nx * g.ny));
+        const double x = __dadd_rn(g.xmin, __dmul_rn((double)i, g.dx)) - cx;
+        const double y = __dadd_rn(g.ymin, __dmul_rn((double)j, g.dy)) - cy;
+        const double z = __dadd_rn(g.zmin, __dmul_rn((double)k, g.dz)) - cz;
+        const double r2 = x * x + y * y + z * z;
+        double pl = 1.0;
+        switch (mode) {
+            case 1: pl = x; break;
+            case 2: pl = y; break;
+            case 3: pl = z; break;
+            case 4: pl = x * y; break;
+            case 5: pl = x * z; break;
+            case 6: pl = y * z; break;
+            case 7: pl = x * x - y * y; break;
+            case 8: pl = 2.0 * z * z - x * x - y * y; break;
+            default: break;
+        }
+        out[p] = pl * exp(-r2 * factor);
+    }
+}
+
+constexpr int GT = 32;          // Gram output tile (GT x GT)
+constexpr int GP = 32;          // points per shared-memory stage
+constexpr int GRAM_THREADS = 256;
+
+// partial[c][i][j] = sum over chunk c of A_i[p] B_j[p] for one GT x GT output tile.
+// 256 threads = 16 x 16, each owns a 2 x 2 block of the tile.
+__global__ void __launch_bounds__(GRAM_THREADS) gram_kernel(const double* __restrict__ A, long long lda, int ka,
+                                                            const double* __restrict__ B, long long ldb, int kb,
+                                                            long long n, long long chunk, double* __restrict__ partial) {
+    __shared__ double sa[GT][GP + 1];
+    __shared__ double sb[GT][GP + 1];
+    const int ti = blockIdx.x * GT, tj = blockIdx.y * GT;
+    const long long p0 = (long long)blockIdx.z * chunk;
+    const long long p1 = min(n, p0 + chunk);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc00 = 0.0, acc01 = 0.0, acc10 = 0.0, acc11 = 0.0;
+    for (long long ps = p0; ps < p1; ps += GP) {
+        // stage GT vectors x GP points of A and B (coalesced along points)
+        for (int e = threadIdx.x; e < GT * GP; e += GRAM_THREADS) {
+            const int r = e / GP, c = e % GP;
+            const long long p = ps + c;
+            const int ia = ti + r, jb = tj + r;
+            sa[r][c] = (ia < ka && p < p1) ? A[(long long)ia * lda + p] : 0.0;
+            sb[r][c] = (jb < kb && p < p1) ? B[(long long)jb * ldb + p] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int c = 0; c < GP; ++c) {
+            const double a0 = sa[ty][c], a1 = sa[ty + 16][c];
+            const double b0 = sb[tx][c], b1 = sb[tx + 16][c];
+            acc00 += a0 * b0;
+            acc01 += a0 * b1;
+            acc10 += a1 * b0;
+            acc11 += a1 * b1;
+        }
+        __syncthreads();
+    }
+    double* out = partial + (long long)blockIdx.z * ka * kb;
+    const int i0 = ti + ty, i1 = ti + ty + 16, j0 = tj + tx, j1 = tj + tx + 16;
+    if (i0 < ka && j0 < kb) out[(long long)i0 * kb + j0] = acc00;
+    if (i0 < ka && j1 < kb) out[(long long)i0 * kb + j1] = acc01;
+    if (i1 < ka && j0 < kb) out[(long long)i1 * kb + j0] = acc10;
+    if (i1 < ka && j1 < kb) out[(long long)i1 * kb + j1] = acc11;
+}
+
+// out[e] = scale * sum_c partial[c][e], fixed chunk order
+__global__ void gram_reduce_kernel(int nchunks, int nel, const double* __restrict__ partial, double scale,
+                                   double* __restrict__ out) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < nchunks; ++c) s += partial[(long long)c * nel + e];
+        out[e] = s * scale;
+    }
+}
+
+constexpr int RJ = 16;  // output columns per rotation block
+
+// out_j = beta*out_j + alpha * sum_i in_i * Y[i*m + j], j in a RJ-column slice per blockIdx.y
+__global__ void __launch_bounds__(256) rotate_kernel(const double* __restrict__ in, long long ldi, int k,
+                                                     const double* __restrict__ Y, int m, double* __restrict__ out,
+                                                     long long ldo, long long n, double alpha, double beta) {
+    extern __shared__ double sy[];  // k x RJ
+    const int j0 = blockIdx.y * RJ;
+    const int nj = min(RJ, m - j0);
+    for (int e = threadIdx.x; e < k * RJ; e += blockDim.x) {
+        const int i = e / RJ, jj = e % RJ;
+        sy[e] = jj < nj ? Y[(long long)i * m + j0 + jj] : 0.0;
+    }
+    __syncthreads();
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        double acc[RJ];
+#pragma unroll
+        for (int jj = 0; jj < RJ; ++jj) acc[jj] = 0.0;
+        for (int i = 0; i < k; ++i) {
+            const double v = __ldg(in + (long long)i * ldi + p);
+#pragma unroll
+            for (int jj = 0; jj < RJ; ++jj) acc[jj] += v * sy[i * RJ + jj];
+        }
+#pragma unroll
+        for (int jj = 0; jj < RJ; ++jj) {
+            if (jj < nj) {
+                double* o = out + (long long)(j0 + jj) * ldo + p;
+                *o = beta == 0.0 ? alpha * acc[jj] : beta * *o + alpha * acc[jj];
+            }
+        }
+    }
+}
+
+// R_b = AX_b - theta_b X_b and per-block partial sums of R_b^2 (blockIdx.y = band)
+__global__ void __launch_bounds__(256) residual_kernel(const double* __restrict__ AX, const double* __restrict__ X,
+                                                       const double* __restrict__ theta, double* __restrict__ R,
+                                                       long long ld, long long n, double* __restrict__ partial) {
+    __shared__ double sh[8];
+    const int b = blockIdx.y;
+    const double t = theta[b];
+    const double* ax = AX + (long long)b * ld;
+    const double* x = X + (long long)b * ld;
+    double* r = R + (long long)b * ld;
+    double s = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double v = ax[p] - t * x[p];
+        r[p] = v;
+        s += v * v;
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partial[(long long)b * gridDim.x + blockIdx.x] = s;
+}
+
+// T_a = R_src(a) / (theta - (kin + V)) with the reference guard (|den| < 1e-10 or non-finite
+// -> T = R), reference davidsonCorrection :521-555, buildHamiltonianDiagonal :483-519.
+__global__ void precond_kernel(const double* __restrict__ R, const double* __restrict__ V, const int* __restrict__ src,
+                               const double* __restrict__ theta, double* __restrict__ T, long long ld, long long n,
+                               double kin) {
+    const int a = blockIdx.y;
+    const int b = src[a];
+    const double t = theta[b];
+    const double* r = R + (long long)b * ld;
+    double* o = T + (long long)a * ld;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double den = t - (kin + V[p]);
+        o[p] = (!isfinite(den) || fabs(den) < 1.0e-10) ? r[p] : r[p] / den;
+    }
+}
+
+__global__ void rows_sum_kernel2(int nrows, int ncols, const double* partial, double* out) {
+    __shared__ double sh[32];
+    for (int r = 0; r < nrows; ++r) {
+        double s = 0.0;
+        for (int c = threadIdx.x; c < ncols; c += blockDim.x) s += partial[(long long)r * ncols + c];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) out[r] = s;
+    }
+}
+
+// ------------------------------------------------------------------ host helpers -----
+
+struct Blocks {
+    dft_context* ctx;
+    Grid g;
+    long long ld;
+};
+
+// C (ka x kb, host, row-major) = dV * A^T B
+void gram(dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B, long long ldb,
+          int kb, std::vector<double>& C) {
+    C.assign((size_t)ka * kb, 0.0);
+    if (ka == 0 || kb == 0) return;
+    const int tx = (ka + GT - 1) / GT, ty = (kb + GT - 1) / GT;
+    long long target = 4LL * ctx->num_sms;
+    long long nch = std::max<long long>(1, target / (tx * ty));
+    long long chunk = (g.N + nch - 1) / nch;
+    chunk = ((chunk + GP - 1) / GP) * GP;
+    nch = (g.N + chunk - 1) / chunk;
+    nch = std::min<long long>(nch, 65535);
+    chunk = (g.N + nch - 1) / nch;
+    const size_t nel = (size_t)ka * kb;
+    double* partial = (double*)ws_get(ctx, WS_SMALL, sizeof(double) * (nel * nch + nel));
+    double* res = partial + nel * nch;
+    gram_kernel<<<dim3(tx, ty, (unsigned)nch), GRAM_THREADS, 0, ctx->stream>>>(A, lda, ka, B, ldb, kb, g.N, chunk,
+                                                                               partial);
+    DFT_LAUNCH_CHECK();
+    const int rb = (int)std::min<size_t>((nel + 255) / 256, 1024);
+    gram_reduce_kernel<<<rb, 256, 0, ctx->stream>>>((int)nch, (int)nel, partial, g.dV, res);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx, 2);
+    double* h = pinned(ctx, nel);
+    DFT_CUDA(cudaMemcpyAsync(h, res, sizeof(double) * nel, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    std::memcpy(C.data(), h, sizeof(double) * nel);
+}
+
+// out = beta*out + alpha * in * Y   (Y: k x m host row-major)
+void rotate(dft_context* ctx, const Grid& g, const double* in, long long ldi, int k, const std::vector<double>& Y, int m,
+            double* out, long long ldo, double alpha, double beta) {
+    if (m == 0) return;
+    if (k == 0) {
+        if (beta == 0.0)
+            for (int j = 0; j < m; ++j)
+                DFT_CUDA(cudaMemsetAsync(out + (long long)j * ldo, 0, sizeof(double) * (size_t)g.N, ctx->stream));
+        return;
+    }
+    double* dy = (double*)ws_get(ctx, WS_TMP, sizeof(double) * (size_t)k * m);
+    DFT_CUDA(cudaMemcpyAsync(dy, Y.data(), sizeof(double) * (size_t)k * m, cudaMemcpyHostToDevice, ctx->stream));
+    const int jt = (m + RJ - 1) / RJ;
+    const size_t smem = sizeof(double) * (size_t)k * RJ;
+    if (smem > 200 * 1024) fail(DFT_INVALID_ARGUMENT, "subspace too large for the rotation kernel (k=%d)", k);
+    static bool attr_set = false;
+    if (!attr_set) {
+        DFT_CUDA(cudaFuncSetAttribute(rotate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_set = true;
+    }
+    long long bx = (g.N + 255) / 256;
+    bx = std::min<long long>(bx, std::max<long long>(1, (8LL * ctx->num_sms + jt - 1) / jt));
+    rotate_kernel<<<dim3((unsigned)bx, jt), 256, smem, ctx->stream>>>(in, ldi, k, dy, m, out, ldo, g.N, alpha, beta);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
+// Orthonormalise the nt columns of T against V[0:k] and among themselves (dV inner product).
+// Dependent directions are dropped; returns the number kept (compacted to the front of T).
+int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, double* T, int nt, long long ld,
+                   double* W) {
+    std::vector<double> C, S, w, Z, Yk;
+    for (int pass = 0; pass < 2 && nt > 0; ++pass) {
+        if (k > 0) {
+            gram(ctx, g, V, ld, k, T, ld, nt, C);  // k x nt
+            rotate(ctx, g, V, ld, k, C, nt, T, ld, -1.0, 1.0);
+        }
+        gram(ctx, g, T, ld, nt, T, ld, nt, S);
+        for (int i = 0; i < nt; ++i)
+            for (int j = 0; j < i; ++j) S[(size_t)i * nt + j] = S[(size_t)j * nt + i] = 0.5 * (S[(size_t)i * nt + j] + S[(size_t)j * nt + i]);
+        std::vector<double> Sc = S;
+        if (!eigh(nt, Sc, w, Z)) fail(DFT_NUMERICAL, "orthonormalisation eigensolve failed");
+        const double wmax = w[nt - 1];
+        if (!(wmax > 0.0) || !std::isfinite(wmax)) return 0;
+        // keep eigen-directions well above round-off; scale by lambda^{-1/2}
+        std::vector<int> keep;
+        for (int j = 0; j < nt; ++j)
+            if (w[j] > wmax * 1e-13 && w[j] > 1e-24) keep.push_back(j);
+        const int nk = (int)keep.size();
+        Yk.assign((size_t)nt * nk, 0.0);
+        for (int i = 0; i < nt; ++i)
+            for (int c = 0; c < nk; ++c) Yk[(size_t)i * nk + c] = Z[(size_t)i * nt + keep[c]] / std::sqrt(w[keep[c]]);
+        rotate(ctx, g, T, ld, nt, Yk, nk, W, ld, 1.0, 0.0);
+        DFT_CUDA(cudaMemcpyAsync(T, W, sizeof(double) * (size_t)ld * nk, cudaMemcpyDeviceToDevice, ctx->stream));
+        nt = nk;
+    }
+    return nt;
+}
+
+}  // namespace
+
+int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, int nbands, double* psi,
+                   long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o) {
+    if (nocc <= 0) fail(DFT_INVALID_ARGUMENT, "El numero de orbitales debe ser mayor que cero.");
+    if (nbands < nocc) fail(DFT_INVALID_ARGUMENT, "nbands must be >= the number of orbitals");
+    if (nbands > g.N) fail(DFT_INVALID_ARGUMENT, "more bands than grid points");
+    if (ld < g.N) fail(DFT_INVALID_ARGUMENT, "ld must be >= nx*ny*nz");
+    const int nb = nbands;
+    const int kmax = (int)std::max<long long>(2LL * nb, std::min<long long>(o.max_subspace * (long long)nb, g.N));
+    const size_t vecb = sizeof(double) * (size_t)ld;
+    double* Vb = (double*)ws_get(ctx, WS_DAV0, vecb * kmax);
+    double* AV = (double*)ws_get(ctx, WS_DAV1, vecb * kmax);
+    double* X = (double*)ws_get(ctx, WS_DAV2, vecb * nb);
+    double* AX = (double*)ws_get(ctx, WS_DAV3, vecb * nb);
+    double* R = (double*)ws_get(ctx, WS_DAV4, vecb * nb);
+    double* W = (double*)ws_get(ctx, WS_DAV5, vecb * std::max(nb, 1));
+    const double kin = g.ix2 + g.iy2 + g.iz2;  // buildHamiltonianDiagonal :496-500 (1/dx^2 + 1/dy^2 + 1/dz^2)
+    const int eb = std::max(1, std::min((int)((g.N + 255) / 256), ctx->num_sms * 2));
+
+    // ---- start block: given vectors or the reference's seeds --------------------------
+    if (init) {
+        DFT_CUDA(cudaMemcpy2DAsync(Vb, vecb, psi, vecb, sizeof(double) * (size_t)g.N, nb, cudaMemcpyDeviceToDevice,
+                                   ctx->stream));
+    } else {
+        seed_kernel<<<dim3(eb, nb), 256, 0, ctx->stream>>>(g, Vb, ld, nb, 0);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+    }
+    int k = orthonormalise(ctx, g, Vb, 0, Vb, nb, ld, W);
+    int seed = nb;
+    while (k < nb) {  // rank-deficient start: top up with further seeds
+        const int need = nb - k;
+        seed_kernel<<<dim3(eb, need), 256, 0, ctx->stream>>>(g, Vb + (long long)k * ld, ld, need, seed);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+        seed += need;
+        const int got = orthonormalise(ctx, g, Vb, k, Vb + (long long)k * ld, need, ld, W);
+        k += got;
+        if (seed > nb + 512) fail(DFT_NOT_CONVERGED, "No se pudo construir el vector inicial.");
+    }
+    apply_hamiltonian(ctx, g, V, Vb, AV, k, ld);
+
+    std::vector<double> G;  // k x k, row-major, grows
+    auto grow_G = [&](int k_old, int k_new) {
+        std::vector<double> Gn((size_t)k_new * k_new, 0.0);
+        for (int i = 0; i < k_old; ++i)
+            for (int j = 0; j < k_old; ++j) Gn[(size_t)i * k_new + j] = G[(size_t)i * k_old + j];
+        std::vector<double> C;
+        gram(ctx, g, Vb, ld, k_new, AV + (long long)k_old * ld, ld, k_new - k_old, C);  // k_new x (k_new-k_old)
+        const int nn = k_new - k_old;
+        for (int i = 0; i < k_new; ++i)
+            for (int c = 0; c < nn; ++c) {
+                const int j = k_old + c;
+                const double v = C[(size_t)i * nn + c];
+                if (i >= k_old && i < j) continue;  // set from the symmetric partner below
+                Gn[(size_t)i * k_new + j] = v;
+                Gn[(size_t)j * k_new + i] = v;
+            }
+        // symmetrise the new diagonal block
+        for (int a = k_old; a < k_new; ++a)
+            for (int b2 = k_old; b2 < a; ++b2) {
+                const double v = 0.5 * (C[(size_t)a * nn + (b2 - k_old)] + C[(size_t)b2 * nn + (a - k_old)]);
+                Gn[(size_t)a * k_new + b2] = Gn[(size_t)b2 * k_new + a] = v;
+            }
+        G.swap(Gn);
+    };
+    grow_G(0, k);
+
+    double* dtheta = (double*)ws_get(ctx, WS_DAV6, sizeof(double) * nb + sizeof(int) * nb + 64);
+    int* dsrc = (int*)(dtheta + nb);
+    std::vector<double> theta(nb), rn(nb), w, Z, Y;
+    std::vector<int> active;
+    int it = 0;
+    bool done = false;
+    for (it = 1; it <= o.max_iterations; ++it) {
+        // ---- Rayleigh–Ritz --------------------------------------------------------------
+        std::vector<double> Gc = G;
+        if (!eigh(k, Gc, w, Z)) fail(DFT_NUMERICAL, "projected eigensolve failed");
+        Y.assign((size_t)k * nb, 0.0);
+        for (int i = 0; i < k; ++i)
+            for (int j = 0; j < nb; ++j) Y[(size_t)i * nb + j] = Z[(size_t)i * k + j];
+        for (int j = 0; j < nb; ++j) theta[j] = w[j];
+        rotate(ctx, g, Vb, ld, k, Y, nb, X, ld, 1.0, 0.0);
+        rotate(ctx, g, AV, ld, k, Y, nb, AX, ld, 1.0, 0.0);
+        // ---- residuals --------------------------------------------------------------------
+        DFT_CUDA(cudaMemcpyAsync(dtheta, theta.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, ctx->stream));
+        double* partial = (double*)ws_get(ctx, WS_REDUCE, sizeof(double) * ((size_t)eb * nb + nb));
+        residual_kernel<<<dim3(eb, nb), 256, 0, ctx->stream>>>(AX, X, dtheta, R, ld, g.N, partial);
+        DFT_LAUNCH_CHECK();
+        rows_sum_kernel2<<<1, 256, 0, ctx->stream>>>(nb, eb, partial, partial + (size_t)eb * nb);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx, 2);
+        double* hs = pinned(ctx, nb);
+        DFT_CUDA(cudaMemcpyAsync(hs, partial + (size_t)eb * nb, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        sync(ctx);
+        bool occ_conv = true;
+        active.clear();
+        for (int b = 0; b < nb; ++b) {
+            rn[b] = std::isfinite(hs[b]) ? std::sqrt(hs[b] * g.dV) : INFINITY;
+            if (!std::isfinite(rn[b])) fail(DFT_NUMERICAL, "non-finite residual in band %d", b);
+            const double tb = b < nocc ? o.tol : std::max(o.tol, 1e-4);
+            if (b < nocc && !(rn[b] < o.tol)) occ_conv = false;
+            if (!(rn[b] < tb)) active.push_back(b);
+        }
+        if (o.verbose) {
+            double mx = 0.0;
+            for (int b = 0; b < nocc; ++b) mx = std::max(mx, rn[b]);
+            fprintf(stderr, "[davidson] it=%d k=%d active=%zu max_occ_res=%.3e theta0=%.10f\n", it, k, active.size(), mx,
+                    theta[0]);
+        }
+        if (occ_conv) {
+            done = true;
+            break;
+        }
+        if (it == o.max_iterations) break;
+        // ---- corrections ------------------------------------------------------------------
+        const int na = (int)active.size();
+        if (k + na > kmax) {  // thick restart to the current Ritz block
+            DFT_CUDA(cudaMemcpyAsync(Vb, X, vecb * nb, cudaMemcpyDeviceToDevice, ctx->stream));
+            DFT_CUDA(cudaMemcpyAsync(AV, AX, vecb * nb, cudaMemcpyDeviceToDevice, ctx->stream));
+            k = nb;
+            G.assign((size_t)k * k, 0.0);
+            for (int i = 0; i < k; ++i) G[(size_t)i * k + i] = theta[i];
+        }
+        double* T = Vb + (long long)k * ld;
+        DFT_CUDA(cudaMemcpyAsync(dsrc, active.data(), sizeof(int) * na, cudaMemcpyHostToDevice, ctx->stream));
+        precond_kernel<<<dim3(eb, na), 256, 0, ctx->stream>>>(R, V, dsrc, dtheta, T, ld, g.N, kin);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+        int nt = orthonormalise(ctx, g, Vb, k, T, na, ld, W);
+        if (nt == 0) {
+            // preconditioned directions fell into the basis: fall back to raw residuals
+            for (int a = 0; a < na; ++a)
+                DFT_CUDA(cudaMemcpyAsync(T + (long long)a * ld, R + (long long)active[a] * ld, vecb,
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+            nt = orthonormalise(ctx, g, Vb, k, T, na, ld, W);
+            if (nt == 0) fail(DFT_NOT_CONVERGED, "La direccion de expansion Davidson es numericamente dependiente.");
+        }
+        apply_hamiltonian(ctx, g, V, T, AV + (long long)k * ld, nt, ld);
+        grow_G(k, k + nt);
+        k += nt;
+    }
+    // ---- outputs -----------------------------------------------------------------------
+    DFT_CUDA(cudaMemcpy2DAsync(psi, vecb, X, vecb, sizeof(double) * (size_t)g.N, nb, cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+    for (int b = 0; b < nb; ++b) {
+        eig_host[b] = theta[b];
+        if (resid_host) resid_host[b] = rn[b];
+    }
+    sync(ctx);
+    if (!done) {
+        double mx = 0.0;
+        for (int b = 0; b < nocc; ++b) mx = std::max(mx, rn[b]);
+        fail(DFT_NOT_CONVERGED, "El orbital molecular no convergio. residual = %g after %d iterations", mx,
+             o.max_iterations);
+    }
+    return it;
+}
+
+}  // namespace dftb

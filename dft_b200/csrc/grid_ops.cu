@@ -1,0 +1,761 @@
+// Grid operators of the 3D Kohn–Sham path on sm_100a: H psi, Jacobi Poisson, XC, density,
+// energies, the nuclear potential and the deterministic reductions they need.
+//
+// Layout: one FP64 array per field, x fastest ((k*ny + j)*nx + i), bands band-major.
+// Stencil kernels walk z inside a thread (a "2.5D" march): each thread keeps psi(k-1),
+// psi(k), psi(k+1) of its (i,j) column in registers, the x/y neighbours come through L1
+// from the lines its warp and block neighbours load, so DRAM sees each value once.
+// Every operator whose reference result is deterministic (H psi, Jacobi, density, the
+// nuclear potential, mixing) uses round-to-nearest intrinsics in the reference's operation
+// order (no FMA contraction), which makes it bit-identical to the reference.
+#include <algorithm>
+#include <cmath>
+
+#include "ops.h"
+#include "xc_device.cuh"
+
+namespace dftb {
+
+// =============================================================== reductions ==========
+namespace {
+
+constexpr int RED_THREADS = 256;
+
+inline int red_blocks(dft_context* ctx, long long n) {
+    long long b = (n + RED_THREADS - 1) / RED_THREADS;
+    long long cap = (long long)ctx->num_sms * 4;
+    return (int)std::max<long long>(1, std::min(b, cap));
+}
+
+// K independent sums over p in [0,n): partial[k*gridDim + block]
+template <int K, class F>
+__global__ void __launch_bounds__(RED_THREADS) reduce_partial_kernel(long long n, F f, double* partial) {
+    __shared__ double sh[RED_THREADS / 32];
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        f(p, acc);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = block_sum(acc[k], sh);
+        if (threadIdx.x == 0) partial[k * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+template <int K>
+__global__ void reduce_final_kernel(int nblocks, const double* partial, double* out) {
+    __shared__ double sh[32];
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partial[k * nblocks + b];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) out[k] = s;
+    }
+}
+
+}  // namespace
+
+// Runs a K-output reduction and returns the sums on the host (synchronises).
+template <int K, class F>
+static void reduce_to_host(dft_context* ctx, long long n, F f, double* out_host) {
+    const int nb = red_blocks(ctx, n);
+    double* partial = (double*)ws_get(ctx, WS_REDUCE, sizeof(double) * ((size_t)K * nb + K));
+    double* res = partial + (size_t)K * nb;
+    reduce_partial_kernel<K><<<nb, RED_THREADS, 0, ctx->stream>>>(n, f, partial);
+    DFT_LAUNCH_CHECK();
+    reduce_final_kernel<K><<<1, 256, 0, ctx->stream>>>(nb, partial, res);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx, 2);
+    double* h = pinned(ctx, K);
+    DFT_CUDA(cudaMemcpyAsync(h, res, sizeof(double) * K, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    for (int k = 0; k < K; ++k) out_host[k] = h[k];
+}
+
+struct DotF {
+    const double *a, *b;
+    __device__ void operator()(long long p, double* acc) const { acc[0] += a[p] * b[p]; }
+};
+struct Dot3F {
+    const double *a, *b;
+    double c;
+    __device__ void operator()(long long p, double* acc) const { acc[0] += __dmul_rn(__dmul_rn(a[p], b[p]), c); }
+};
+struct DiffF {
+    const double *o, *n;
+    __device__ void operator()(long long p, double* acc) const {
+        const double d = n[p] - o[p];
+        acc[0] += d * d;
+        acc[1] += n[p] * n[p];
+    }
+};
+
+double dot(dft_context* ctx, long long n, const double* a, const double* b) {
+    double r;
+    reduce_to_host<1>(ctx, n, DotF{a, b}, &r);
+    return r;
+}
+
+double dot3(dft_context* ctx, long long n, const double* a, const double* b, double c) {
+    double r;
+    reduce_to_host<1>(ctx, n, Dot3F{a, b, c}, &r);
+    return r;
+}
+
+// calculateMolecularDensityDifference, reference MolecularSCFHelpers.cpp:46-95
+double density_difference(dft_context* ctx, const Grid& g, const double* old_d, const double* new_d) {
+    double s[2];
+    reduce_to_host<2>(ctx, g.N, DiffF{old_d, new_d}, s);
+    const double dn = std::sqrt(s[0] * g.dV), nn = std::sqrt(s[1] * g.dV);
+    if (nn <= 1.0e-14) return dn;
+    return dn / nn;
+}
+
+// =============================================================== elementwise =========
+namespace {
+__global__ void add2_kernel(long long n, const double* a, const double* b, double* o) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        o[p] = __dadd_rn(a[p], b[p]);
+}
+__global__ void add3_kernel(long long n, const double* a, const double* b, const double* c, double* o) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        o[p] = __dadd_rn(__dadd_rn(a[p], b[p]), c[p]);
+}
+__global__ void mix_kernel(long long n, double* d, const double* o, double m) {
+    const double om = 1.0 - m;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        d[p] = __dadd_rn(__dmul_rn(om, d[p]), __dmul_rn(m, o[p]));
+}
+inline int ew_blocks(dft_context* ctx, long long n) {
+    long long b = (n + 255) / 256;
+    return (int)std::max<long long>(1, std::min<long long>(b, (long long)ctx->num_sms * 8));
+}
+}  // namespace
+
+void add2(dft_context* ctx, long long n, const double* a, const double* b, double* out) {
+    add2_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, a, b, out);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+void add3(dft_context* ctx, long long n, const double* a, const double* b, const double* c, double* out) {
+    add3_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, a, b, c, out);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+void mix(dft_context* ctx, long long n, double* d, const double* o, double m) {
+    mix_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, d, o, m);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
+// =============================================================== H psi ===============
+namespace {
+
+constexpr int HB_X = 32, HB_Y = 8;
+
+// One thread per (i,j) column of one band, marching k over a z-chunk.
+// reference KohnShamHamiltonianMolecule.cpp:59-177: lap = k0*c (+ neighbours in the order
+// x-, x+, y-, y+, z-, z+), H psi = -0.5*lap + V*c; absent neighbours are skipped.
+__global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* __restrict__ V,
+                                                         const double* __restrict__ psi, double* __restrict__ out,
+                                                         long long ld, int zchunk, int nzc, double k0) {
+    const int i = blockIdx.x * HB_X + threadIdx.x;
+    const int j = blockIdx.y * HB_Y + threadIdx.y;
+    const int band = blockIdx.z / nzc;
+    const int kc = blockIdx.z - band * nzc;
+    if (i >= g.nx || j >= g.ny) return;
+    const double* __restrict__ p = psi + (long long)band * ld;
+    double* __restrict__ o = out + (long long)band * ld;
+    const long long sxy = (long long)g.nx * g.ny;
+    const int kb = kc * zchunk;
+    const int ke = min(g.nz, kb + zchunk);
+    long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
+    double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
+    double cur = __ldg(p + idx);
+    const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+    for (int k = kb; k < ke; ++k, idx += sxy) {
+        const bool zr = k + 1 < g.nz;
+        const double above = zr ? __ldg(p + idx + sxy) : 0.0;
+        double lap = __dmul_rn(k0, cur);
+        if (xl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - 1), g.ix2));
+        if (xr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + 1), g.ix2));
+        if (yl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - g.nx), g.iy2));
+        if (yr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + g.nx), g.iy2));
+        if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below, g.iz2));
+        if (zr) lap = __dadd_rn(lap, __dmul_rn(above, g.iz2));
+        o[idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(__ldg(V + idx), cur));
+        below = cur;
+        cur = above;
+    }
+}
+
+inline int pick_zchunk(const Grid& g, long long columns_blocks, int nbands, int num_sms) {
+    // enough CTAs to fill the machine a few times over, but chunks long enough to amortise
+    // the two-plane warm-up of the z march
+    int zc = 32;
+    while (zc > 4 && columns_blocks * nbands * ((g.nz + zc - 1) / zc) < 4LL * num_sms) zc >>= 1;
+    return zc;
+}
+
+}  // namespace
+
+void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const double* psi, double* hpsi, int nbands,
+                       long long ld) {
+    if (nbands <= 0) return;
+    const double k0 = -2.0 * (g.ix2 + g.iy2 + g.iz2);
+    dim3 block(HB_X, HB_Y);
+    const int bx = (g.nx + HB_X - 1) / HB_X, by = (g.ny + HB_Y - 1) / HB_Y;
+    const int zc = pick_zchunk(g, (long long)bx * by, nbands, ctx->num_sms);
+    const int nzc = (g.nz + zc - 1) / zc;
+    // gridDim.z limit is 65535: split the band block if needed
+    const int max_bands = std::max(1, 65535 / nzc);
+    for (int b0 = 0; b0 < nbands; b0 += max_bands) {
+        const int nb = std::min(max_bands, nbands - b0);
+        dim3 grid(bx, by, nb * nzc);
+        hpsi_kernel<<<grid, block, 0, ctx->stream>>>(g, V, psi + (long long)b0 * ld, hpsi + (long long)b0 * ld, ld, zc,
+                                                     nzc, k0);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+    }
+}
+
+// =============================================================== Jacobi Poisson ======
+namespace {
+
+struct JacobiCtrl {
+    unsigned long long diff_bits;  // running max |dV| of the sweep in flight (as uint64 of a non-negative double)
+    unsigned int ticket;           // blocks finished in the sweep in flight
+    int done;                      // 1 once the stop rule fired or the cap was reached
+    long long sweep;               // completed sweeps; the current iterate lives in buf[sweep & 1]
+    double last_diff;              // max |dV| of the last completed sweep
+};
+
+// Boundary fill, reference HartreePotentialMolecule.cpp:37-95 and :171-202.  Interior = 0.
+// x_i = xmin + i*dx exactly as CartesianGrid::getX; Q is the total charge.
+__global__ void jacobi_init_kernel(Grid g, double Q, double* a, double* b) {
+    const long long n = g.N;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx);
+        const int j = (int)((p / g.nx) % g.ny);
+        const int k = (int)(p / ((long long)g.nx * g.ny));
+        double v = 0.0;
+        if (i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz) {
+            const double x = __dadd_rn(g.xmin, __dmul_rn((double)i, g.dx));
+            const double y = __dadd_rn(g.ymin, __dmul_rn((double)j, g.dy));
+            const double z = __dadd_rn(g.zmin, __dmul_rn((double)k, g.dz));
+            const double d[6] = {fabs(x - g.xmin), fabs(x - g.xmax), fabs(y - g.ymin),
+                                 fabs(y - g.ymax), fabs(z - g.zmin), fabs(z - g.zmax)};
+            double m2 = INFINITY;
+            for (int q = 0; q < 6; ++q) m2 = fmin(m2, __dmul_rn(d[q], d[q]));
+            if (m2 > 0.0) {
+                const double r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+                if (r > 0.0) v = Q / r;
+            }
+        }
+        a[p] = v;
+        b[p] = v;
+    }
+}
+
+// Sequential total charge (the reference's summation order), used only when a boundary
+// face is not exactly on a node so boundary values are non-zero.
+__global__ void total_charge_seq_kernel(long long n, const double* rho, double dV, double* out) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double s = 0.0;
+        for (long long p = 0; p < n; ++p) s += rho[p];
+        *out = s * dV;
+    }
+}
+
+constexpr int JB_X = 32, JB_Y = 8;
+
+// One Jacobi sweep over the interior (reference HartreePotentialMolecule.cpp:207-321):
+// V' = (ix2 (V[x-]+V[x+]) + iy2 (V[y-]+V[y+]) + iz2 (V[z-]+V[z+]) + 4 pi rho) / den,
+// max |V'-V| folded into ctrl; the last block to finish closes the sweep.
+__global__ void __launch_bounds__(JB_X* JB_Y) jacobi_sweep_kernel(Grid g, const double* __restrict__ rho,
+                                                                  double* buf0, double* buf1, JacobiCtrl* ctrl,
+                                                                  double den, double tol, long long cap,
+                                                                  int zchunk) {
+    __shared__ double sh[JB_X * JB_Y / 32];
+    __shared__ int s_done;
+    __shared__ long long s_sweep;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        s_done = __ldcg(&ctrl->done);
+        s_sweep = __ldcg(&ctrl->sweep);
+    }
+    __syncthreads();
+    if (s_done) return;
+    const double* __restrict__ cur = (s_sweep & 1) ? buf1 : buf0;
+    double* __restrict__ nxt = (s_sweep & 1) ? buf0 : buf1;
+    const double c4pi = 4.0 * xcf::PI;
+    const int i = blockIdx.x * JB_X + threadIdx.x;
+    const int j = blockIdx.y * JB_Y + threadIdx.y;
+    double md = 0.0;
+    if (i >= 1 && i + 1 < g.nx && j >= 1 && j + 1 < g.ny) {
+        const long long sxy = (long long)g.nx * g.ny;
+        const int kb = max(1, (int)blockIdx.z * zchunk);
+        const int ke = min(g.nz - 1, (int)(blockIdx.z + 1) * zchunk);
+        if (kb < ke) {
+            long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
+            double below = cur[idx - sxy];
+            double c = cur[idx];
+            for (int k = kb; k < ke; ++k, idx += sxy) {
+                const double above = cur[idx + sxy];
+                const double sx = __dadd_rn(cur[idx - 1], cur[idx + 1]);
+                const double sy = __dadd_rn(cur[idx - g.nx], cur[idx + g.nx]);
+                const double sz = __dadd_rn(below, above);
+                double acc = __dadd_rn(__dmul_rn(g.ix2, sx), __dmul_rn(g.iy2, sy));
+                acc = __dadd_rn(acc, __dmul_rn(g.iz2, sz));
+                acc = __dadd_rn(acc, __dmul_rn(c4pi, __ldg(rho + idx)));
+                const double v = __ddiv_rn(acc, den);
+                nxt[idx] = v;
+                md = fmax(md, fabs(v - c));
+                below = c;
+                c = above;
+            }
+        }
+    }
+    // block max -> global max (non-negative doubles order like their bit patterns)
+    const int tid = threadIdx.y * JB_X + threadIdx.x;
+    md = warp_max(md);
+    if ((tid & 31) == 0) sh[tid >> 5] = md;
+    __syncthreads();
+    if (tid == 0) {
+        double m = sh[0];
+        for (int w = 1; w < JB_X * JB_Y / 32; ++w) m = fmax(m, sh[w]);
+        atomicMax(&ctrl->diff_bits, (unsigned long long)__double_as_longlong(m));
+        __threadfence();
+        const unsigned int total = gridDim.x * gridDim.y * gridDim.z;
+        const unsigned int t = atomicAdd(&ctrl->ticket, 1u);
+        if (t == total - 1) {
+            __threadfence();
+            const double d = __longlong_as_double((long long)atomicExch(&ctrl->diff_bits, 0ull));
+            ctrl->ticket = 0;
+            ctrl->last_diff = d;
+            ctrl->sweep = s_sweep + 1;
+            if (d < tol || s_sweep + 1 >= cap) ctrl->done = 1;
+            __threadfence();
+        }
+    }
+}
+
+}  // namespace
+
+JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol, long max_sweeps) {
+    if (max_sweeps < 0) fail(DFT_INVALID_ARGUMENT, "max_sweeps must be >= 0");
+    double* buf1 = (double*)ws_get(ctx, WS_JACOBI, sizeof(double) * (size_t)g.N);
+    JacobiCtrl* ctrl = (JacobiCtrl*)ws_get(ctx, WS_CTRL, sizeof(JacobiCtrl) + 64);
+    // Boundary values are Q/|r| only on faces whose last node misses the bound by rounding
+    // (reference :60-79); on every grid whose x_{n-1} == xmax they are all zero and Q is unused.
+    const bool exact_faces = (g.xmin + (double)(g.nx - 1) * g.dx == g.xmax) &&
+                             (g.ymin + (double)(g.ny - 1) * g.dy == g.ymax) &&
+                             (g.zmin + (double)(g.nz - 1) * g.dz == g.zmax);
+    double Q = 0.0;
+    if (!exact_faces) {
+        double* q = (double*)ws_get(ctx, WS_TMP2, sizeof(double));
+        total_charge_seq_kernel<<<1, 32, 0, ctx->stream>>>(g.N, rho, g.dV, q);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+        double* h = pinned(ctx, 1);
+        DFT_CUDA(cudaMemcpyAsync(h, q, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        sync(ctx);
+        Q = h[0];
+    }
+    jacobi_init_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, Q, vh, buf1);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+    DFT_CUDA(cudaMemsetAsync(ctrl, 0, sizeof(JacobiCtrl), ctx->stream));
+    if (max_sweeps == 0 || g.nx < 3 || g.ny < 3 || g.nz < 3) {
+        // no interior: the reference still runs its sweep loop, finds max|dV| = 0 < tol and stops
+        return {max_sweeps == 0 ? 0L : 1L, 0.0};
+    }
+    const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
+    dim3 block(JB_X, JB_Y);
+    const int bx = (g.nx + JB_X - 1) / JB_X, by = (g.ny + JB_Y - 1) / JB_Y;
+    int zc = 32;
+    while (zc > 4 && (long long)bx * by * ((g.nz + zc - 1) / zc) < 2LL * ctx->num_sms) zc >>= 1;
+    dim3 grid(bx, by, (g.nz + zc - 1) / zc);
+    JacobiCtrl* hc = (JacobiCtrl*)pinned(ctx, (sizeof(JacobiCtrl) + 7) / 8);
+    long launched = 0;
+    // Sweeps are launched in batches; a launch after the stop rule fired returns at once, so
+    // a batch may overrun the stopping sweep without changing the result.
+    long batch = 32;
+    while (true) {
+        const long nb = std::min<long>(batch, max_sweeps - launched);
+        for (long s = 0; s < nb; ++s) {
+            jacobi_sweep_kernel<<<grid, block, 0, ctx->stream>>>(g, rho, vh, buf1, ctrl, den, tol, max_sweeps, zc);
+        }
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx, nb);
+        launched += nb;
+        DFT_CUDA(cudaMemcpyAsync(hc, ctrl, sizeof(JacobiCtrl), cudaMemcpyDeviceToHost, ctx->stream));
+        sync(ctx);
+        if (hc->done || launched >= max_sweeps) break;
+        batch = std::min<long>(batch * 2, 512);
+    }
+    const long sweeps = (long)hc->sweep;
+    if (sweeps & 1) {
+        DFT_CUDA(cudaMemcpyAsync(vh, buf1, sizeof(double) * (size_t)g.N, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return {sweeps, hc->last_diff};
+}
+
+// =============================================================== XC ==================
+namespace {
+
+// calculateCartesianDerivative, reference ExchangeCorrelationMolecule.cpp:11-170
+__device__ __forceinline__ double dderiv(const Grid& g, const double* __restrict__ f, long long p, int i, int j, int k,
+                                         int dir) {
+    if (dir == 0) {
+        if (i == 0) return (f[p + 1] - f[p]) / g.dx;
+        if (i == g.nx - 1) return (f[p] - f[p - 1]) / g.dx;
+        return (f[p + 1] - f[p - 1]) / (2.0 * g.dx);
+    }
+    if (dir == 1) {
+        const long long s = g.nx;
+        if (j == 0) return (f[p + s] - f[p]) / g.dy;
+        if (j == g.ny - 1) return (f[p] - f[p - s]) / g.dy;
+        return (f[p + s] - f[p - s]) / (2.0 * g.dy);
+    }
+    const long long s = (long long)g.nx * g.ny;
+    if (k == 0) return (f[p + s] - f[p]) / g.dz;
+    if (k == g.nz - 1) return (f[p] - f[p - s]) / g.dz;
+    return (f[p + s] - f[p - s]) / (2.0 * g.dz);
+}
+
+__device__ __forceinline__ double gradmag(const Grid& g, const double* __restrict__ f, long long p, int i, int j, int k) {
+    const double gx = dderiv(g, f, p, i, j, k, 0), gy = dderiv(g, f, p, i, j, k, 1), gz = dderiv(g, f, p, i, j, k, 2);
+    return sqrt(gx * gx + gy * gy + gz * gz);
+}
+
+// Pass 1: functional at every point above the floor.  Writes d f/d n_sigma and the gradient
+// coefficients c_sigma (zero below the floor, reference :626-706) and per-block partial sums
+// of n eps dV (reference :749-842).  One evaluation serves both spins and the energy.
+template <int KIND, bool POT, bool ENERGY>
+__global__ void __launch_bounds__(256) xc_point_kernel(Grid g, const double* __restrict__ na,
+                                                       const double* __restrict__ nb, double* __restrict__ da,
+                                                       double* __restrict__ db, double* __restrict__ ca,
+                                                       double* __restrict__ cb, double* __restrict__ partial) {
+    __shared__ double sh[8];
+    double e = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const double a = na[p], b = nb[p];
+        const double n = a + b;
+        double rda = 0.0, rdb = 0.0, rca = 0.0, rcb = 0.0;
+        if (n > xcf::RHO_FLOOR) {
+            const int i = (int)(p % g.nx);
+            const int j = (int)((p / g.nx) % g.ny);
+            const int k = (int)(p / ((long long)g.nx * g.ny));
+            double ga = 0.0, gb = 0.0;
+            if (KIND == 1) {
+                ga = gradmag(g, na, p, i, j, k);
+                gb = gradmag(g, nb, p, i, j, k);
+            }
+            const xcf::Result r = xcf::evaluate<KIND>(a, b, ga, gb);
+            rda = r.va;
+            rdb = r.vb;
+            rca = r.ca;
+            rcb = r.cb;
+            if (ENERGY) e += n * r.eps * g.dV;
+        }
+        if (POT) {
+            da[p] = rda;
+            db[p] = rdb;
+            if (KIND == 1) {
+                ca[p] = rca;
+                cb[p] = rcb;
+            }
+        }
+    }
+    if (ENERGY) {
+        e = block_sum(e, sh);
+        if (threadIdx.x == 0) partial[blockIdx.x] = e;
+    }
+}
+
+// div(c grad f) at (i,j,k), reference calculateCartesianDivergence :216-572
+__device__ __forceinline__ double ddiv(const Grid& g, const double* __restrict__ c, const double* __restrict__ f,
+                                       long long p, int i, int j, int k) {
+    const double cc = c[p];
+    double dx, dy, dz;
+    {
+        const double fc = cc * dderiv(g, f, p, i, j, k, 0);
+        if (i == 0) dx = (c[p + 1] * dderiv(g, f, p + 1, i + 1, j, k, 0) - fc) / g.dx;
+        else if (i == g.nx - 1) dx = (fc - c[p - 1] * dderiv(g, f, p - 1, i - 1, j, k, 0)) / g.dx;
+        else
+            dx = (c[p + 1] * dderiv(g, f, p + 1, i + 1, j, k, 0) - c[p - 1] * dderiv(g, f, p - 1, i - 1, j, k, 0)) /
+                 (2.0 * g.dx);
+    }
+    {
+        const long long s = g.nx;
+        const double fc = cc * dderiv(g, f, p, i, j, k, 1);
+        if (j == 0) dy = (c[p + s] * dderiv(g, f, p + s, i, j + 1, k, 1) - fc) / g.dy;
+        else if (j == g.ny - 1) dy = (fc - c[p - s] * dderiv(g, f, p - s, i, j - 1, k, 1)) / g.dy;
+        else
+            dy = (c[p + s] * dderiv(g, f, p + s, i, j + 1, k, 1) - c[p - s] * dderiv(g, f, p - s, i, j - 1, k, 1)) /
+                 (2.0 * g.dy);
+    }
+    {
+        const long long s = (long long)g.nx * g.ny;
+        const double fc = cc * dderiv(g, f, p, i, j, k, 2);
+        if (k == 0) dz = (c[p + s] * dderiv(g, f, p + s, i, j, k + 1, 2) - fc) / g.dz;
+        else if (k == g.nz - 1) dz = (fc - c[p - s] * dderiv(g, f, p - s, i, j, k - 1, 2)) / g.dz;
+        else
+            dz = (c[p + s] * dderiv(g, f, p + s, i, j, k + 1, 2) - c[p - s] * dderiv(g, f, p - s, i, j, k - 1, 2)) /
+                 (2.0 * g.dz);
+    }
+    return dx + dy + dz;
+}
+
+// Pass 2 (GGA only): v_sigma = d_sigma - div(c_sigma grad n_sigma) above the floor, else 0.
+__global__ void __launch_bounds__(256) xc_div_kernel(Grid g, const double* __restrict__ na,
+                                                     const double* __restrict__ nb, const double* __restrict__ da,
+                                                     const double* __restrict__ db, const double* __restrict__ ca,
+                                                     const double* __restrict__ cb, double* __restrict__ va,
+                                                     double* __restrict__ vb) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const double n = na[p] + nb[p];
+        double ra = 0.0, rb = 0.0;
+        if (n > xcf::RHO_FLOOR) {
+            const int i = (int)(p % g.nx);
+            const int j = (int)((p / g.nx) % g.ny);
+            const int k = (int)(p / ((long long)g.nx * g.ny));
+            if (va) ra = da[p] - ddiv(g, ca, na, p, i, j, k);
+            if (vb) rb = db[p] - ddiv(g, cb, nb, p, i, j, k);
+        }
+        if (va) va[p] = ra;
+        if (vb) vb[p] = rb;
+    }
+}
+
+// LDA potential: the divergence term vanishes identically (c = 0), v = d above the floor.
+__global__ void xc_lda_copy_kernel(long long n, const double* __restrict__ na, const double* __restrict__ nb,
+                                   const double* __restrict__ da, const double* __restrict__ db, double* va,
+                                   double* vb) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const bool on = na[p] + nb[p] > xcf::RHO_FLOOR;
+        if (va) va[p] = on ? da[p] : 0.0;
+        if (vb) vb[p] = on ? db[p] : 0.0;
+    }
+}
+
+template <int KIND>
+__global__ void xc_eval_kernel(long long m, const double* na, const double* nb, const double* ga, const double* gb,
+                               double* out5) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < m; p += (long long)gridDim.x * blockDim.x) {
+        const xcf::Result r = xcf::evaluate<KIND>(na[p], nb[p], ga[p], gb[p]);
+        out5[5 * p + 0] = r.eps;
+        out5[5 * p + 1] = r.va;
+        out5[5 * p + 2] = r.vb;
+        out5[5 * p + 3] = r.ca;
+        out5[5 * p + 4] = r.cb;
+    }
+}
+
+template <int KIND>
+double xc_impl(dft_context* ctx, const Grid& g, const double* na, const double* nb, double* va, double* vb,
+               bool want_energy) {
+    const bool pot = va || vb;
+    const size_t N = (size_t)g.N;
+    double* tmp = pot ? (double*)ws_get(ctx, WS_XC, sizeof(double) * 4 * N) : nullptr;
+    double *da = tmp, *db = tmp ? tmp + N : nullptr, *ca = tmp ? tmp + 2 * N : nullptr, *cb = tmp ? tmp + 3 * N : nullptr;
+    const int nbk = std::max(1, std::min((int)((g.N + 255) / 256), ctx->num_sms * 8));
+    double* partial = (double*)ws_get(ctx, WS_REDUCE, sizeof(double) * ((size_t)nbk + 8));
+    if (pot && want_energy)
+        xc_point_kernel<KIND, true, true><<<nbk, 256, 0, ctx->stream>>>(g, na, nb, da, db, ca, cb, partial);
+    else if (pot)
+        xc_point_kernel<KIND, true, false><<<nbk, 256, 0, ctx->stream>>>(g, na, nb, da, db, ca, cb, partial);
+    else
+        xc_point_kernel<KIND, false, true><<<nbk, 256, 0, ctx->stream>>>(g, na, nb, da, db, ca, cb, partial);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+    if (pot) {
+        if (KIND == 1)
+            xc_div_kernel<<<nbk, 256, 0, ctx->stream>>>(g, na, nb, da, db, ca, cb, va, vb);
+        else
+            xc_lda_copy_kernel<<<nbk, 256, 0, ctx->stream>>>(g.N, na, nb, da, db, va, vb);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+    }
+    if (!want_energy) return 0.0;
+    double* res = partial + nbk;
+    reduce_final_kernel<1><<<1, 256, 0, ctx->stream>>>(nbk, partial, res);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+    double* h = pinned(ctx, 1);
+    DFT_CUDA(cudaMemcpyAsync(h, res, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    return h[0];
+}
+
+}  // namespace
+
+double xc(dft_context* ctx, const Grid& g, int kind, const double* na, const double* nb, double* va, double* vb,
+          bool want_energy) {
+    if (kind == DFT_XC_PBE96) return xc_impl<1>(ctx, g, na, nb, va, vb, want_energy);
+    if (kind == DFT_XC_PZ81) return xc_impl<0>(ctx, g, na, nb, va, vb, want_energy);
+    fail(DFT_INVALID_ARGUMENT, "unknown functional kind %d", kind);
+}
+
+void xc_evaluate(dft_context* ctx, int kind, long long m, const double* na, const double* nb, const double* ga,
+                 const double* gb, double* out5) {
+    if (m <= 0) return;
+    const int nbk = std::max(1, std::min((int)((m + 255) / 256), ctx->num_sms * 8));
+    if (kind == DFT_XC_PBE96) xc_eval_kernel<1><<<nbk, 256, 0, ctx->stream>>>(m, na, nb, ga, gb, out5);
+    else if (kind == DFT_XC_PZ81) xc_eval_kernel<0><<<nbk, 256, 0, ctx->stream>>>(m, na, nb, ga, gb, out5);
+    else fail(DFT_INVALID_ARGUMENT, "unknown functional kind %d", kind);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
+// =============================================================== density / energies ==
+namespace {
+
+constexpr int MAX_OCC_BANDS = 1024;
+struct OccTable {
+    double w[MAX_OCC_BANDS];
+};
+
+// reference ElectronDensityMolecule.cpp:58-71: density += electrons * psi * psi, band order
+__global__ void density_kernel(long long n, const double* __restrict__ psi, int nbands, long long ld, OccTable occ,
+                               double* __restrict__ out) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int b = 0; b < nbands; ++b) {
+            const double w = occ.w[b];
+            if (w <= 0.0) continue;
+            const double v = psi[(long long)b * ld + p];
+            d = __dadd_rn(d, __dmul_rn(__dmul_rn(w, v), v));
+        }
+        out[p] = d;
+    }
+}
+
+// Kinetic energy density with the reference's face stencil (TotalEnergyMolecule.cpp:80-177):
+// lap = sum over existing neighbours (psi_nb - psi)/h^2, term = psi * (-0.5 lap) * dV.
+// One block row of partials per band.
+__global__ void __launch_bounds__(256) kinetic_kernel(Grid g, const double* __restrict__ psi, long long ld,
+                                                      double* partial) {
+    __shared__ double sh[8];
+    const int band = blockIdx.y;
+    const double* __restrict__ f = psi + (long long)band * ld;
+    const double hx = g.dx * g.dx, hy = g.dy * g.dy, hz = g.dz * g.dz;
+    const long long sxy = (long long)g.nx * g.ny;
+    double e = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx);
+        const int j = (int)((p / g.nx) % g.ny);
+        const int k = (int)(p / sxy);
+        const double c = f[p];
+        double lap = 0.0;
+        if (i > 0) lap += (f[p - 1] - c) / hx;
+        if (i + 1 < g.nx) lap += (f[p + 1] - c) / hx;
+        if (j > 0) lap += (f[p - g.nx] - c) / hy;
+        if (j + 1 < g.ny) lap += (f[p + g.nx] - c) / hy;
+        if (k > 0) lap += (f[p - sxy] - c) / hz;
+        if (k + 1 < g.nz) lap += (f[p + sxy] - c) / hz;
+        e += c * (-0.5 * lap) * g.dV;
+    }
+    e = block_sum(e, sh);
+    if (threadIdx.x == 0) partial[(long long)band * gridDim.x + blockIdx.x] = e;
+}
+
+__global__ void rows_sum_kernel(int nrows, int ncols, const double* partial, double* out) {
+    __shared__ double sh[32];
+    for (int r = 0; r < nrows; ++r) {
+        double s = 0.0;
+        for (int c = threadIdx.x; c < ncols; c += blockDim.x) s += partial[(long long)r * ncols + c];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) out[r] = s;
+    }
+}
+
+// NuclearPotential::calculateAtPoint, reference NuclearPotential.cpp:36-76
+__global__ void nuclear_kernel(Grid g, int nnuc, const double* __restrict__ nuc, double* __restrict__ v,
+                               int* singular) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx);
+        const int j = (int)((p / g.nx) % g.ny);
+        const int k = (int)(p / ((long long)g.nx * g.ny));
+        const double x = __dadd_rn(g.xmin, __dmul_rn((double)i, g.dx));
+        const double y = __dadd_rn(g.ymin, __dmul_rn((double)j, g.dy));
+        const double z = __dadd_rn(g.zmin, __dmul_rn((double)k, g.dz));
+        double s = 0.0;
+        for (int a = 0; a < nnuc; ++a) {
+            const double ddx = x - nuc[4 * a + 1], ddy = y - nuc[4 * a + 2], ddz = z - nuc[4 * a + 3];
+            const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
+            if (d2 == 0.0) {
+                atomicExch(singular, 1);
+                continue;
+            }
+            s = __dsub_rn(s, __ddiv_rn(nuc[4 * a], sqrt(d2)));
+        }
+        v[p] = s;
+    }
+}
+
+}  // namespace
+
+void spin_density(dft_context* ctx, long long n, const double* psi, int nbands, long long ld, const double* occ_host,
+                  double* out) {
+    if (nbands > MAX_OCC_BANDS) fail(DFT_INVALID_ARGUMENT, "at most %d bands", MAX_OCC_BANDS);
+    OccTable t;
+    for (int b = 0; b < nbands; ++b) t.w[b] = occ_host[b];
+    density_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, psi, nbands, ld, t, out);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
+void kinetic_per_band(dft_context* ctx, const Grid& g, const double* psi, int nbands, long long ld, double* out_host) {
+    if (nbands <= 0) return;
+    if (nbands > 65535) fail(DFT_INVALID_ARGUMENT, "too many bands");
+    const int nbk = std::max(1, std::min((int)((g.N + 255) / 256), ctx->num_sms * 2));
+    double* partial = (double*)ws_get(ctx, WS_REDUCE, sizeof(double) * ((size_t)nbk * nbands + nbands));
+    double* res = partial + (size_t)nbk * nbands;
+    kinetic_kernel<<<dim3(nbk, nbands), 256, 0, ctx->stream>>>(g, psi, ld, partial);
+    DFT_LAUNCH_CHECK();
+    rows_sum_kernel<<<1, 256, 0, ctx->stream>>>(nbands, nbk, partial, res);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx, 2);
+    double* h = pinned(ctx, nbands);
+    DFT_CUDA(cudaMemcpyAsync(h, res, sizeof(double) * nbands, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    for (int b = 0; b < nbands; ++b) out_host[b] = h[b];
+}
+
+double kinetic_energy(dft_context* ctx, const Grid& g, const double* psi, int nbands, long long ld,
+                      const double* occ_host) {
+    std::vector<double> e(std::max(nbands, 1));
+    kinetic_per_band(ctx, g, psi, nbands, ld, e.data());
+    // energy += electrons * orbitalEnergy, in band order (reference TotalEnergyMolecule.cpp:181-195)
+    double s = 0.0;
+    for (int b = 0; b < nbands; ++b)
+        if (occ_host[b] > 0.0) s += occ_host[b] * e[b];
+    return s;
+}
+
+void nuclear_potential(dft_context* ctx, const Grid& g, int nnuc, const int* Z, const double* xyz, double* vext) {
+    if (nnuc <= 0) fail(DFT_INVALID_ARGUMENT, "La molecula debe contener al menos un nucleo.");
+    std::vector<double> nuc(4 * (size_t)nnuc);
+    for (int a = 0; a < nnuc; ++a) {
+        if (Z[a] <= 0) fail(DFT_INVALID_ARGUMENT, "Atomic number must be greater than zero.");
+        nuc[4 * a] = (double)Z[a];
+        nuc[4 * a + 1] = xyz[3 * a];
+        nuc[4 * a + 2] = xyz[3 * a + 1];
+        nuc[4 * a + 3] = xyz[3 * a + 2];
+    }
+    double* dn = (double*)ws_get(ctx, WS_TMP2, sizeof(double) * nuc.size() + 64);
+    int* flag = (int*)(dn + nuc.size());
+    DFT_CUDA(cudaMemcpyAsync(dn, nuc.data(), sizeof(double) * nuc.size(), cudaMemcpyHostToDevice, ctx->stream));
+    DFT_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
+    nuclear_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, nnuc, dn, vext, flag);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+    int* h = (int*)pinned(ctx, 1);
+    DFT_CUDA(cudaMemcpyAsync(h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    if (*h) fail(DFT_SINGULAR, "NuclearPotential is singular at a nuclear position.");
+}
+
+}  // namespace dftb

@@ -1,0 +1,70 @@
+// Internal (C++) interface of the dft_b200 device operators.  The extern "C" layer in
+// capi.cu validates arguments, catches dftb::Error and forwards here.  All pointers are
+// device pointers; every function is stream-ordered on ctx->stream unless it returns a
+// host scalar, in which case it synchronises.
+#pragma once
+
+#include "common.cuh"
+
+namespace dftb {
+
+// H psi over a band block (bit-identical to the reference per band).
+void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const double* psi, double* hpsi, int nbands,
+                       long long ld);
+
+// Jacobi Poisson with the reference's stopping rule.  Returns the sweep count.
+struct JacobiResult {
+    long sweeps;
+    double last_diff;
+};
+JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol, long max_sweeps);
+
+// rho = a + b
+void add2(dft_context* ctx, long long n, const double* a, const double* b, double* out);
+// out = (a + b) + c
+void add3(dft_context* ctx, long long n, const double* a, const double* b, const double* c, double* out);
+// d = (1-m) d + m o   (mixDensity, MolecularSCFHelpers.cpp:27-44)
+void mix(dft_context* ctx, long long n, double* d, const double* o, double m);
+
+// sum_p a[p]*b[p] (optionally * w[p]); deterministic block order
+double dot(dft_context* ctx, long long n, const double* a, const double* b);
+// sum_p a[p]*b[p]*c[p] evaluated as (a*b)*c per term
+double dot3(dft_context* ctx, long long n, const double* a, const double* b, double c);
+
+// relative L2 density difference (calculateMolecularDensityDifference)
+double density_difference(dft_context* ctx, const Grid& g, const double* old_d, const double* new_d);
+
+// XC potential (both spins) and/or energy.  va/vb may be null.  Returns E_xc if want_energy.
+double xc(dft_context* ctx, const Grid& g, int kind, const double* na, const double* nb, double* va, double* vb,
+          bool want_energy);
+void xc_evaluate(dft_context* ctx, int kind, long long m, const double* na, const double* nb, const double* ga,
+                 const double* gb, double* out5);
+
+// density from a band block with host weights
+void spin_density(dft_context* ctx, long long n, const double* psi, int nbands, long long ld, const double* occ_host,
+                  double* out);
+double kinetic_energy(dft_context* ctx, const Grid& g, const double* psi, int nbands, long long ld,
+                      const double* occ_host);
+// per-band <psi_b| -1/2 lap |psi_b> dV (face stencil), into out_host[nbands]
+void kinetic_per_band(dft_context* ctx, const Grid& g, const double* psi, int nbands, long long ld, double* out_host);
+void nuclear_potential(dft_context* ctx, const Grid& g, int nnuc, const int* Z, const double* xyz, double* vext);
+
+// Block Davidson eigensolver (davidson.cu).
+struct EigOpts {
+    double tol = 1e-7;
+    int max_iterations = 2000;
+    int max_subspace = 3;
+    int verbose = 0;
+};
+int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, int nbands, double* psi,
+                   long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o);
+
+// Molecular SCF (scf.cu).
+void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z, const double* xyz, int charge,
+                  int multiplicity, int kind, const dft_scf_opts* opts, dft_scf_result* res);
+
+// Radial atoms, one persistent launch (radial.cu).
+void solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, long points, double rmax,
+                 dft_atom_result* results);
+
+}  // namespace dftb

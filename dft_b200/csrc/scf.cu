@@ -1,0 +1,228 @@
+// Molecular SCF driver: the reference loop (SelfConsistentFieldMolecule.cpp:50-561 with
+// executeMolecularSCFIteration, MolecularSCFIteration.cpp:12-252) over device-resident
+// fields.  Densities, potentials and orbitals never leave HBM; only scalars (energies,
+// norms, the small projected matrices) come back to the host.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <limits>
+#include <vector>
+
+#include "ops.h"
+
+namespace dftb {
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+inline double ms_since(Clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
+}
+
+struct DevBuf {
+    double* p = nullptr;
+    DevBuf() = default;
+    explicit DevBuf(size_t n) {
+        if (n) DFT_CUDA(cudaMalloc(&p, n * sizeof(double)));
+    }
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+}  // namespace
+
+void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z, const double* xyz, int charge,
+                  int multiplicity, int kind, const dft_scf_opts* opts, dft_scf_result* res) {
+    const auto t_start = Clock::now();
+    const Grid g = make_grid(grid);
+    if (!res) fail(DFT_INVALID_ARGUMENT, "result is NULL");
+    if (kind != DFT_XC_PZ81 && kind != DFT_XC_PBE96) fail(DFT_INVALID_ARGUMENT, "unknown functional kind %d", kind);
+    dft_scf_opts o;
+    if (opts) o = *opts;
+    else dft_scf_default_options(&o);
+    // ---- input checks, reference SelfConsistentFieldMolecule.cpp:58-127 -----------------
+    if (nnuc <= 0) fail(DFT_INVALID_ARGUMENT, "La molecula debe contener al menos un nucleo.");
+    if (multiplicity < 1) fail(DFT_INVALID_ARGUMENT, "La multiplicidad electronica debe ser al menos 1.");
+    int nuclear = 0;
+    for (int a = 0; a < nnuc; ++a) {
+        if (Z[a] <= 0) fail(DFT_INVALID_ARGUMENT, "Atomic number must be greater than zero.");
+        nuclear += Z[a];
+    }
+    const int ne = nuclear - charge;
+    if (ne < 0) fail(DFT_INVALID_ARGUMENT, "La carga molecular produce un numero negativo de electrones.");
+    if (ne == 0) fail(DFT_INVALID_ARGUMENT, "El SCF molecular requiere al menos un electron.");
+    const int sd = multiplicity - 1;
+    if (sd > ne) fail(DFT_INVALID_ARGUMENT, "La multiplicidad electronica es incompatible con el numero de electrones.");
+    if ((ne - sd) % 2 != 0)
+        fail(DFT_INVALID_ARGUMENT, "La multiplicidad electronica es incompatible con la paridad del numero de electrones.");
+    const int na = (ne + sd) / 2, nb = (ne - sd) / 2;
+    const bool closed = multiplicity == 1;
+    // zero beta electrons: the reference's solveMolecularOrbitals(0 orbitals) throws (:1240-1246)
+    if (nb == 0) fail(DFT_INVALID_ARGUMENT, "El numero de orbitales debe ser mayor que cero.");
+
+    const long long N = g.N, ld = N;
+    const int extra = std::max(0, o.extra_bands);
+    const int bands_a = (int)std::min<long long>(na + extra, N);
+    const int bands_b = (int)std::min<long long>(nb + extra, N);
+    EigOpts eo;
+    eo.tol = o.eig.tol > 0 ? o.eig.tol : 1e-7;
+    eo.max_iterations = o.eig.max_iterations > 0 ? o.eig.max_iterations : 2000;
+    eo.max_subspace = o.eig.max_subspace >= 2 ? o.eig.max_subspace : 3;
+    eo.verbose = o.eig.verbose;
+
+    DevBuf vext(N), da(N), db(N), rho(N), vh(N), vxa(N), vxb(N), va(N), vb(N), oa(N), ob(N), orho(N), ovh(N);
+    DevBuf psia((size_t)bands_a * ld), psib(closed ? 0 : (size_t)bands_b * ld);
+    std::vector<double> eiga(bands_a), eigb(bands_b), resa(bands_a), resb(bands_b);
+    std::vector<double> occa(bands_a, 0.0), occb(bands_b, 0.0);
+    for (int i = 0; i < na; ++i) occa[i] = 1.0;  // buildSpinOccupations: one electron per orbital
+    for (int i = 0; i < nb; ++i) occb[i] = 1.0;
+
+    nuclear_potential(ctx, g, nnuc, Z, xyz, vext.p);
+    // NuclearRepulsion::calculate (NuclearRepulsion.cpp:6-54)
+    double enn = 0.0;
+    for (int a = 0; a < nnuc; ++a)
+        for (int c = a + 1; c < nnuc; ++c) {
+            const double dx = xyz[3 * a] - xyz[3 * c], dy = xyz[3 * a + 1] - xyz[3 * c + 1],
+                         dz = xyz[3 * a + 2] - xyz[3 * c + 2];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 == 0.0) fail(DFT_SINGULAR, "NuclearRepulsion is undefined for coincident nuclei.");
+            enn += (double)Z[a] * (double)Z[c] / std::sqrt(d2);
+        }
+
+    // ---- initial densities from orbitals in the bare V_ext (MolecularSCFHelpers.cpp:515-579) --
+    int it_a = solve_orbitals(ctx, g, vext.p, na, bands_a, psia.p, ld, false, eiga.data(), resa.data(), eo);
+    (void)it_a;
+    spin_density(ctx, N, psia.p, bands_a, ld, occa.data(), da.p);
+    if (closed) {
+        DFT_CUDA(cudaMemcpyAsync(db.p, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        solve_orbitals(ctx, g, vext.p, nb, bands_b, psib.p, ld, false, eigb.data(), resb.data(), eo);
+        spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), db.p);
+    }
+
+    // ---- SCF loop, constants SelfConsistentFieldMolecule.cpp:27-31 ----------------------
+    double prevE = std::numeric_limits<double>::infinity();
+    double prevD = std::numeric_limits<double>::infinity();
+    double mixing = 0.25;  // DFTConstants::MIXING
+    double E[6] = {0, 0, 0, 0, 0, 0};
+    double effd = 0.0, resid = 0.0, dE = std::numeric_limits<double>::infinity();
+    bool converged = false;
+    int it = 0;
+    res->history_len = 0;
+    std::vector<double> Ta(bands_a), Tb(bands_b);
+    for (it = 1; it <= o.max_iterations; ++it) {
+        const auto t_it = Clock::now();
+        dft_scf_iteration rec{};
+        rec.iteration = it;
+        const double imix = mixing;
+        // n -> V_H(n) (MolecularSCFIteration.cpp:45-66)
+        auto t0 = Clock::now();
+        add2(ctx, N, da.p, db.p, rho.p);
+        JacobiResult jin = hartree(ctx, g, rho.p, vh.p, o.poisson_tol, o.poisson_max_sweeps);
+        sync(ctx);
+        rec.ms_hartree = ms_since(t0);
+        rec.poisson_sweeps_in = jin.sweeps;
+        // v_xc (:68-90): the closed-shell shortcut reuses alpha
+        t0 = Clock::now();
+        xc(ctx, g, kind, da.p, db.p, vxa.p, closed ? nullptr : vxb.p, false);
+        add3(ctx, N, vext.p, vh.p, vxa.p, va.p);
+        if (!closed) add3(ctx, N, vext.p, vh.p, vxb.p, vb.p);
+        sync(ctx);
+        rec.ms_xc = ms_since(t0);
+        // orbitals (:117-144), warm-started from the previous iteration
+        t0 = Clock::now();
+        rec.eig_iterations_alpha = solve_orbitals(ctx, g, va.p, na, bands_a, psia.p, ld, true, eiga.data(), resa.data(), eo);
+        if (!closed)
+            rec.eig_iterations_beta = solve_orbitals(ctx, g, vb.p, nb, bands_b, psib.p, ld, true, eigb.data(), resb.data(), eo);
+        rec.ms_orbitals = ms_since(t0);
+        // output densities (:160-187)
+        t0 = Clock::now();
+        spin_density(ctx, N, psia.p, bands_a, ld, occa.data(), oa.p);
+        if (closed) DFT_CUDA(cudaMemcpyAsync(ob.p, oa.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+        else spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), ob.p);
+        add2(ctx, N, oa.p, ob.p, orho.p);
+        JacobiResult jout = hartree(ctx, g, orho.p, ovh.p, o.poisson_tol, o.poisson_max_sweeps);
+        sync(ctx);
+        rec.ms_density = ms_since(t0);
+        rec.poisson_sweeps_out = jout.sweeps;
+        // energies (TotalEnergyMolecule.cpp:237-333): orbitals alpha then beta in one sum
+        t0 = Clock::now();
+        kinetic_per_band(ctx, g, psia.p, na, ld, Ta.data());
+        if (!closed) kinetic_per_band(ctx, g, psib.p, nb, ld, Tb.data());
+        double T = 0.0;
+        for (int i = 0; i < na; ++i) T += 1.0 * Ta[i];
+        for (int i = 0; i < nb; ++i) T += 1.0 * (closed ? Ta[i] : Tb[i]);
+        const double eext = dot3(ctx, N, orho.p, vext.p, g.dV);
+        const double eh = 0.5 * dot(ctx, N, orho.p, ovh.p) * g.dV;
+        const double exc = xc(ctx, g, kind, oa.p, ob.p, nullptr, nullptr, true);
+        E[0] = T;
+        E[1] = eext;
+        E[2] = eh;
+        E[3] = exc;
+        E[4] = enn;
+        E[5] = T + eext + eh + exc + enn;
+        // convergence measures (:201-250, MolecularSCFHelpers.cpp:46-183)
+        const double dd = density_difference(ctx, g, rho.p, orho.p);
+        const double sdd = std::max(density_difference(ctx, g, da.p, oa.p), density_difference(ctx, g, db.p, ob.p));
+        effd = std::max(dd, sdd);
+        resid = 0.0;
+        for (int i = 0; i < na; ++i) resid = std::max(resid, resa[i]);
+        if (!closed)
+            for (int i = 0; i < nb; ++i) resid = std::max(resid, resb[i]);
+        rec.ms_energy = ms_since(t0);
+        dE = std::isfinite(prevE) ? std::fabs(E[5] - prevE) : std::numeric_limits<double>::infinity();
+        converged = dE < o.energy_tol && effd < o.density_tol && resid < o.ks_tol;
+        rec.energy = E[5];
+        rec.energy_difference = dE;
+        rec.density_difference = effd;
+        rec.ks_residual = resid;
+        rec.mixing = imix;
+        rec.ms_total = ms_since(t_it);
+        if (res->history && res->history_len < res->history_capacity) res->history[res->history_len++] = rec;
+        if (o.verbose)
+            fprintf(stderr,
+                    "[scf] it=%3d E=%.12f dE=%.3e dRho=%.3e KS=%.3e mix=%.3f sweeps=%ld/%ld eig_it=%d/%d  %.1f ms\n", it,
+                    E[5], dE, effd, resid, imix, jin.sweeps, jout.sweeps, rec.eig_iterations_alpha,
+                    rec.eig_iterations_beta, rec.ms_total);
+        if (converged) break;
+        if (o.stop_abs_de > 0.0 && dE < o.stop_abs_de) break;
+        // adaptive mixing with the pre-update factor applied (:447-484)
+        if (std::isfinite(prevD)) {
+            if (effd > prevD * 1.05) mixing = std::max(0.10, mixing * 0.75);
+            else if (effd < prevD) mixing = std::min(0.50, mixing * 1.10);
+        }
+        mix(ctx, N, da.p, oa.p, imix);
+        mix(ctx, N, db.p, ob.p, imix);
+        prevD = effd;
+        prevE = E[5];
+    }
+    sync(ctx);
+    res->kinetic = E[0];
+    res->external = E[1];
+    res->hartree = E[2];
+    res->exchange_correlation = E[3];
+    res->nuclear_repulsion = E[4];
+    res->total = E[5];
+    res->iterations = std::min(it, o.max_iterations);
+    res->converged = converged ? 1 : 0;
+    res->density_difference = effd;
+    res->energy_difference = dE;
+    res->max_ks_residual = resid;
+    res->n_alpha = na;
+    res->n_beta = nb;
+    if (res->eigenvalues) {
+        for (int i = 0; i < na; ++i) res->eigenvalues[i] = eiga[i];
+        for (int i = 0; i < nb; ++i) res->eigenvalues[na + i] = closed ? eiga[i] : eigb[i];
+    }
+    if (res->alpha_density)
+        DFT_CUDA(cudaMemcpyAsync(res->alpha_density, oa.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream));
+    if (res->beta_density)
+        DFT_CUDA(cudaMemcpyAsync(res->beta_density, ob.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    res->seconds = ms_since(t_start) * 1e-3;
+}
+
+}  // namespace dftb

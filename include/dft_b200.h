@@ -1,0 +1,212 @@
+/*
+ * dft_b200 — C ABI of the B200-native real-space Kohn–Sham engine.
+ *
+ * This is the drop-in boundary for the reference's (willandru/DFT) C++ driver API:
+ * every entry point below replaces one reference function, cited beside it, and a
+ * header-only C++ shim (dft_b200.hpp) re-exports the reference signatures on top.
+ * Plain C types only: no CUDA, torch or STL types cross this boundary.
+ *
+ * Conventions
+ *  - Status: every function returns dft_status_t; on failure dft_last_error_message()
+ *    holds a one-line reason (thread-local).  The reference's exceptions map to
+ *    DFT_INVALID_ARGUMENT (std::invalid_argument) and DFT_NOT_CONVERGED / DFT_SINGULAR
+ *    (std::runtime_error).
+ *  - Memory: entry points ending in _dev take DEVICE pointers (from dft_device_alloc or
+ *    any cudaMalloc'd buffer on the context's device) and run stream-ordered on the
+ *    context's stream; results are ready after dft_context_synchronize().  Entry points
+ *    without the suffix take HOST pointers and block until done.
+ *  - Grids: point (i,j,k) lives at (k*ny + j)*nx + i, x fastest; spacing
+ *    (max-min)/(n-1) exactly as CartesianGrid (reference CartesianGrid.cpp:5-48).
+ *    A band block is band-major: band b starts at psi + b*ld (ld >= nx*ny*nz).
+ *  - Units: Hartree atomic units.  One context = one GPU; calls on one context are not
+ *    thread-safe.
+ */
+#ifndef DFT_B200_H
+#define DFT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    DFT_OK = 0,
+    DFT_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument */
+    DFT_NOT_CONVERGED = 2,    /* reference: std::runtime_error from the Davidson solver */
+    DFT_CAP_REACHED = 3,      /* an iteration cap was hit where the reference would throw */
+    DFT_SINGULAR = 4,         /* reference: singular tridiagonal pivot / nucleus on a node */
+    DFT_CUDA_ERROR = 5,       /* a CUDA runtime call failed */
+    DFT_NUMERICAL = 6         /* NaN/Inf detected in device data */
+} dft_status_t;
+
+typedef enum { DFT_XC_PZ81 = 0, DFT_XC_PBE96 = 1 } dft_xc_kind; /* PZ81.h / PBE96.h */
+
+/* CartesianGrid(nx,ny,nz,xmin,xmax,ymin,ymax,zmin,zmax), reference CartesianGrid.h:5-60 */
+typedef struct {
+    long nx, ny, nz;
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+} dft_grid;
+
+typedef struct dft_context dft_context;
+
+const char* dft_last_error_message(void);
+const char* dft_version(void);
+
+/* ---- context and device memory (no reference counterpart: the reference has no device) ---- */
+dft_status_t dft_context_create(int device, dft_context** out);
+dft_status_t dft_context_destroy(dft_context* ctx);
+dft_status_t dft_context_synchronize(dft_context* ctx);
+/* The cudaStream_t the context launches on, as an opaque handle (for event timing). */
+void* dft_context_stream(dft_context* ctx);
+/* Number of kernels this context has launched so far (diagnostics, bench accounting). */
+long long dft_context_launch_count(dft_context* ctx);
+dft_status_t dft_device_alloc(dft_context* ctx, size_t bytes, void** out);
+dft_status_t dft_device_free(dft_context* ctx, void* ptr);
+dft_status_t dft_copy_h2d(dft_context* ctx, void* dst, const void* src, size_t bytes);
+dft_status_t dft_copy_d2h(dft_context* ctx, void* dst, const void* src, size_t bytes);
+
+/* ---- 3D operators on device buffers ---------------------------------------------------- */
+
+/* applyMolecularKohnShamHamiltonian (reference KohnShamHamiltonianMolecule.h:7-11,
+ * KohnShamHamiltonianMolecule.cpp:7-183) over a block of nbands bands:
+ * hpsi_b = -1/2 lap_h psi_b + V psi_b, psi = 0 outside the box.  Bit-identical to the
+ * reference for each band. */
+dft_status_t dft_apply_hamiltonian_dev(dft_context* ctx, const dft_grid* g, const double* V, const double* psi,
+                                       double* hpsi, int nbands, long ld);
+
+/* calculateHartreePotential (reference HartreePotentialMolecule.h:7-10,
+ * HartreePotentialMolecule.cpp:99-324): boundary fill Q/|r| (zero on a face), then Jacobi
+ * sweeps for lap V = -4 pi rho from a cold (zero) interior start, stopping at the first
+ * sweep whose max|dV| < tol or after max_sweeps sweeps (tol = 1e-8, max_sweeps = 10000
+ * reproduce the reference bit-for-bit).  sweeps_out (host, may be NULL) receives the
+ * number of sweeps run; last_diff_out (host, may be NULL) the last sweep's max|dV|. */
+dft_status_t dft_hartree_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
+                             long max_sweeps, long* sweeps_out, double* last_diff_out);
+
+/* calculateHartreeEnergy (reference HartreePotentialMolecule.cpp:326-379): 1/2 sum rho V dV. */
+dft_status_t dft_hartree_energy_dev(dft_context* ctx, const dft_grid* g, const double* rho, const double* vh,
+                                    double* energy_out);
+
+/* calculateMolecularSpinExchangeCorrelationPotential for spin 0 and 1 in one pass, plus
+ * calculateMolecularExchangeCorrelationEnergy (reference ExchangeCorrelationMolecule.h:8-21,
+ * ExchangeCorrelationMolecule.cpp:576-842).  va/vb may be NULL to skip a spin; exc_out
+ * (host, may be NULL) receives E_xc. */
+dft_status_t dft_xc_dev(dft_context* ctx, const dft_grid* g, dft_xc_kind kind, const double* na, const double* nb,
+                        double* va, double* vb, double* exc_out);
+
+/* XCFunctional::evaluate (reference XCFunctional.h:15-22) at m independent points;
+ * out5 is m x {energyPerElectron, potentialAlpha, potentialBeta, gradCoefAlpha, gradCoefBeta}. */
+dft_status_t dft_xc_evaluate_dev(dft_context* ctx, dft_xc_kind kind, long m, const double* na, const double* nb,
+                                 const double* ga, const double* gb, double* out5);
+
+/* calculateMolecularSpinDensity (reference ElectronDensityMolecule.cpp:5-76):
+ * out = sum_b occ[b] psi_b^2 in band order; occ is a host array of nbands weights. */
+dft_status_t dft_spin_density_dev(dft_context* ctx, long npoints, const double* psi, int nbands, long ld,
+                                  const double* occ, double* out);
+
+/* calculateMolecularKineticEnergy (reference TotalEnergyMolecule.cpp:13-199, the face
+ * stencil of existing neighbours): sum_b occ[b] <psi_b| -1/2 lap |psi_b> dV. */
+dft_status_t dft_kinetic_energy_dev(dft_context* ctx, const dft_grid* g, const double* psi, int nbands, long ld,
+                                    const double* occ, double* energy_out);
+
+/* NuclearPotential::calculate (reference NuclearPotential.cpp:6-76); Z and xyz are HOST
+ * arrays of nnuc charges and positions.  DFT_SINGULAR if a node coincides with a nucleus. */
+dft_status_t dft_nuclear_potential_dev(dft_context* ctx, const dft_grid* g, int nnuc, const int* Z,
+                                       const double* xyz, double* vext);
+
+/* ---- eigensolver --------------------------------------------------------------------- */
+
+typedef struct {
+    double tol;          /* residual norm (dV-weighted) for occupied bands; 1e-7 (reference :19) */
+    int max_iterations;  /* block iterations cap */
+    int max_subspace;    /* basis size cap in multiples of nbands (>= 2) */
+    int verbose;         /* 1: per-iteration lines on stderr */
+} dft_eig_opts;
+
+/* solveMolecularOrbitals (reference EigenvalueSolverMolecule.h:20-28,
+ * EigenvalueSolverMolecule.cpp:1233-1300): the lowest nocc eigenpairs of H = -1/2 lap_h + V,
+ * computed by a block Davidson method over nbands >= nocc bands.  psi (nbands x ld, device)
+ * holds the start vectors on entry (any non-zero block; orthonormalised internally) and the
+ * dV-normalised eigenvectors on exit; eig (host, nbands) the eigenvalues.  When init is 0,
+ * psi's contents are ignored and the reference's Gaussian x polynomial seeds are used.
+ * iterations_out (host, may be NULL).  DFT_NOT_CONVERGED if the occupied residuals stay
+ * above tol after max_iterations (reference: runtime_error). */
+dft_status_t dft_solve_orbitals_dev(dft_context* ctx, const dft_grid* g, const double* V, int nocc, int nbands,
+                                    double* psi, long ld, int init, double* eig, const dft_eig_opts* opts,
+                                    int* iterations_out);
+
+/* ---- SCF drivers (host in, host out) ------------------------------------------------- */
+
+typedef struct {
+    int max_iterations;      /* 250 (DFTConstants.h:13) */
+    double energy_tol;       /* 1e-11 (DFTConstants.h:16) */
+    double density_tol;      /* 1e-9  (DFTConstants.h:15) */
+    double ks_tol;           /* 1e-7  (DFTConstants.h:17) */
+    double stop_abs_de;      /* > 0: also stop as soon as |dE| < stop_abs_de (time-to-|dE| metric) */
+    double poisson_tol;      /* 1e-8  (HartreePotentialMolecule.cpp:15) */
+    long poisson_max_sweeps; /* 10000 (HartreePotentialMolecule.cpp:14) */
+    int extra_bands;         /* unoccupied buffer bands per spin in the block eigensolver */
+    dft_eig_opts eig;        /* eigensolver options (tol = 1e-7 reproduces the reference) */
+    int verbose;             /* 1: one line per SCF iteration on stderr */
+} dft_scf_opts;
+
+/* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)
+ * plus device phase times that the reference leaves at zero. */
+typedef struct {
+    int iteration;
+    double energy, energy_difference, density_difference, ks_residual, mixing;
+    long poisson_sweeps_in, poisson_sweeps_out;
+    int eig_iterations_alpha, eig_iterations_beta;
+    double ms_hartree, ms_xc, ms_orbitals, ms_density, ms_energy, ms_total;
+} dft_scf_iteration;
+
+typedef struct {
+    /* EnergyComponents (reference DFTData.h:47-54) */
+    double kinetic, external, hartree, exchange_correlation, nuclear_repulsion, total;
+    int iterations, converged;
+    double density_difference, energy_difference, max_ks_residual;
+    int n_alpha, n_beta;
+    double* eigenvalues;            /* caller buffer, >= n_alpha + n_beta entries (alpha then beta), or NULL */
+    double* alpha_density;          /* caller buffers of N doubles, or NULL */
+    double* beta_density;
+    dft_scf_iteration* history;     /* caller buffer of history_capacity records, or NULL */
+    int history_capacity, history_len;
+    double seconds;                 /* wall time of the solve */
+} dft_scf_result;
+
+void dft_scf_default_options(dft_scf_opts* opts);
+
+/* solveMolecularSelfConsistentField (reference SelfConsistentFieldMolecule.h:8-14,
+ * SelfConsistentFieldMolecule.cpp:50-561; iteration MolecularSCFIteration.cpp:12-252):
+ * nuclei Z[nnuc] at xyz[3*nnuc] (host), charge, multiplicity (1 = closed shell, beta := alpha),
+ * functional kind.  Fills *result (host).  Returns DFT_OK whether or not the SCF converged
+ * (result->converged says which), as the reference does. */
+dft_status_t dft_scf_molecule(dft_context* ctx, const dft_grid* g, int nnuc, const int* Z, const double* xyz,
+                              int charge, int multiplicity, dft_xc_kind kind, const dft_scf_opts* opts,
+                              dft_scf_result* result);
+
+/* ---- radial atoms --------------------------------------------------------------------- */
+
+typedef struct {
+    int Z;
+    int kind;                      /* dft_xc_kind */
+    double kinetic, external, hartree, exchange_correlation, total; /* EnergyComponents */
+    int iterations, converged;
+    double density_difference, max_ks_residual;
+    int n_orbitals;                /* occupied (n,l,spin) orbitals, alpha then beta */
+    double eigenvalues[16];
+    int status;                    /* dft_status_t of this run */
+} dft_atom_result;
+
+/* solveAtom / solveSelfConsistentField (reference AtomicDFT.h:7-11, AtomicDFT.cpp:7-42,
+ * SelfConsistentField.cpp:539-786) for nruns independent atoms (Z[r] in 1..30 with the
+ * reference's configurations, kinds[r]) on RadialGrid(points, rmax), all advanced by one
+ * persistent kernel launch, one thread block per run.  results: host array of nruns. */
+dft_status_t dft_solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, long points, double rmax,
+                             dft_atom_result* results);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DFT_B200_H */

@@ -1,0 +1,238 @@
+"""GPU parity of the 3D operators against the CPU oracle (oracle/dft_oracle.c, itself pinned
+bit-for-bit to the reference in test_oracle_pin.py) and the reference's own fixture.
+
+Bars: H psi, Jacobi Poisson (values and sweep count), density and the nuclear potential are
+bit-identical; XC and reductions agree to relative 1e-12 (device libm and summation order).
+"""
+import numpy as np
+import pytest
+
+import dft_b200
+from conftest import gaussian_density, golden, grid_coords
+from oracle.bindings import PBE96, PZ81
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [
+    ((11, 9, 8), (-3.0, 3.4, -2.5, 2.9, -2.2, 2.0)),
+    ((33, 17, 21), (-4.0, 4.0, -2.0, 2.0, -2.5, 2.5)),
+    ((5, 6, 4), (-2.0, 2.2, -1.0, 1.5, -1.7, 1.3)),   # faces not exactly on xmax: non-zero boundary values
+    ((48, 48, 48), (-7.05, 7.05) * 3),                 # the H2 48^3, h = 0.3 grid
+]
+XC_RTOL = 1e-12
+
+
+def G(n, b):
+    return dft_b200.CartesianGrid(*n, *b)
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("n,b", GRIDS)
+def test_hpsi_bit_exact(engine, port, n, b):
+    rng = np.random.default_rng(11)
+    N = int(np.prod(n))
+    nb_, ld = 3, N + 37  # padded leading dimension
+    V = rng.standard_normal(N)
+    psi = np.zeros((nb_, ld))
+    psi[:, :N] = rng.standard_normal((nb_, N))
+    dV, dP, dH = engine.upload(V), engine.upload(psi), engine.array(nb_ * ld)
+    engine.apply_hamiltonian(G(n, b), dV, dP, dH, nb_, ld)
+    H = dH.to_host((nb_, ld))
+    for k in range(nb_):
+        assert np.array_equal(H[k, :N], port.apply_hamiltonian(n, b, V, psi[k, :N])), k
+
+
+def test_hpsi_large_numpy_restatement(engine):
+    """128^3 x 4 bands: bit-identical to a vectorised numpy restatement of the same stencil order."""
+    n, b = (128, 128, 128), (-12.7, 12.7) * 3
+    g = G(n, b)
+    N = g.getSize()
+    rng = np.random.default_rng(5)
+    V = rng.standard_normal(N)
+    psi = rng.standard_normal((4, N))
+    dH = engine.array(4 * N)
+    engine.apply_hamiltonian(g, engine.upload(V), engine.upload(psi), dH, 4, N)
+    H = dH.to_host((4, N))
+    dx = (b[1] - b[0]) / (n[0] - 1)
+    ix = 1.0 / (dx * dx)
+    k0 = -2.0 * (ix + ix + ix)
+    for band in (0, 3):
+        p = psi[band].reshape(n[2], n[1], n[0])
+        lap = k0 * p
+        for ax, sl in ((2, -1), (2, 1), (1, -1), (1, 1), (0, -1), (0, 1)):
+            nb = np.zeros_like(p)
+            src = [slice(None)] * 3
+            dst = [slice(None)] * 3
+            if sl == -1:  # neighbour at index-1
+                dst[ax], src[ax] = slice(1, None), slice(None, -1)
+            else:
+                dst[ax], src[ax] = slice(None, -1), slice(1, None)
+            nb[tuple(dst)] = p[tuple(src)] * ix
+            mask = np.zeros_like(p, dtype=bool)
+            mask[tuple(dst)] = True
+            lap = np.where(mask, lap + nb, lap)
+        ref = -0.5 * lap + V.reshape(p.shape) * p
+        assert np.array_equal(H[band], ref.ravel())
+
+
+@pytest.mark.parametrize("n,b", GRIDS[:3] + [((24, 24, 24), (-6.0, 6.0) * 3)])
+def test_jacobi_bit_exact_and_sweeps(engine, port, n, b):
+    na, nb = gaussian_density(n, b, 2)
+    rho = na + nb
+    ref = np.empty(rho.size)
+    import ctypes as C
+    sw = C.c_long()
+    ld = C.c_double()
+    port.check(port.fn("hartree_potential_ex")(np.asarray(n, dtype=np.int64).ctypes.data_as(C.POINTER(C.c_long)),
+                                               np.asarray(b, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double)),
+                                               rho.ctypes.data_as(C.POINTER(C.c_double)),
+                                               ref.ctypes.data_as(C.POINTER(C.c_double)), C.byref(sw), C.byref(ld)))
+    d_rho, d_vh = engine.upload(rho), engine.array(rho.size)
+    sweeps, last = engine.hartree(G(n, b), d_rho, d_vh)
+    assert sweeps == sw.value
+    assert last == ld.value
+    assert np.array_equal(d_vh.to_host(), ref)
+
+
+def test_jacobi_cap(engine, port):
+    """The silent sweep cap (HartreePotentialMolecule.cpp:207): stop after max_sweeps."""
+    n, b = (24, 24, 24), (-6.0, 6.0) * 3
+    na, nb = gaussian_density(n, b, 4)
+    d_rho, d_vh = engine.upload(na + nb), engine.array(na.size)
+    sweeps, last = engine.hartree(G(n, b), d_rho, d_vh, tol=1e-8, max_sweeps=37)
+    assert sweeps == 37 and last > 1e-8
+    sweeps0, _ = engine.hartree(G(n, b), d_rho, d_vh, tol=1e-8, max_sweeps=0)
+    assert sweeps0 == 0
+
+
+def test_reference_ops_fixture(engine):
+    """Against outputs of the reference itself (tests/golden/ops_ref.json)."""
+    fx = golden("ops_ref.json")
+    n, b = tuple(fx["n"]), tuple(fx["bounds"])
+    g = G(n, b)
+    N = g.getSize()
+    na, nb, V = map(np.asarray, (fx["na"], fx["nb"], fx["V"]))
+    psi = np.asarray(fx["psi"])
+    dH = engine.array(3 * N)
+    engine.apply_hamiltonian(g, engine.upload(V), engine.upload(psi), dH, 3, N)
+    assert np.array_equal(dH.to_host((3, N)), np.asarray(fx["hpsi"]))
+    dvh = engine.array(N)
+    engine.hartree(g, engine.upload(na + nb), dvh)
+    assert np.array_equal(dvh.to_host(), np.asarray(fx["vh"]))
+    d_na, d_nb = engine.upload(na), engine.upload(nb)
+    for kind, tag in ((PZ81, "pz81"), (PBE96, "pbe96")):
+        va, vb = engine.array(N), engine.array(N)
+        exc = engine.xc(g, kind, d_na, d_nb, va, vb)
+        assert rel(va.to_host(), fx[f"vxc_{tag}_a"]) < XC_RTOL
+        assert rel(vb.to_host(), fx[f"vxc_{tag}_b"]) < XC_RTOL
+        assert abs(exc - fx[f"exc_{tag}"]) <= XC_RTOL * abs(fx[f"exc_{tag}"])
+    d_psi = engine.upload(psi)
+    assert abs(engine.kinetic_energy(g, d_psi, 3, N, [1, 1, 1]) - fx["T"]) <= 1e-12 * abs(fx["T"])
+    dd = engine.array(N)
+    engine.spin_density(N, d_psi, 3, N, [1, 1, 1], dd)
+    assert np.array_equal(dd.to_host(), np.asarray(fx["dens"]))
+    dv = engine.array(N)
+    engine.nuclear_potential(g, fx["Zs"], np.ravel(fx["xyz"]), dv)
+    assert np.array_equal(dv.to_host(), np.asarray(fx["vext"]))
+
+
+@pytest.mark.parametrize("n,b", GRIDS)
+@pytest.mark.parametrize("kind", [PZ81, PBE96])
+def test_xc_potential_and_energy(engine, port, n, b, kind):
+    na, nb = gaussian_density(n, b, 9)
+    g = G(n, b)
+    N = g.getSize()
+    va, vb = engine.array(N), engine.array(N)
+    e = engine.xc(g, kind, engine.upload(na), engine.upload(nb), va, vb)
+    assert rel(va.to_host(), port.xc_potential(kind, n, b, na, nb, 0)) < XC_RTOL
+    assert rel(vb.to_host(), port.xc_potential(kind, n, b, na, nb, 1)) < XC_RTOL
+    eo = port.xc_energy(kind, n, b, na, nb)
+    assert abs(e - eo) <= XC_RTOL * abs(eo)
+
+
+@pytest.mark.parametrize("kind", [PZ81, PBE96])
+def test_xc_evaluate_pointwise(engine, port, kind):
+    rng = np.random.default_rng(3)
+    m = 20000
+    na = 10.0 ** rng.uniform(-24, 2, m)
+    nb = 10.0 ** rng.uniform(-24, 2, m)
+    nb[::7] = 0.0
+    na[::11] = 0.0
+    ga = rng.standard_normal(m) * 10.0 ** rng.uniform(-6, 2, m)
+    gb = rng.standard_normal(m) * 10.0 ** rng.uniform(-6, 2, m)
+    ga[::13] = 0.0
+    out = engine.array(5 * m)
+    engine.xc_evaluate(kind, m, engine.upload(na), engine.upload(nb), engine.upload(ga), engine.upload(gb), out)
+    got = out.to_host((m, 5))
+    want = port.xc_evaluate(kind, na, nb, ga, gb)
+    scale = np.maximum(np.abs(want), 1e-300)
+    err = np.abs(got - want) / scale
+    err[np.abs(want) < 1e-200] = np.abs(got - want)[np.abs(want) < 1e-200]
+    assert np.max(err) < 1e-11
+
+
+def test_density_kinetic_bit_and_tol(engine, port):
+    n, b = (33, 17, 21), (-4.0, 4.0, -2.0, 2.0, -2.5, 2.5)
+    g = G(n, b)
+    N = g.getSize()
+    rng = np.random.default_rng(8)
+    psi = rng.standard_normal((5, N))
+    occ = [1, 1, 0, 2, 1]
+    d = engine.array(N)
+    dp = engine.upload(psi)
+    engine.spin_density(N, dp, 5, N, occ, d)
+    assert np.array_equal(d.to_host(), port.spin_density(psi, occ))
+    t = engine.kinetic_energy(g, dp, 5, N, occ)
+    to = port.kinetic_energy(n, b, psi, occ)
+    assert abs(t - to) <= 1e-12 * abs(to)
+
+
+def test_nuclear_potential(engine, port):
+    n, b = (48, 48, 48), (-7.05, 7.05) * 3
+    Z = [8, 1, 1, 6]
+    xyz = np.array([0.0, 0.01, 0.0, 1.4305, 0.0, 1.1084, -1.4305, 0.0, 1.1084, 2.0, 2.1, -1.3])
+    d = engine.array(48 ** 3)
+    engine.nuclear_potential(G(n, b), Z, xyz, d)
+    assert np.array_equal(d.to_host(), port.nuclear_potential(n, b, Z, xyz))
+    X, Y, Zc = grid_coords(n, b)
+    on_node = [1, X[1000], Y[1000], Zc[1000]]
+    with pytest.raises(dft_b200.DFTError) as ei:
+        engine.nuclear_potential(G(n, b), [1], np.array(on_node[1:]), d)
+    assert ei.value.status == dft_b200.DFT_SINGULAR
+
+
+@pytest.mark.parametrize("case", ["h2o_11", "h2_16"])
+def test_block_davidson_vs_reference_algorithm(engine, port, case):
+    """Eigenpairs of the block solver vs the reference's state-by-state Davidson (oracle)."""
+    if case == "h2o_11":
+        n, b, Z = (11, 9, 8), (-3.0, 3.4, -2.5, 2.9, -2.2, 2.0), [8, 1, 1]
+        xyz = np.array([0.05, 0.07, 0.03, 1.43, 0.07, 1.1, -1.43, 0.07, 1.1])
+        nocc = 4
+    else:
+        n, b, Z = (16, 16, 16), (-6.0, 6.0) * 3, [1, 1]
+        xyz = np.array([-0.7, 0.0, 0.0, 0.7, 0.0, 0.0])
+        nocc = 3
+    g = G(n, b)
+    N = g.getSize()
+    V = port.nuclear_potential(n, b, Z, xyz)
+    e_ref, psi_ref = port.solve_orbitals(n, b, V, nocc)
+    nbands = nocc + 3
+    psi = engine.array(nbands * N)
+    eig, it = engine.solve_orbitals(g, engine.upload(V), nocc, nbands, psi, N, init=False)
+    assert np.max(np.abs(eig[:nocc] - e_ref)) < 1e-9
+    P = psi.to_host((nbands, N))
+    dV = g.getDx() * g.getDy() * g.getDz()
+    # dV-normalised, orthonormal, and the same subspace as the reference's orbitals
+    S = P[:nocc] @ P[:nocc].T * dV
+    assert np.max(np.abs(S - np.eye(nocc))) < 1e-10
+    overlap = psi_ref @ P[:nocc].T * dV
+    assert np.max(np.abs(np.abs(np.linalg.det(overlap)) - 1.0)) < 1e-6
+    # KS residuals below the reference tolerance
+    for k in range(nocc):
+        hp = port.apply_hamiltonian(n, b, V, P[k])
+        r = np.sqrt(np.sum((hp - eig[k] * P[k]) ** 2) * dV)
+        assert r < 1e-7
