@@ -62,6 +62,8 @@ class dft_scf_result(C.Structure):
                 ("energy_difference", C.c_double), ("max_ks_residual", C.c_double), ("n_alpha", C.c_int),
                 ("n_beta", C.c_int), ("eigenvalues", C.POINTER(C.c_double)),
                 ("alpha_density", C.POINTER(C.c_double)), ("beta_density", C.POINTER(C.c_double)),
+                ("alpha_potential", C.POINTER(C.c_double)), ("beta_potential", C.POINTER(C.c_double)),
+                ("orbitals", C.POINTER(C.c_double)),
                 ("history", C.POINTER(dft_scf_iteration)), ("history_capacity", C.c_int),
                 ("history_len", C.c_int), ("seconds", C.c_double)]
 

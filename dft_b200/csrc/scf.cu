@@ -221,6 +221,16 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         DFT_CUDA(cudaMemcpyAsync(res->alpha_density, oa.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream));
     if (res->beta_density)
         DFT_CUDA(cudaMemcpyAsync(res->beta_density, ob.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream));
+    if (res->alpha_potential)
+        DFT_CUDA(cudaMemcpyAsync(res->alpha_potential, va.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream));
+    if (res->beta_potential)
+        DFT_CUDA(cudaMemcpyAsync(res->beta_potential, closed ? va.p : vb.p, sizeof(double) * N, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    if (res->orbitals) {
+        DFT_CUDA(cudaMemcpyAsync(res->orbitals, psia.p, sizeof(double) * N * na, cudaMemcpyDeviceToHost, ctx->stream));
+        DFT_CUDA(cudaMemcpyAsync(res->orbitals + (size_t)na * N, closed ? psia.p : psib.p, sizeof(double) * N * nb,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    }
     sync(ctx);
     res->seconds = ms_since(t_start) * 1e-3;
 }

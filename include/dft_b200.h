@@ -170,6 +170,9 @@ typedef struct {
     double* eigenvalues;            /* caller buffer, >= n_alpha + n_beta entries (alpha then beta), or NULL */
     double* alpha_density;          /* caller buffers of N doubles, or NULL */
     double* beta_density;
+    double* alpha_potential;        /* effective potentials of the last iteration (N doubles each), or NULL */
+    double* beta_potential;
+    double* orbitals;               /* caller buffer of (n_alpha + n_beta) x N doubles (alpha then beta), or NULL */
     dft_scf_iteration* history;     /* caller buffer of history_capacity records, or NULL */
     int history_capacity, history_len;
     double seconds;                 /* wall time of the solve */
