@@ -1,0 +1,123 @@
+"""Per-operator timings of libdft_b200 on one GPU (CUDA events on the library's stream).
+
+    python -m dft_b200.microbench hpsi   --n 192 --bands 16 [--reps 5]
+    python -m dft_b200.microbench jacobi --n 48  [--sweeps 10000]
+    python -m dft_b200.microbench xc     --n 128 --functional PBE96
+    python -m dft_b200.microbench scf    --n 48  [--iterations 1]     # H2 at h = 0.3 (n = 48)
+    python -m dft_b200.microbench radial                              # 60 atoms, one launch
+
+Each mode prints one JSON line with the time and the achieved bandwidth for the
+operator's algorithmic bytes.  Used for roofline numbers and as the command under ncu.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import statistics
+
+import numpy as np
+
+import dft_b200 as d
+
+
+def _events(torch, stream, fn, reps, flush=None):
+    times = []
+    for _ in range(reps):
+        with torch.cuda.stream(stream):
+            if flush is not None:
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        fn()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def cube(n, h):
+    half = 0.5 * h * (n - 1)
+    return d.CartesianGrid(n, n, n, -half, half, -half, half, -half, half)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--h", type=float, default=0.2)
+    ap.add_argument("--bands", type=int, default=16)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--sweeps", type=int, default=10000)
+    ap.add_argument("--iterations", type=int, default=1)
+    ap.add_argument("--functional", default="PBE96")
+    a = ap.parse_args()
+    import torch
+
+    eng = d.Engine(0)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {"mode": a.mode}
+    if a.mode == "hpsi":
+        g = cube(a.n, a.h)
+        N = g.getSize()
+        V, P, H = eng.array(N), eng.array(N * a.bands), eng.array(N * a.bands)
+        t = _events(torch, stream, lambda: eng.apply_hamiltonian(g, V, P, H, a.bands, N), a.reps, flush)
+        ms = statistics.median(t)
+        byts = (16.0 + 8.0 / a.bands) * N * a.bands
+        out.update(n=a.n, bands=a.bands, ms=ms, gbs=byts / (ms * 1e-3) / 1e9, bytes=byts)
+    elif a.mode == "jacobi":
+        g = cube(a.n, a.h)
+        N = g.getSize()
+        x = np.linspace(-1, 1, a.n)
+        X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+        rho = eng.upload(np.exp(-8 * (X ** 2 + Y ** 2 + Z ** 2)).ravel())
+        vh = eng.array(N)
+        res = {}
+
+        def run():
+            res["s"] = eng.hartree(g, rho, vh, 1e-8, a.sweeps)[0]
+
+        t = _events(torch, stream, run, a.reps)
+        ms = statistics.median(t)
+        interior = (a.n - 2) ** 3
+        out.update(n=a.n, sweeps=res["s"], ms=ms, us_per_sweep=1e3 * ms / res["s"],
+                   gbs=24.0 * interior * res["s"] / (ms * 1e-3) / 1e9)
+    elif a.mode == "xc":
+        g = cube(a.n, a.h)
+        N = g.getSize()
+        x = np.linspace(-1, 1, a.n)
+        X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+        r2 = (X ** 2 + Y ** 2 + Z ** 2).ravel()
+        na, nb = eng.upload(np.exp(-6 * r2)), eng.upload(0.7 * np.exp(-5 * r2))
+        va, vb = eng.array(N), eng.array(N)
+        t = _events(torch, stream, lambda: eng.xc(g, a.functional, na, nb, va, vb, energy=True), a.reps, flush)
+        ms = statistics.median(t)
+        out.update(n=a.n, functional=a.functional, ms=ms, gpoints_per_s=N / (ms * 1e-3) / 1e9,
+                   gbs=32.0 * N / (ms * 1e-3) / 1e9)
+    elif a.mode == "scf":
+        g = cube(a.n, 0.3 if a.n == 48 else a.h)
+        m = d.Molecule()
+        m.addNucleus(1, -0.7, 0, 0)
+        m.addNucleus(1, 0.7, 0, 0)
+        o = d.default_scf_options(max_iterations=a.iterations, extra_bands=3)
+        r = eng.scf_molecule(g, m, 0, 1, "PZ81", o)
+        out.update(n=a.n, iterations=r.iterations, energy=r.total, seconds=r.seconds, launches=eng.launches)
+    elif a.mode == "radial":
+        Zs = list(range(1, 31)) * 2
+        ks = ["PZ81"] * 30 + ["PBE96"] * 30
+        res = {}
+
+        def run():
+            res["r"] = eng.solve_atoms(Zs, ks)
+
+        t = _events(torch, stream, run, max(1, a.reps // 2))
+        ms = statistics.median(t)
+        out.update(runs=60, ms=ms, runs_per_s=60 / (ms * 1e-3),
+                   max_iterations=max(r.iterations for r in res["r"]))
+    print(json.dumps(out), flush=True)
+    eng.close()
+
+
+if __name__ == "__main__":
+    main()
