@@ -93,6 +93,8 @@ _SIGS = {
     "dft_copy_d2h": ([_P, _P, _P, C.c_size_t], C.c_int),
     "dft_apply_hamiltonian_dev": ([_P, C.POINTER(dft_grid), _P, _P, _P, C.c_int, C.c_long], C.c_int),
     "dft_hartree_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double, C.c_long, C.POINTER(C.c_long), _D], C.c_int),
+    "dft_hartree_noalloc_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double, C.c_long, C.POINTER(C.c_long), _D],
+                                C.c_int),
     "dft_hartree_energy_dev": ([_P, C.POINTER(dft_grid), _P, _P, _D], C.c_int),
     "dft_xc_dev": ([_P, C.POINTER(dft_grid), C.c_int, _P, _P, _P, _P, _D], C.c_int),
     "dft_xc_evaluate_dev": ([_P, C.c_int, C.c_long, _P, _P, _P, _P, _P], C.c_int),

@@ -176,6 +176,18 @@ dft_status_t dft_hartree_dev(dft_context* ctx, const dft_grid* g, const double* 
     });
 }
 
+dft_status_t dft_hartree_noalloc_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
+                                     long max_sweeps, long* sweeps_out, double* last_diff_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && rho && vh, "NULL argument");
+        NEED(rho != vh, "rho and vh must not alias");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::JacobiResult r = dftb::hartree_noalloc(ctx, G, rho, vh, tol, max_sweeps);
+        if (sweeps_out) *sweeps_out = r.sweeps;
+        if (last_diff_out) *last_diff_out = r.last_diff;
+    });
+}
+
 dft_status_t dft_hartree_energy_dev(dft_context* ctx, const dft_grid* g, const double* rho, const double* vh,
                                     double* energy_out) {
     return guard(ctx, [&] {

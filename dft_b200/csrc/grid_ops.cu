@@ -10,6 +10,7 @@
 // order (no FMA contraction), which makes it bit-identical to the reference.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "ops.h"
 #include "xc_device.cuh"
@@ -399,6 +400,103 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
         DFT_CUDA(cudaMemcpyAsync(vh, buf1, sizeof(double) * (size_t)g.N, cudaMemcpyDeviceToDevice, ctx->stream));
     }
     return {sweeps, hc->last_diff};
+}
+
+// =============================================================== allocation-free Poisson
+// The Jacobi solve above takes its second iterate buffer and its control words from the
+// context's workspace, which grows with cudaMalloc.  Some callers cannot let a library
+// allocate device memory: a host application that owns the whole device memory budget
+// through its own pooled allocator, or a plugin called from inside such an application's
+// compute step, where a cudaMalloc/cudaFree would also synchronise the device.  For them
+// hartree_noalloc runs the same kernels on a fixed scratch array compiled into the library.
+//
+// Limit: grids of at most NOALLOC_MAX_POINTS points (128^3).  Every GPU that loads the
+// library holds the array (16 MiB + 128 B) until the process exits.  All calls share it:
+// calls that overlap on the GPU (several streams or contexts on one device) race on it.
+namespace {
+
+constexpr long long NOALLOC_MAX_POINTS = 128LL * 128 * 128;
+constexpr int NOALLOC_CTRL_DOUBLES = 16;  // JacobiCtrl and the boundary charge live after the buffer
+
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_MAX_POINTS + NOALLOC_CTRL_DOUBLES];
+
+static_assert(sizeof(JacobiCtrl) + sizeof(double) <= NOALLOC_CTRL_DOUBLES * sizeof(double), "control words");
+
+// Device address of g_noalloc_scratch, looked up once per device with that device current.
+double* noalloc_scratch(int device) {
+    static double* addr[64] = {};
+    static std::mutex m;
+    if (device < 0 || device >= 64) fail(DFT_INVALID_ARGUMENT, "device index %d out of range", device);
+    std::lock_guard<std::mutex> lock(m);
+    if (!addr[device]) {
+        double* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            fail(DFT_CUDA_ERROR, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s", cudaGetErrorString(e));
+        addr[device] = p;
+    }
+    return addr[device];
+}
+
+}  // namespace
+
+JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol,
+                             long max_sweeps) {
+    if (g.N > NOALLOC_MAX_POINTS)
+        fail(DFT_INVALID_ARGUMENT,
+             "grid of %lld points exceeds the allocation-free Poisson limit of %lld points (128^3); "
+             "use dft_hartree_dev",
+             g.N, NOALLOC_MAX_POINTS);
+    if (max_sweeps < 0) fail(DFT_INVALID_ARGUMENT, "max_sweeps must be >= 0");
+    double* scratch = noalloc_scratch(ctx->device);
+    double* buf1 = scratch;
+    JacobiCtrl* ctrl = (JacobiCtrl*)(scratch + NOALLOC_MAX_POINTS);
+    double* qslot = scratch + NOALLOC_MAX_POINTS + NOALLOC_CTRL_DOUBLES - 1;
+    const bool exact_faces = (g.xmin + (double)(g.nx - 1) * g.dx == g.xmax) &&
+                             (g.ymin + (double)(g.ny - 1) * g.dy == g.ymax) &&
+                             (g.zmin + (double)(g.nz - 1) * g.dz == g.zmax);
+    double Q = 0.0;
+    if (!exact_faces) {
+        total_charge_seq_kernel<<<1, 32, 0, ctx->stream>>>(g.N, rho, g.dV, qslot);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+        DFT_CUDA(cudaMemcpyAsync(&Q, qslot, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        sync(ctx);
+    }
+    jacobi_init_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, Q, vh, buf1);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+    // the array keeps the previous call's control words: clear them
+    DFT_CUDA(cudaMemsetAsync(ctrl, 0, sizeof(JacobiCtrl), ctx->stream));
+    if (max_sweeps == 0 || g.nx < 3 || g.ny < 3 || g.nz < 3) {
+        sync(ctx);
+        return {max_sweeps == 0 ? 0L : 1L, 0.0};
+    }
+    const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
+    dim3 block(JB_X, JB_Y);
+    const int bx = (g.nx + JB_X - 1) / JB_X, by = (g.ny + JB_Y - 1) / JB_Y;
+    int zc = 32;
+    while (zc > 4 && (long long)bx * by * ((g.nz + zc - 1) / zc) < 2LL * ctx->num_sms) zc >>= 1;
+    dim3 grid(bx, by, (g.nz + zc - 1) / zc);
+    JacobiCtrl hc;
+    long launched = 0, batch = 32;
+    while (true) {
+        const long nb = std::min<long>(batch, max_sweeps - launched);
+        for (long s = 0; s < nb; ++s)
+            jacobi_sweep_kernel<<<grid, block, 0, ctx->stream>>>(g, rho, vh, buf1, ctrl, den, tol, max_sweeps, zc);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx, nb);
+        launched += nb;
+        DFT_CUDA(cudaMemcpyAsync(&hc, ctrl, sizeof(JacobiCtrl), cudaMemcpyDeviceToHost, ctx->stream));
+        sync(ctx);
+        if (hc.done || launched >= max_sweeps) break;
+        batch = std::min<long>(batch * 2, 512);
+    }
+    const long sweeps = (long)hc.sweep;
+    if (sweeps & 1)
+        DFT_CUDA(cudaMemcpyAsync(vh, buf1, sizeof(double) * (size_t)g.N, cudaMemcpyDeviceToDevice, ctx->stream));
+    sync(ctx);
+    return {sweeps, hc.last_diff};
 }
 
 // =============================================================== XC ==================

@@ -18,6 +18,9 @@ struct JacobiResult {
     double last_diff;
 };
 JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol, long max_sweeps);
+// The same solve on the library's fixed scratch array: no device allocation (grid_ops.cu).
+JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol,
+                             long max_sweeps);
 
 // rho = a + b
 void add2(dft_context* ctx, long long n, const double* a, const double* b, double* out);

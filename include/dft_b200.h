@@ -84,6 +84,21 @@ dft_status_t dft_apply_hamiltonian_dev(dft_context* ctx, const dft_grid* g, cons
 dft_status_t dft_hartree_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
                              long max_sweeps, long* sweeps_out, double* last_diff_out);
 
+/* The Hartree solve of dft_hartree_dev (same arguments, same bit-identical results) for
+ * callers that cannot let a library allocate device memory: applications whose own pooled
+ * allocator owns the device memory budget, or plugins running inside such an
+ * application's compute step, where cudaMalloc/cudaFree would also stall the device.
+ * This entry point calls no cudaMalloc, cudaFree or other allocating routine; its scratch
+ * (the second Jacobi iterate and the control words) is a fixed array compiled into the
+ * library, so every GPU that loads the library holds 16 MiB + 128 B until the process
+ * exits.  Limit: nx*ny*nz <= 2,097,152 points (128^3); larger grids are rejected with
+ * DFT_INVALID_ARGUMENT.  The first call on each device looks up the array's device
+ * address (once, with that device current); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (several streams or
+ * contexts on one device at once) race on it.  No counterpart in the reference. */
+dft_status_t dft_hartree_noalloc_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
+                                     long max_sweeps, long* sweeps_out, double* last_diff_out);
+
 /* calculateHartreeEnergy (reference HartreePotentialMolecule.cpp:326-379): 1/2 sum rho V dV. */
 dft_status_t dft_hartree_energy_dev(dft_context* ctx, const dft_grid* g, const double* rho, const double* vh,
                                     double* energy_out);
