@@ -85,6 +85,7 @@ _SIGS = {
     "dft_context_create": ([C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "dft_context_destroy": ([_P], C.c_int),
     "dft_context_synchronize": ([_P], C.c_int),
+    "dft_context_set_tuning": ([_P, C.c_char_p, C.c_long], C.c_int),
     "dft_context_stream": ([_P], C.c_void_p),
     "dft_context_launch_count": ([_P], C.c_longlong),
     "dft_device_alloc": ([_P, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
@@ -292,6 +293,9 @@ class Engine:
 
     def synchronize(self):
         _check(load().dft_context_synchronize(self.ctx))
+
+    def set_tuning(self, key: str, value: int):
+        _check(load().dft_context_set_tuning(self.ctx, key.encode(), int(value)))
 
     @property
     def stream(self) -> int:

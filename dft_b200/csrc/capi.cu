@@ -119,6 +119,20 @@ dft_status_t dft_context_synchronize(dft_context* ctx) {
     });
 }
 
+dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long value) {
+    return guard(ctx, [&] {
+        NEED(ctx && key, "NULL argument");
+        const std::string k(key);
+        if (k == "jacobi_sweeps_per_launch") {
+            NEED(value == 0 || value == 1 || value == 2 || value == 4 || value == 8,
+                 "jacobi_sweeps_per_launch must be 0 (auto), 1, 2, 4 or 8");
+            ctx->jacobi_sweeps_per_launch = (int)value;
+        } else {
+            dftb::fail(DFT_INVALID_ARGUMENT, "unknown tuning key '%s'", key);
+        }
+    });
+}
+
 void* dft_context_stream(dft_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 long long dft_context_launch_count(dft_context* ctx) { return ctx ? ctx->launches : 0; }
 

@@ -93,6 +93,8 @@ struct dft_context {
     cudaStream_t stream = nullptr;
     long long launches = 0;
     int num_sms = 148;
+    // tuning knobs (dft_context_set_tuning)
+    int jacobi_sweeps_per_launch = 0;  // 0 = auto, 1 = one sweep per launch, 2/4/8 = temporal blocking
     // named scratch buffers (reductions, Jacobi ping-pong, XC intermediates, Davidson)
     dftb::Workspace ws[24];
     double* host_pinned = nullptr;  // small pinned staging area for scalars

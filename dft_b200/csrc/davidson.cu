@@ -108,13 +108,17 @@ __global__ void __launch_bounds__(GRAM_THREADS) gram_kernel(const double* __rest
     if (i1 < ka && j1 < kb) out[(long long)i1 * kb + j1] = acc11;
 }
 
-// out[e] = scale * sum_c partial[c][e], fixed chunk order
+// out[e] = scale * sum_c partial[c][e]: one warp per element, lanes stride the chunks, fixed
+// shuffle order (deterministic)
 __global__ void gram_reduce_kernel(int nchunks, int nel, const double* __restrict__ partial, double scale,
                                    double* __restrict__ out) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    for (int e = blockIdx.x * warps + (threadIdx.x >> 5); e < nel; e += gridDim.x * warps) {
         double s = 0.0;
-        for (int c = 0; c < nchunks; ++c) s += partial[(long long)c * nel + e];
-        out[e] = s * scale;
+        for (int c = lane; c < nchunks; c += 32) s += partial[(long long)c * nel + e];
+        s = warp_sum(s);
+        if (lane == 0) out[e] = s * scale;
     }
 }
 
@@ -224,7 +228,7 @@ void gram(dft_context* ctx, const Grid& g, const double* A, long long lda, int k
     gram_kernel<<<dim3(tx, ty, (unsigned)nch), GRAM_THREADS, 0, ctx->stream>>>(A, lda, ka, B, ldb, kb, g.N, chunk,
                                                                                partial);
     DFT_LAUNCH_CHECK();
-    const int rb = (int)std::min<size_t>((nel + 255) / 256, 1024);
+    const int rb = (int)std::min<size_t>((nel + 7) / 8, 4096);  // 8 warps per block, one element per warp
     gram_reduce_kernel<<<rb, 256, 0, ctx->stream>>>((int)nch, (int)nel, partial, g.dV, res);
     DFT_LAUNCH_CHECK();
     count_launch(ctx, 2);
@@ -302,14 +306,19 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
     if (nbands > g.N) fail(DFT_INVALID_ARGUMENT, "more bands than grid points");
     if (ld < g.N) fail(DFT_INVALID_ARGUMENT, "ld must be >= nx*ny*nz");
     const int nb = nbands;
-    const int kmax = (int)std::max<long long>(2LL * nb, std::min<long long>(o.max_subspace * (long long)nb, g.N));
+    // basis cap: max_subspace x nbands, and at least nbands + 16 (the reference's subspace of 16);
+    // a restart keeps the lowest kr Ritz vectors (thick restart)
+    long long km = std::max<long long>(o.max_subspace * (long long)nb, nb + 16LL);
+    km = std::max<long long>(km, 2LL * nb);
+    const int kmax = (int)std::min<long long>(km, g.N);
+    const int kr = std::max(nb, std::min(kmax - 1, kmax / 2));
     const size_t vecb = sizeof(double) * (size_t)ld;
     double* Vb = (double*)ws_get(ctx, WS_DAV0, vecb * kmax);
     double* AV = (double*)ws_get(ctx, WS_DAV1, vecb * kmax);
     double* X = (double*)ws_get(ctx, WS_DAV2, vecb * nb);
     double* AX = (double*)ws_get(ctx, WS_DAV3, vecb * nb);
     double* R = (double*)ws_get(ctx, WS_DAV4, vecb * nb);
-    double* W = (double*)ws_get(ctx, WS_DAV5, vecb * std::max(nb, 1));
+    double* W = (double*)ws_get(ctx, WS_DAV5, vecb * std::max(nb, kr));
     const double kin = g.ix2 + g.iy2 + g.iz2;  // buildHamiltonianDiagonal :496-500 (1/dx^2 + 1/dy^2 + 1/dz^2)
     const int eb = std::max(1, std::min((int)((g.N + 255) / 256), ctx->num_sms * 2));
 
@@ -412,12 +421,18 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         if (it == o.max_iterations) break;
         // ---- corrections ------------------------------------------------------------------
         const int na = (int)active.size();
-        if (k + na > kmax) {  // thick restart to the current Ritz block
-            DFT_CUDA(cudaMemcpyAsync(Vb, X, vecb * nb, cudaMemcpyDeviceToDevice, ctx->stream));
-            DFT_CUDA(cudaMemcpyAsync(AV, AX, vecb * nb, cudaMemcpyDeviceToDevice, ctx->stream));
-            k = nb;
+        if (k + na > kmax) {  // thick restart to the lowest kr Ritz vectors
+            const int keep = std::min(k, std::max(nb, std::min(kr, kmax - na)));
+            std::vector<double> Zk((size_t)k * keep);
+            for (int i = 0; i < k; ++i)
+                for (int j = 0; j < keep; ++j) Zk[(size_t)i * keep + j] = Z[(size_t)i * k + j];
+            rotate(ctx, g, Vb, ld, k, Zk, keep, W, ld, 1.0, 0.0);
+            DFT_CUDA(cudaMemcpyAsync(Vb, W, vecb * keep, cudaMemcpyDeviceToDevice, ctx->stream));
+            rotate(ctx, g, AV, ld, k, Zk, keep, W, ld, 1.0, 0.0);
+            DFT_CUDA(cudaMemcpyAsync(AV, W, vecb * keep, cudaMemcpyDeviceToDevice, ctx->stream));
+            k = keep;
             G.assign((size_t)k * k, 0.0);
-            for (int i = 0; i < k; ++i) G[(size_t)i * k + i] = theta[i];
+            for (int i = 0; i < k; ++i) G[(size_t)i * k + i] = w[i];
         }
         double* T = Vb + (long long)k * ld;
         DFT_CUDA(cudaMemcpyAsync(dsrc, active.data(), sizeof(int) * na, cudaMemcpyHostToDevice, ctx->stream));

@@ -174,10 +174,12 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
     long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
     double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
     double cur = __ldg(p + idx);
+    double above = kb + 1 < g.nz ? __ldg(p + idx + sxy) : 0.0;
     const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
     for (int k = kb; k < ke; ++k, idx += sxy) {
         const bool zr = k + 1 < g.nz;
-        const double above = zr ? __ldg(p + idx + sxy) : 0.0;
+        // two planes in flight: fetch k+2 before working on k
+        const double next = (k + 2 < g.nz && k + 1 < ke) ? __ldg(p + idx + 2 * sxy) : 0.0;
         double lap = __dmul_rn(k0, cur);
         if (xl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - 1), g.ix2));
         if (xr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + 1), g.ix2));
@@ -188,6 +190,7 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
         o[idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(__ldg(V + idx), cur));
         below = cur;
         cur = above;
+        above = next;
     }
 }
 
@@ -341,7 +344,214 @@ __global__ void __launch_bounds__(JB_X* JB_Y) jacobi_sweep_kernel(Grid g, const 
     }
 }
 
+// ---- temporally blocked Jacobi: up to TMAX sweeps per launch -----------------------------
+//
+// A block owns a (32-2*TMAX)^2 column tile and a z-chunk of the output and holds a 32 x 32
+// column region (tile + TMAX halo) in shared memory.  It marches z: each step loads one input
+// plane (level 0) and advances every time level t = 1..tsw by one plane (level t computes
+// plane zin - t from the three level-(t-1) planes around it, kept in a 3-plane ring per level).
+// Each level is exactly one Jacobi sweep of the reference (same arithmetic as
+// jacobi_sweep_kernel); halo columns and the z-halo of the chunk are recomputed redundantly
+// and discarded.  Per-level max|dV| over owned points goes to ctrl->level_bits[t]; the last
+// block to finish finds the first level that met the stop rule (or the cap).  If that level
+// is below tsw the host replays the launch from its (untouched) input with fewer levels.
+constexpr int TB_R = 32;  // region edge (columns)
+
+struct JacobiTBCtrl {
+    unsigned long long level_bits[9];  // running max |dV| per level of the launch in flight
+    unsigned int ticket;
+    int done;
+    long long sweep;        // sweeps completed by finished launches
+    long long launches;     // finished launches; the input of launch L is buf[L & 1]
+    int final_level;        // level of the launch that met the stop rule
+    int final_in_parity;    // input parity of that launch
+    double last_diff;
+};
+
+template <int TMAX>
+__global__ void __launch_bounds__(TB_R* TB_R, 1)
+    jacobi_tb_kernel(Grid g, const double* __restrict__ rho, double* buf0, double* buf1, JacobiTBCtrl* ctrl,
+                     double den, double tol, long long cap, int zchunk, int tsw, int replay_parity) {
+    extern __shared__ double ring[];  // [TMAX levels][3 slots][TB_R][TB_R]
+    __shared__ double red[TB_R][TMAX + 1];
+    __shared__ int s_done;
+    __shared__ long long s_sweep, s_launch;
+    const bool replay = replay_parity >= 0;
+    const int rx = threadIdx.x, ry = threadIdx.y, tid = ry * TB_R + rx;
+    if (tid == 0) {
+        if (replay) {
+            s_done = 0;
+            s_launch = replay_parity;
+            s_sweep = 0;
+        } else {
+            s_done = __ldcg(&ctrl->done);
+            s_launch = __ldcg(&ctrl->launches);
+            s_sweep = __ldcg(&ctrl->sweep);
+        }
+    }
+    __syncthreads();
+    if (s_done) return;
+    const double* __restrict__ vin = (s_launch & 1) ? buf1 : buf0;
+    double* __restrict__ vout = (s_launch & 1) ? buf0 : buf1;
+    constexpr int TT = TB_R - 2 * TMAX;  // owned tile edge
+    const int x = (int)blockIdx.x * TT - TMAX + rx;
+    const int y = (int)blockIdx.y * TT - TMAX + ry;
+    const bool in_grid = x >= 0 && x < g.nx && y >= 0 && y < g.ny;
+    const bool edge_col = x == 0 || x == g.nx - 1 || y == 0 || y == g.ny - 1;
+    const bool owned = in_grid && rx >= TMAX && rx < TMAX + TT && ry >= TMAX && ry < TMAX + TT;
+    const int z0 = (int)blockIdx.z * zchunk;
+    const int z1 = min(g.nz, z0 + zchunk);
+    const long long sxy = (long long)g.nx * g.ny;
+    const long long col = (long long)y * g.nx + x;
+    const double c4pi = 4.0 * xcf::PI;
+    constexpr int PL = TB_R * TB_R;
+    auto cell = [&](int level, int z, int dx, int dy) -> double& {
+        return ring[((level * 3 + ((z % 3) + 3) % 3) * PL) + (ry + dy) * TB_R + (rx + dx)];
+    };
+    double md[TMAX + 1];
+#pragma unroll
+    for (int t = 0; t <= TMAX; ++t) md[t] = 0.0;
+    for (int zin = z0 - tsw; zin < z1 + tsw; ++zin) {
+        if (zin >= 0 && zin < g.nz) cell(0, zin, 0, 0) = in_grid ? vin[(long long)zin * sxy + col] : 0.0;
+        __syncthreads();
+#pragma unroll
+        for (int t = 1; t <= TMAX; ++t) {
+            if (t <= tsw) {
+                const int zt = zin - t;
+                const bool active = zt >= 0 && zt < g.nz && zt >= z0 - (tsw - t) && zt < z1 + (tsw - t);
+                if (active) {
+                    const double c = cell(t - 1, zt, 0, 0);
+                    double v = c;
+                    const bool interior = in_grid && !edge_col && zt > 0 && zt < g.nz - 1 && rx > 0 &&
+                                          rx < TB_R - 1 && ry > 0 && ry < TB_R - 1;
+                    if (interior) {
+                        const double sx = __dadd_rn(cell(t - 1, zt, -1, 0), cell(t - 1, zt, 1, 0));
+                        const double sy = __dadd_rn(cell(t - 1, zt, 0, -1), cell(t - 1, zt, 0, 1));
+                        const double sz = __dadd_rn(cell(t - 1, zt - 1, 0, 0), cell(t - 1, zt + 1, 0, 0));
+                        double acc = __dadd_rn(__dmul_rn(g.ix2, sx), __dmul_rn(g.iy2, sy));
+                        acc = __dadd_rn(acc, __dmul_rn(g.iz2, sz));
+                        acc = __dadd_rn(acc, __dmul_rn(c4pi, __ldg(rho + (long long)zt * sxy + col)));
+                        v = __ddiv_rn(acc, den);
+                        if (owned && zt >= z0 && zt < z1) md[t] = fmax(md[t], fabs(v - c));
+                    }
+                    if (t == tsw) {
+                        if (owned && zt >= z0 && zt < z1) vout[(long long)zt * sxy + col] = v;
+                    } else {
+                        cell(t, zt, 0, 0) = v;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (replay) return;
+    // per-level block max -> global per-level max
+#pragma unroll
+    for (int t = 1; t <= TMAX; ++t) {
+        double m = warp_max(md[t]);
+        if (rx == 0) red[ry][t] = m;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int t = 1; t <= tsw; ++t) {
+            double m = 0.0;
+            for (int w = 0; w < TB_R; ++w) m = fmax(m, red[w][t]);
+            atomicMax(&ctrl->level_bits[t], (unsigned long long)__double_as_longlong(m));
+        }
+        __threadfence();
+        const unsigned int total = gridDim.x * gridDim.y * gridDim.z;
+        if (atomicAdd(&ctrl->ticket, 1u) == total - 1) {
+            __threadfence();
+            int fin = 0;
+            double dlast = 0.0;
+            for (int t = 1; t <= tsw; ++t) {
+                const double d = __longlong_as_double((long long)atomicExch(&ctrl->level_bits[t], 0ull));
+                if (!fin) {
+                    dlast = d;
+                    if (d < tol || s_sweep + t >= cap) fin = t;
+                }
+            }
+            ctrl->ticket = 0;
+            ctrl->last_diff = dlast;
+            if (fin) {
+                ctrl->done = 1;
+                ctrl->final_level = fin;
+                ctrl->final_in_parity = (int)(s_launch & 1);
+                ctrl->sweep = s_sweep + fin;
+            } else {
+                ctrl->sweep = s_sweep + tsw;
+            }
+            ctrl->launches = s_launch + 1;
+            __threadfence();
+        }
+    }
+}
+
 }  // namespace
+
+// Jacobi with up to `tmax` sweeps per launch (2, 4 or 8), bit-identical to the one-sweep path.
+static JacobiResult hartree_tb(dft_context* ctx, const Grid& g, const double* rho, double* vh, double* buf1,
+                               double tol, long max_sweeps, int tmax) {
+    JacobiTBCtrl* ctrl = (JacobiTBCtrl*)ws_get(ctx, WS_CTRL, sizeof(JacobiTBCtrl) + 64);
+    DFT_CUDA(cudaMemsetAsync(ctrl, 0, sizeof(JacobiTBCtrl), ctx->stream));
+    const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
+    const int tt = TB_R - 2 * tmax;
+    const int bx = (g.nx + tt - 1) / tt, by = (g.ny + tt - 1) / tt;
+    int zc = 64;
+    while (zc > 8 && (long long)bx * by * ((g.nz + zc - 1) / zc) < 2LL * ctx->num_sms) zc >>= 1;
+    zc = std::max(zc, std::min(g.nz, 2 * tmax));
+    dim3 grid(bx, by, (g.nz + zc - 1) / zc), block(TB_R, TB_R);
+    const size_t smem = sizeof(double) * (size_t)tmax * 3 * TB_R * TB_R;
+    auto launch = [&](int tsw, int replay_parity) {
+        if (tmax == 2)
+            jacobi_tb_kernel<2><<<grid, block, smem, ctx->stream>>>(g, rho, vh, buf1, ctrl, den, tol, max_sweeps, zc,
+                                                                    tsw, replay_parity);
+        else if (tmax == 4)
+            jacobi_tb_kernel<4><<<grid, block, smem, ctx->stream>>>(g, rho, vh, buf1, ctrl, den, tol, max_sweeps, zc,
+                                                                    tsw, replay_parity);
+        else
+            jacobi_tb_kernel<8><<<grid, block, smem, ctx->stream>>>(g, rho, vh, buf1, ctrl, den, tol, max_sweeps, zc,
+                                                                    tsw, replay_parity);
+    };
+    static bool attr[3] = {false, false, false};
+    const int ai = tmax == 2 ? 0 : (tmax == 4 ? 1 : 2);
+    if (!attr[ai]) {
+        if (tmax == 2)
+            DFT_CUDA(cudaFuncSetAttribute(jacobi_tb_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        else if (tmax == 4)
+            DFT_CUDA(cudaFuncSetAttribute(jacobi_tb_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        else
+            DFT_CUDA(cudaFuncSetAttribute(jacobi_tb_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr[ai] = true;
+    }
+    JacobiTBCtrl* hc = (JacobiTBCtrl*)pinned(ctx, (sizeof(JacobiTBCtrl) + 7) / 8);
+    long sweeps_launched = 0, batch = 8;
+    while (true) {
+        long nl = 0;
+        while (nl < batch && sweeps_launched < max_sweeps) {
+            launch(tmax, -1);
+            sweeps_launched += tmax;
+            ++nl;
+        }
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx, nl);
+        DFT_CUDA(cudaMemcpyAsync(hc, ctrl, sizeof(JacobiTBCtrl), cudaMemcpyDeviceToHost, ctx->stream));
+        sync(ctx);
+        if (hc->done || sweeps_launched >= max_sweeps) break;
+        batch = std::min<long>(batch * 2, 256);
+    }
+    if (!hc->done) fail(DFT_CAP_REACHED, "Jacobi control state inconsistent");
+    int out_parity = hc->final_in_parity ^ 1;  // the output buffer of the final launch
+    if (hc->final_level < tmax) {
+        // the stop rule fired inside the launch: recompute from its input with fewer levels
+        launch(hc->final_level, hc->final_in_parity);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+    }
+    if (out_parity == 1)
+        DFT_CUDA(cudaMemcpyAsync(vh, buf1, sizeof(double) * (size_t)g.N, cudaMemcpyDeviceToDevice, ctx->stream));
+    return {(long)hc->sweep, hc->last_diff};
+}
 
 JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol, long max_sweeps) {
     if (max_sweeps < 0) fail(DFT_INVALID_ARGUMENT, "max_sweeps must be >= 0");
@@ -371,6 +581,10 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
         // no interior: the reference still runs its sweep loop, finds max|dV| = 0 < tol and stops
         return {max_sweeps == 0 ? 0L : 1L, 0.0};
     }
+    // sweeps per launch: temporal blocking by default (8 on grids up to 80^3 points, else 4)
+    int tmax = ctx->jacobi_sweeps_per_launch;
+    if (tmax == 0) tmax = g.N <= 80LL * 80 * 80 ? 8 : 4;
+    if (tmax == 2 || tmax == 4 || tmax == 8) return hartree_tb(ctx, g, rho, vh, buf1, tol, max_sweeps, tmax);
     const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
     dim3 block(JB_X, JB_Y);
     const int bx = (g.nx + JB_X - 1) / JB_X, by = (g.ny + JB_Y - 1) / JB_Y;

@@ -79,8 +79,16 @@ def test_hpsi_large_numpy_restatement(engine):
         assert np.array_equal(H[band], ref.ravel())
 
 
-@pytest.mark.parametrize("n,b", GRIDS[:3] + [((24, 24, 24), (-6.0, 6.0) * 3)])
-def test_jacobi_bit_exact_and_sweeps(engine, port, n, b):
+@pytest.fixture(params=[0, 1, 2, 4, 8], ids=lambda t: f"spl{t}")
+def sweeps_per_launch(request, engine):
+    """Every Jacobi launch shape (one sweep per launch, temporal blocks of 2/4/8, auto)."""
+    engine.set_tuning("jacobi_sweeps_per_launch", request.param)
+    yield request.param
+    engine.set_tuning("jacobi_sweeps_per_launch", 0)
+
+
+@pytest.mark.parametrize("n,b", GRIDS[:3] + [((24, 24, 24), (-6.0, 6.0) * 3), ((40, 37, 70), (-6.0, 6.0) * 3)])
+def test_jacobi_bit_exact_and_sweeps(engine, port, n, b, sweeps_per_launch):
     na, nb = gaussian_density(n, b, 2)
     rho = na + nb
     ref = np.empty(rho.size)
@@ -98,13 +106,20 @@ def test_jacobi_bit_exact_and_sweeps(engine, port, n, b):
     assert np.array_equal(d_vh.to_host(), ref)
 
 
-def test_jacobi_cap(engine, port):
-    """The silent sweep cap (HartreePotentialMolecule.cpp:207): stop after max_sweeps."""
+def test_jacobi_cap(engine, port, sweeps_per_launch):
+    """The silent sweep cap (HartreePotentialMolecule.cpp:207): stop after max_sweeps, with the
+    iterate of exactly that sweep (37 is not a multiple of any block size)."""
     n, b = (24, 24, 24), (-6.0, 6.0) * 3
     na, nb = gaussian_density(n, b, 4)
     d_rho, d_vh = engine.upload(na + nb), engine.array(na.size)
     sweeps, last = engine.hartree(G(n, b), d_rho, d_vh, tol=1e-8, max_sweeps=37)
     assert sweeps == 37 and last > 1e-8
+    v37 = d_vh.to_host()
+    engine.set_tuning("jacobi_sweeps_per_launch", 1)
+    ref = engine.array(na.size)
+    engine.hartree(G(n, b), d_rho, ref, tol=1e-8, max_sweeps=37)
+    assert np.array_equal(v37, ref.to_host())
+    engine.set_tuning("jacobi_sweeps_per_launch", sweeps_per_launch)
     sweeps0, _ = engine.hartree(G(n, b), d_rho, d_vh, tol=1e-8, max_sweeps=0)
     assert sweeps0 == 0
 
@@ -175,9 +190,9 @@ def test_xc_evaluate_pointwise(engine, port, kind):
     engine.xc_evaluate(kind, m, engine.upload(na), engine.upload(nb), engine.upload(ga), engine.upload(gb), out)
     got = out.to_host((m, 5))
     want = port.xc_evaluate(kind, na, nb, ga, gb)
-    # per column, relative to the column's magnitude at that density scale
-    err = np.abs(got - want) / np.maximum(np.abs(want), 1e-12 * np.max(np.abs(want), axis=0))
-    assert np.max(err) < 1e-11
+    # |got - want| <= 1e-11 |want| + 1e-15 max|column| (the absolute term covers cancellations)
+    colmax = np.max(np.abs(want), axis=0)
+    assert np.all(np.abs(got - want) <= 1e-11 * np.abs(want) + 1e-15 * colmax)
 
 
 def test_density_kinetic_bit_and_tol(engine, port):
