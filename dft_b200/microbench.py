@@ -51,10 +51,12 @@ def main():
     ap.add_argument("--sweeps", type=int, default=10000)
     ap.add_argument("--iterations", type=int, default=1)
     ap.add_argument("--functional", default="PBE96")
+    ap.add_argument("--spl", type=int, default=0, help="Jacobi sweeps per launch (0 = auto)")
     a = ap.parse_args()
     import torch
 
     eng = d.Engine(0)
+    eng.set_tuning("jacobi_sweeps_per_launch", a.spl)
     stream = torch.cuda.ExternalStream(eng.stream)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     out = {"mode": a.mode}
@@ -81,7 +83,7 @@ def main():
         t = _events(torch, stream, run, a.reps)
         ms = statistics.median(t)
         interior = (a.n - 2) ** 3
-        out.update(n=a.n, sweeps=res["s"], ms=ms, us_per_sweep=1e3 * ms / res["s"],
+        out.update(n=a.n, spl=a.spl, sweeps=res["s"], ms=ms, us_per_sweep=1e3 * ms / res["s"],
                    gbs=24.0 * interior * res["s"] / (ms * 1e-3) / 1e9)
     elif a.mode == "xc":
         g = cube(a.n, a.h)
