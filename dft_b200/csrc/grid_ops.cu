@@ -174,12 +174,10 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
     long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
     double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
     double cur = __ldg(p + idx);
-    double above = kb + 1 < g.nz ? __ldg(p + idx + sxy) : 0.0;
     const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
     for (int k = kb; k < ke; ++k, idx += sxy) {
         const bool zr = k + 1 < g.nz;
-        // two planes in flight: fetch k+2 before working on k
-        const double next = (k + 2 < g.nz && k + 1 < ke) ? __ldg(p + idx + 2 * sxy) : 0.0;
+        const double above = zr ? __ldg(p + idx + sxy) : 0.0;
         double lap = __dmul_rn(k0, cur);
         if (xl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - 1), g.ix2));
         if (xr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + 1), g.ix2));
@@ -190,7 +188,6 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
         o[idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(__ldg(V + idx), cur));
         below = cur;
         cur = above;
-        above = next;
     }
 }
 
@@ -409,10 +406,21 @@ __global__ void __launch_bounds__(TB_R* TB_R, 1)
         return ring[((level * 3 + ((z % 3) + 3) % 3) * PL) + (ry + dy) * TB_R + (rx + dx)];
     };
     double md[TMAX + 1];
+    double rr[TMAX + 1];  // rr[t] = rho of this column at plane zin - t (level t's source term)
 #pragma unroll
-    for (int t = 0; t <= TMAX; ++t) md[t] = 0.0;
+    for (int t = 0; t <= TMAX; ++t) md[t] = rr[t] = 0.0;
+    auto load = [&](const double* f, int z) -> double {
+        return (in_grid && z >= 0 && z < g.nz) ? __ldg(f + (long long)z * sxy + col) : 0.0;
+    };
+    // one plane of V and of rho are fetched a step ahead, so their latency overlaps the levels
+    double vpre = load(vin, z0 - tsw), rpre = 0.0;
     for (int zin = z0 - tsw; zin < z1 + tsw; ++zin) {
-        if (zin >= 0 && zin < g.nz) cell(0, zin, 0, 0) = in_grid ? vin[(long long)zin * sxy + col] : 0.0;
+#pragma unroll
+        for (int t = TMAX; t >= 2; --t) rr[t] = rr[t - 1];
+        rr[1] = rpre;
+        if (zin >= 0 && zin < g.nz) cell(0, zin, 0, 0) = vpre;
+        vpre = load(vin, zin + 1);
+        rpre = load(rho, zin);
         __syncthreads();
 #pragma unroll
         for (int t = 1; t <= TMAX; ++t) {
@@ -430,7 +438,7 @@ __global__ void __launch_bounds__(TB_R* TB_R, 1)
                         const double sz = __dadd_rn(cell(t - 1, zt - 1, 0, 0), cell(t - 1, zt + 1, 0, 0));
                         double acc = __dadd_rn(__dmul_rn(g.ix2, sx), __dmul_rn(g.iy2, sy));
                         acc = __dadd_rn(acc, __dmul_rn(g.iz2, sz));
-                        acc = __dadd_rn(acc, __dmul_rn(c4pi, __ldg(rho + (long long)zt * sxy + col)));
+                        acc = __dadd_rn(acc, __dmul_rn(c4pi, rr[t]));
                         v = __ddiv_rn(acc, den);
                         if (owned && zt >= z0 && zt < z1) md[t] = fmax(md[t], fabs(v - c));
                     }

