@@ -52,6 +52,9 @@ def main():
     ap.add_argument("--iterations", type=int, default=1)
     ap.add_argument("--functional", default="PBE96")
     ap.add_argument("--spl", type=int, default=0, help="Jacobi sweeps per launch (0 = auto)")
+    ap.add_argument("--system", default="h2_48", help="scf mode: h2_48, h2o_128, cluster20")
+    ap.add_argument("--stop-abs-de", type=float, default=0.0)
+    ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args()
     import torch
 
@@ -98,13 +101,22 @@ def main():
         out.update(n=a.n, functional=a.functional, ms=ms, gpoints_per_s=N / (ms * 1e-3) / 1e9,
                    gbs=32.0 * N / (ms * 1e-3) / 1e9)
     elif a.mode == "scf":
-        g = cube(a.n, 0.3 if a.n == 48 else a.h)
+        from dft_b200 import systems
+        w = systems.get(a.system)
+        g = d.CartesianGrid(*w["n"], *w["bounds"])
         m = d.Molecule()
-        m.addNucleus(1, -0.7, 0, 0)
-        m.addNucleus(1, 0.7, 0, 0)
-        o = d.default_scf_options(max_iterations=a.iterations, extra_bands=3)
-        r = eng.scf_molecule(g, m, 0, 1, "PZ81", o)
-        out.update(n=a.n, iterations=r.iterations, energy=r.total, seconds=r.seconds, launches=eng.launches)
+        for z, p in zip(w["Z"], w["xyz"]):
+            m.addNucleus(z, *p)
+        o = d.default_scf_options(max_iterations=a.iterations, extra_bands=w["extra_bands"], verbose=int(a.verbose),
+                                  stop_abs_de=a.stop_abs_de)
+        o.eig.verbose = int(a.verbose > 1)
+        r = eng.scf_molecule(g, m, 0, w["multiplicity"], w["functional"], o)
+        out.update(system=a.system, iterations=r.iterations, converged=r.converged, energy=r.total,
+                   seconds=r.seconds, launches=eng.launches, eigenvalues=r.eigenvalues[:8],
+                   history=[{k: h[k] for k in ("iteration", "energy", "energy_difference", "density_difference",
+                                               "ks_residual", "poisson_sweeps_in", "poisson_sweeps_out",
+                                               "eig_iterations_alpha", "ms_hartree", "ms_xc", "ms_orbitals",
+                                               "ms_density", "ms_energy", "ms_total")} for h in r.history])
     elif a.mode == "radial":
         Zs = list(range(1, 31)) * 2
         ks = ["PZ81"] * 30 + ["PBE96"] * 30

@@ -1,0 +1,63 @@
+"""The benchmark systems (synthetic inputs, seeded), shared by bench.py and microbench.
+
+h2_48        H2, Z=1 at +-0.7 bohr on x, 48^3 grid, h = 0.3, centred box, PZ81, multiplicity 1
+h2o_128      H2O (O at the origin, O-H 1.81 bohr, HOH 104.5 deg), 128^3 grid, h = 0.2, PBE96,
+             multiplicity 1, 5 occupied + 7 extra bands
+cluster20    20 nuclei with Z drawn from {1, 6, 7, 8}, positions uniform in a 24-bohr cube centred
+             in a 192^3 grid (h = 0.2), minimum separation 2.0 bohr, no nucleus within 1e-12 of a
+             node, neutral, multiplicity 1 + (N_e mod 2), PBE96 (seeded numpy generator)
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def _cube(n, h):
+    half = round(0.5 * h * (n - 1), 10)  # e.g. 12.7 for 128 points at h = 0.2
+    return (n, n, n), (-half, half) * 3
+
+
+def h2_48():
+    n, b = (48, 48, 48), (-7.05, 7.05) * 3
+    return dict(name="h2_48", n=n, bounds=b, Z=[1, 1], xyz=[[-0.7, 0.0, 0.0], [0.7, 0.0, 0.0]], multiplicity=1,
+                functional="PZ81", extra_bands=3,
+                desc="H2 PZ81 48^3 h=0.3, 1a+1b (multiplicity 1), 4 bands/spin")
+
+
+def h2o_128(n=128, h=0.2):
+    ang = math.radians(104.5 / 2)
+    x, z = 1.81 * math.sin(ang), 1.81 * math.cos(ang)
+    grid_n, b = _cube(n, h)
+    return dict(name=f"h2o_{n}", n=grid_n, bounds=b, Z=[8, 1, 1], xyz=[[0.0, 0.0, 0.0], [x, 0.0, z], [-x, 0.0, z]],
+                multiplicity=1, functional="PBE96", extra_bands=7,
+                desc=f"H2O PBE96 {n}^3 h={h}, multiplicity 1, 5 occupied + 7 extra bands")
+
+
+def cluster(natoms=20, n=192, h=0.2, box=24.0, min_sep=2.0, seed=20261203, extra_bands=8):
+    rng = np.random.default_rng(seed)
+    grid_n, b = _cube(n, h)
+    lo = b[0]
+    Z, xyz = [], []
+    while len(Z) < natoms:
+        p = rng.uniform(-0.5 * box, 0.5 * box, 3)
+        if any(np.linalg.norm(p - q) < min_sep for q in xyz):
+            continue
+        # keep nuclei off grid nodes (the nuclear potential is singular there)
+        f = (p - lo) / h
+        if np.any(np.abs(f - np.round(f)) * h < 1e-12):
+            continue
+        xyz.append(p)
+        Z.append(int(rng.choice([1, 6, 7, 8])))
+    ne = sum(Z)
+    return dict(name=f"cluster{natoms}_{n}", n=grid_n, bounds=b, Z=Z, xyz=[list(map(float, p)) for p in xyz],
+                multiplicity=1 + (ne % 2), functional="PBE96", extra_bands=extra_bands,
+                desc=f"{natoms}-atom cluster (Z in {{1,6,7,8}}, seed {seed}), {ne} electrons, PBE96 {n}^3 h={h}")
+
+
+SYSTEMS = {"h2_48": h2_48, "h2o_128": h2o_128, "cluster20": cluster}
+
+
+def get(name, **kw):
+    return SYSTEMS[name](**kw)
