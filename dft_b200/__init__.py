@@ -36,7 +36,8 @@ class dft_grid(C.Structure):
 
 
 class dft_eig_opts(C.Structure):
-    _fields_ = [("tol", C.c_double), ("max_iterations", C.c_int), ("max_subspace", C.c_int), ("verbose", C.c_int)]
+    _fields_ = [("tol", C.c_double), ("max_iterations", C.c_int), ("max_subspace", C.c_int), ("verbose", C.c_int),
+                ("preconditioner", C.c_int)]
 
 
 class dft_scf_opts(C.Structure):
@@ -360,10 +361,10 @@ class Engine:
                                                 _dp(xyz), _ptr(vext)))
 
     def solve_orbitals(self, grid, V, nocc, nbands, psi, ld, init=False, tol=1e-7, max_iterations=2000,
-                       max_subspace=3, verbose=False):
+                       max_subspace=3, verbose=False, preconditioner=4):
         g = grid.c()
         eig = np.zeros(nbands)
-        o = dft_eig_opts(tol, max_iterations, max_subspace, int(verbose))
+        o = dft_eig_opts(tol, max_iterations, max_subspace, int(verbose), int(preconditioner))
         it = C.c_int()
         _check(load().dft_solve_orbitals_dev(self.ctx, C.byref(g), _ptr(V), nocc, nbands, _ptr(psi), ld, int(init),
                                              _dp(eig), C.byref(o), C.byref(it)))

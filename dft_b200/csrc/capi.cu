@@ -124,8 +124,8 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
         NEED(ctx && key, "NULL argument");
         const std::string k(key);
         if (k == "jacobi_sweeps_per_launch") {
-            NEED(value == 0 || value == 1 || value == 2 || value == 4 || value == 8,
-                 "jacobi_sweeps_per_launch must be 0 (auto), 1, 2, 4 or 8");
+            NEED(value == 0 || value == -1 || value == 1 || value == 2 || value == 4 || value == 8,
+                 "jacobi_sweeps_per_launch must be 0 (auto), -1 (persistent), 1, 2, 4 or 8");
             ctx->jacobi_sweeps_per_launch = (int)value;
         } else {
             dftb::fail(DFT_INVALID_ARGUMENT, "unknown tuning key '%s'", key);
@@ -271,6 +271,7 @@ dft_status_t dft_solve_orbitals_dev(dft_context* ctx, const dft_grid* g, const d
             if (opts->tol > 0) o.tol = opts->tol;
             if (opts->max_iterations > 0) o.max_iterations = opts->max_iterations;
             if (opts->max_subspace >= 2) o.max_subspace = opts->max_subspace;
+            o.precond_steps = opts->preconditioner;
             o.verbose = opts->verbose;
         }
         const int it = dftb::solve_orbitals(ctx, G, V, nocc, nbands, psi, ld, init != 0, eig, nullptr, o);
@@ -293,6 +294,7 @@ void dft_scf_default_options(dft_scf_opts* o) {
     o->eig.max_iterations = 2000;
     o->eig.max_subspace = 3;
     o->eig.verbose = 0;
+    o->eig.preconditioner = 4;
     o->verbose = 0;
 }
 

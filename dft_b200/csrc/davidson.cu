@@ -191,6 +191,45 @@ __global__ void precond_kernel(const double* __restrict__ R, const double* __res
     }
 }
 
+// Kinetic preconditioner step: one damped-Jacobi step for (T + sigma_a) t = r_a, T = -1/2 lap_h
+// with psi = 0 outside the box.  out = (1-w) t + w (r + 1/2 S(t)) / (kin + sigma_a), where S is
+// the weighted sum of the six neighbours; t == nullptr means t = 0 (then out = w r / d).
+// Smooths the high-frequency (large kinetic energy) part of the residual, which the reference's
+// diagonal preconditioner leaves almost untouched on fine grids.
+__global__ void __launch_bounds__(256) kinetic_smooth_kernel(Grid g, const double* __restrict__ t,
+                                                             const double* __restrict__ R, const int* __restrict__ src,
+                                                             const double* __restrict__ sigma, double* __restrict__ out,
+                                                             long long ld, int zchunk, int nzc, double w) {
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 8 + threadIdx.y;
+    const int a = blockIdx.z / nzc;
+    const int kc = blockIdx.z - a * nzc;
+    if (i >= g.nx || j >= g.ny) return;
+    const double* __restrict__ r = R + (long long)src[a] * ld;
+    const double* __restrict__ tp = t ? t + (long long)a * ld : nullptr;
+    double* __restrict__ o = out + (long long)a * ld;
+    const double d = g.ix2 + g.iy2 + g.iz2 + sigma[a];
+    const long long sxy = (long long)g.nx * g.ny;
+    const int kb = kc * zchunk, ke = min(g.nz, kb + zchunk);
+    long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
+    if (!tp) {
+        for (int k = kb; k < ke; ++k, idx += sxy) o[idx] = w * r[idx] / d;
+        return;
+    }
+    double below = kb > 0 ? tp[idx - sxy] : 0.0, cur = tp[idx];
+    for (int k = kb; k < ke; ++k, idx += sxy) {
+        const double above = k + 1 < g.nz ? tp[idx + sxy] : 0.0;
+        double s = g.iz2 * (below + above);
+        if (i > 0) s += g.ix2 * tp[idx - 1];
+        if (i + 1 < g.nx) s += g.ix2 * tp[idx + 1];
+        if (j > 0) s += g.iy2 * tp[idx - g.nx];
+        if (j + 1 < g.ny) s += g.iy2 * tp[idx + g.nx];
+        o[idx] = (1.0 - w) * cur + w * (r[idx] + 0.5 * s) / d;
+        below = cur;
+        cur = above;
+    }
+}
+
 __global__ void rows_sum_kernel2(int nrows, int ncols, const double* partial, double* out) {
     __shared__ double sh[32];
     for (int r = 0; r < nrows; ++r) {
@@ -371,8 +410,9 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
     };
     grow_G(0, k);
 
-    double* dtheta = (double*)ws_get(ctx, WS_DAV6, sizeof(double) * nb + sizeof(int) * nb + 64);
-    int* dsrc = (int*)(dtheta + nb);
+    double* dtheta = (double*)ws_get(ctx, WS_DAV6, sizeof(double) * 2 * nb + sizeof(int) * nb + 64);
+    double* dsigma = dtheta + nb;
+    int* dsrc = (int*)(dsigma + nb);
     std::vector<double> theta(nb), rn(nb), w, Z, Y;
     std::vector<int> active;
     int it = 0;
@@ -404,7 +444,8 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         for (int b = 0; b < nb; ++b) {
             rn[b] = std::isfinite(hs[b]) ? std::sqrt(hs[b] * g.dV) : INFINITY;
             if (!std::isfinite(rn[b])) fail(DFT_NUMERICAL, "non-finite residual in band %d", b);
-            const double tb = b < nocc ? o.tol : std::max(o.tol, 1e-4);
+            // buffer bands only need to stay ahead of the occupied ones
+            const double tb = b < nocc ? o.tol : std::max(o.tol, 1e-3);
             if (b < nocc && !(rn[b] < o.tol)) occ_conv = false;
             if (!(rn[b] < tb)) active.push_back(b);
         }
@@ -436,9 +477,35 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         }
         double* T = Vb + (long long)k * ld;
         DFT_CUDA(cudaMemcpyAsync(dsrc, active.data(), sizeof(int) * na, cudaMemcpyHostToDevice, ctx->stream));
-        precond_kernel<<<dim3(eb, na), 256, 0, ctx->stream>>>(R, V, dsrc, dtheta, T, ld, g.N, kin);
-        DFT_LAUNCH_CHECK();
-        count_launch(ctx);
+        if (o.precond_steps <= 0) {
+            precond_kernel<<<dim3(eb, na), 256, 0, ctx->stream>>>(R, V, dsrc, dtheta, T, ld, g.N, kin);
+            DFT_LAUNCH_CHECK();
+            count_launch(ctx);
+        } else {
+            // (T + sigma_b) t = r_b with sigma_b = max(-theta_b, 1 Ha): the far-field (V ~ 0) form of
+            // (H - theta_b) for bound states; t0 = r/d, then damped-Jacobi steps (w = 2/3)
+            std::vector<double> sig(na);
+            for (int a = 0; a < na; ++a) sig[a] = std::max(-theta[active[a]], 1.0);
+            DFT_CUDA(cudaMemcpyAsync(dsigma, sig.data(), sizeof(double) * na, cudaMemcpyHostToDevice, ctx->stream));
+            int zc = 32;
+            const int sbx = (g.nx + 31) / 32, sby = (g.ny + 7) / 8;
+            while (zc > 4 && (long long)sbx * sby * na * ((g.nz + zc - 1) / zc) < 4LL * ctx->num_sms) zc >>= 1;
+            const int nzc = (g.nz + zc - 1) / zc;
+            if ((long long)na * nzc > 65535) zc = (int)((g.nz + 65535 / na - 1) / (65535 / na)), zc = std::max(zc, 1);
+            const int nzc2 = (g.nz + zc - 1) / zc;
+            dim3 sgrid(sbx, sby, na * nzc2), sblock(32, 8);
+            kinetic_smooth_kernel<<<sgrid, sblock, 0, ctx->stream>>>(g, nullptr, R, dsrc, dsigma, T, ld, zc, nzc2, 1.0);
+            double *cur = T, *nxt = W;
+            for (int s = 0; s < o.precond_steps; ++s) {
+                kinetic_smooth_kernel<<<sgrid, sblock, 0, ctx->stream>>>(g, cur, R, dsrc, dsigma, nxt, ld, zc, nzc2,
+                                                                         2.0 / 3.0);
+                std::swap(cur, nxt);
+            }
+            DFT_LAUNCH_CHECK();
+            count_launch(ctx, 1 + o.precond_steps);
+            if (cur != T)
+                DFT_CUDA(cudaMemcpyAsync(T, cur, vecb * na, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
         int nt = orthonormalise(ctx, g, Vb, k, T, na, ld, W);
         if (nt == 0) {
             // preconditioned directions fell into the basis: fall back to raw residuals

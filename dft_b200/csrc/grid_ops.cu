@@ -495,7 +495,135 @@ __global__ void __launch_bounds__(TB_R* TB_R, 1)
     }
 }
 
+// ---- persistent Jacobi: the whole solve in one cooperative launch --------------------------
+// For small grids the sweep is a few microseconds of work and launch latency dominates.  All
+// blocks stay resident (cooperative launch) and meet at a grid barrier after every sweep;
+// every block reads the same global max|dV| after the barrier, so all stop at the same sweep.
+// Loads of the iterates bypass L1 (__ldcg): other SMs rewrite them every sweep.
+// The barrier wait is bounded: a block that waits longer than ~2^24 polls sets ctrl->error and
+// leaves, and so do the others at their next barrier.
+struct JacobiPCtrl {
+    unsigned long long slot[3];  // per-sweep max |dV| (sweep s uses slot s % 3)
+    unsigned int count;          // grid barrier arrivals
+    unsigned int gen;            // grid barrier generation
+    int error;
+    int pad;
+    long long sweeps;
+    double last_diff;
+};
+
+__device__ __forceinline__ bool grid_barrier(JacobiPCtrl* c, unsigned int nblocks) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        int ok = 1;
+        const unsigned int gen = atomicAdd(&c->gen, 0u);
+        __threadfence();
+        if (atomicAdd(&c->count, 1u) == nblocks - 1) {
+            atomicExch(&c->count, 0u);
+            __threadfence();
+            atomicAdd(&c->gen, 1u);
+        } else {
+            long long polls = 0;
+            while (atomicAdd(&c->gen, 0u) == gen) {
+                if (++polls > (1LL << 24) || atomicAdd(&c->error, 0) != 0) {
+                    atomicExch(&c->error, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(256) jacobi_persistent_kernel(Grid g, const double* __restrict__ rho, double* buf0,
+                                                                double* buf1, JacobiPCtrl* ctrl, double den, double tol,
+                                                                long long cap) {
+    __shared__ double sh[8];
+    __shared__ double s_d;
+    const double c4pi = 4.0 * xcf::PI;
+    const long long sxy = (long long)g.nx * g.ny;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const unsigned int nblocks = gridDim.x;
+    for (long long s = 0; s < cap; ++s) {
+        const double* cur = (s & 1) ? buf1 : buf0;
+        double* nxt = (s & 1) ? buf0 : buf1;
+        double md = 0.0;
+        for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += stride) {
+            const int i = (int)(p % g.nx);
+            const int j = (int)((p / g.nx) % g.ny);
+            const int k = (int)(p / sxy);
+            if (i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz) continue;
+            const double c = __ldcg(cur + p);
+            const double sx = __dadd_rn(__ldcg(cur + p - 1), __ldcg(cur + p + 1));
+            const double sy = __dadd_rn(__ldcg(cur + p - g.nx), __ldcg(cur + p + g.nx));
+            const double sz = __dadd_rn(__ldcg(cur + p - sxy), __ldcg(cur + p + sxy));
+            double acc = __dadd_rn(__dmul_rn(g.ix2, sx), __dmul_rn(g.iy2, sy));
+            acc = __dadd_rn(acc, __dmul_rn(g.iz2, sz));
+            acc = __dadd_rn(acc, __dmul_rn(c4pi, __ldg(rho + p)));
+            const double v = __ddiv_rn(acc, den);
+            __stcg(nxt + p, v);
+            md = fmax(md, fabs(v - c));
+        }
+        md = warp_max(md);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = md;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m = sh[0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sh[w]);
+            atomicMax(&ctrl->slot[s % 3], (unsigned long long)__double_as_longlong(m));
+        }
+        if (!grid_barrier(ctrl, nblocks)) return;
+        if (threadIdx.x == 0) {
+            s_d = __longlong_as_double((long long)atomicAdd(&ctrl->slot[s % 3], 0ull));
+            if (blockIdx.x == 0) atomicExch(&ctrl->slot[(s + 2) % 3], 0ull);  // read by all before barrier s
+        }
+        __syncthreads();
+        const double d = s_d;
+        if (d < tol || s + 1 >= cap) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                ctrl->sweeps = s + 1;
+                ctrl->last_diff = d;
+            }
+            return;
+        }
+    }
+}
+
 }  // namespace
+
+// The whole solve in one cooperative launch (small grids).
+static JacobiResult hartree_persistent(dft_context* ctx, const Grid& g, const double* rho, double* vh, double* buf1,
+                                       double tol, long max_sweeps) {
+    JacobiPCtrl* ctrl = (JacobiPCtrl*)ws_get(ctx, WS_CTRL, sizeof(JacobiPCtrl) + 64);
+    DFT_CUDA(cudaMemsetAsync(ctrl, 0, sizeof(JacobiPCtrl), ctx->stream));
+    int per_sm = 0;
+    DFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_persistent_kernel, 256, 0));
+    const long long want = (g.N + 255) / 256;
+    const int nblocks = (int)std::max<long long>(1, std::min<long long>(want, (long long)per_sm * ctx->num_sms));
+    double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
+    long long cap = max_sweeps;
+    Grid gg = g;
+    const double* r = rho;
+    double* b0 = vh;
+    double* b1 = buf1;
+    void* args[] = {&gg, &r, &b0, &b1, &ctrl, &den, &tol, &cap};
+    DFT_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_persistent_kernel, dim3(nblocks), dim3(256), args, 0,
+                                         ctx->stream));
+    count_launch(ctx);
+    JacobiPCtrl* hc = (JacobiPCtrl*)pinned(ctx, (sizeof(JacobiPCtrl) + 7) / 8);
+    DFT_CUDA(cudaMemcpyAsync(hc, ctrl, sizeof(JacobiPCtrl), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    if (hc->error) fail(DFT_CUDA_ERROR, "Jacobi grid barrier timed out");
+    if (hc->sweeps & 1)
+        DFT_CUDA(cudaMemcpyAsync(vh, buf1, sizeof(double) * (size_t)g.N, cudaMemcpyDeviceToDevice, ctx->stream));
+    return {(long)hc->sweeps, hc->last_diff};
+}
 
 // Jacobi with up to `tmax` sweeps per launch (2, 4 or 8), bit-identical to the one-sweep path.
 static JacobiResult hartree_tb(dft_context* ctx, const Grid& g, const double* rho, double* vh, double* buf1,
@@ -589,9 +717,11 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
         // no interior: the reference still runs its sweep loop, finds max|dV| = 0 < tol and stops
         return {max_sweeps == 0 ? 0L : 1L, 0.0};
     }
-    // sweeps per launch: temporal blocking by default (8 on grids up to 80^3 points, else 4)
+    // launch shape: one persistent launch on small grids (launch-latency bound), one sweep per
+    // launch otherwise; 2/4/8 select the temporally blocked kernel
     int tmax = ctx->jacobi_sweeps_per_launch;
-    if (tmax == 0) tmax = g.N <= 80LL * 80 * 80 ? 8 : 4;
+    if (tmax == 0) tmax = g.N <= 64LL * 64 * 64 ? -1 : 1;
+    if (tmax == -1) return hartree_persistent(ctx, g, rho, vh, buf1, tol, max_sweeps);
     if (tmax == 2 || tmax == 4 || tmax == 8) return hartree_tb(ctx, g, rho, vh, buf1, tol, max_sweeps, tmax);
     const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
     dim3 block(JB_X, JB_Y);

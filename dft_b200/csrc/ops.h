@@ -58,6 +58,7 @@ struct EigOpts {
     int max_iterations = 2000;
     int max_subspace = 3;
     int verbose = 0;
+    int precond_steps = 4;  // 0 = the reference's diagonal preconditioner
 };
 int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, int nbands, double* psi,
                    long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o);

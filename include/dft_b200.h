@@ -58,7 +58,8 @@ dft_status_t dft_context_create(int device, dft_context** out);
 dft_status_t dft_context_destroy(dft_context* ctx);
 dft_status_t dft_context_synchronize(dft_context* ctx);
 /* Kernel-shape knobs (results do not depend on them).  Keys:
- *   "jacobi_sweeps_per_launch": 0 = auto (default), 1 = one Jacobi sweep per launch,
+ *   "jacobi_sweeps_per_launch": 0 = auto (default), -1 = the whole solve in one persistent
+ *                               (cooperative) launch, 1 = one Jacobi sweep per launch,
  *                               2, 4 or 8 = temporally blocked sweeps per launch. */
 dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long value);
 /* The cudaStream_t the context launches on, as an opaque handle (for event timing). */
@@ -141,6 +142,8 @@ typedef struct {
     int max_iterations;  /* block iterations cap */
     int max_subspace;    /* basis size cap in multiples of nbands (>= 2) */
     int verbose;         /* 1: per-iteration lines on stderr */
+    int preconditioner;  /* 0: the reference's diagonal (theta - diag)^-1 (EigenvalueSolverMolecule.cpp:521-555);
+                            k > 0: k damped-Jacobi smoothing steps on (T + sigma) t = r (default 4) */
 } dft_eig_opts;
 
 /* solveMolecularOrbitals (reference EigenvalueSolverMolecule.h:20-28,

@@ -181,7 +181,7 @@ inline std::vector<MolecularOrbital> solveMolecularOrbitals(const CartesianGrid&
     const dft_grid g = detail::grid_of(grid);
     detail::Dev V(effectivePotential), P(block);
     std::vector<double> eig(nb);
-    dft_eig_opts o{1.0e-7, (int)std::min<std::size_t>(maxIterations, 1000000), 3, 0};
+    dft_eig_opts o{1.0e-7, (int)std::min<std::size_t>(maxIterations, 1000000), 3, 0, 4};
     detail::check(dft_solve_orbitals_dev(detail::ctx(), &g, V.d(), (int)numberOfOrbitals, nb, P.d(), (long)N,
                                          initialOrbitals.empty() ? 0 : 1, eig.data(), &o, nullptr));
     const std::vector<double> psi = P.get((size_t)nb * N);

@@ -79,7 +79,7 @@ def test_hpsi_large_numpy_restatement(engine):
         assert np.array_equal(H[band], ref.ravel())
 
 
-@pytest.fixture(params=[0, 1, 2, 4, 8], ids=lambda t: f"spl{t}")
+@pytest.fixture(params=[0, -1, 1, 2, 4, 8], ids=lambda t: f"spl{t}")
 def sweeps_per_launch(request, engine):
     """Every Jacobi launch shape (one sweep per launch, temporal blocks of 2/4/8, auto)."""
     engine.set_tuning("jacobi_sweeps_per_launch", request.param)
@@ -231,8 +231,9 @@ def test_nuclear_potential(engine, port):
     assert ei.value.status == dft_b200.DFT_SINGULAR
 
 
+@pytest.mark.parametrize("precond", [0, 4], ids=["diag", "kinetic4"])
 @pytest.mark.parametrize("case", ["h2o_11", "h2_16"])
-def test_block_davidson_vs_reference_algorithm(engine, port, case):
+def test_block_davidson_vs_reference_algorithm(engine, port, case, precond):
     """Eigenpairs of the block solver vs the reference's state-by-state Davidson (oracle)."""
     if case == "h2o_11":
         n, b, Z = (11, 9, 8), (-3.0, 3.4, -2.5, 2.9, -2.2, 2.0), [8, 1, 1]
@@ -249,7 +250,7 @@ def test_block_davidson_vs_reference_algorithm(engine, port, case):
     e_ref, psi_ref = port.solve_orbitals(n, b, V, nocc)
     nbands = nocc + 3
     psi = engine.array(nbands * N)
-    eig, it = engine.solve_orbitals(g, engine.upload(V), nocc, nbands, psi, N, init=False)
+    eig, it = engine.solve_orbitals(g, engine.upload(V), nocc, nbands, psi, N, init=False, preconditioner=precond)
     assert np.max(np.abs(eig[:nocc] - e_ref)) < 1e-9
     P = psi.to_host((nbands, N))
     dV = g.getDx() * g.getDy() * g.getDz()
