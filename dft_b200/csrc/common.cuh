@@ -61,6 +61,9 @@ inline Grid make_grid(const dft_grid* g) {
         fail(DFT_INVALID_ARGUMENT, "CartesianGrid requires valid spatial bounds.");
     if (g->nx > (1 << 20) || g->ny > (1 << 20) || g->nz > (1 << 20))
         fail(DFT_INVALID_ARGUMENT, "grid dimension too large");
+    // stencil kernels use 32-bit offsets within one field
+    if ((long long)g->nx * g->ny * g->nz >= (1LL << 31) - 1)
+        fail(DFT_INVALID_ARGUMENT, "grids of 2^31 points or more are not supported");
     Grid d;
     d.nx = (int)g->nx;
     d.ny = (int)g->ny;

@@ -168,13 +168,14 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
     if (i >= g.nx || j >= g.ny) return;
     const double* __restrict__ p = psi + (long long)band * ld;
     double* __restrict__ o = out + (long long)band * ld;
-    const long long sxy = (long long)g.nx * g.ny;
+    const int sxy = g.nx * g.ny;  // 32-bit offsets within a band (host checks N < 2^31)
     const int kb = kc * zchunk;
     const int ke = min(g.nz, kb + zchunk);
-    long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
+    int idx = kb * sxy + j * g.nx + i;
     double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
     double cur = __ldg(p + idx);
     const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+#pragma unroll 4
     for (int k = kb; k < ke; ++k, idx += sxy) {
         const bool zr = k + 1 < g.nz;
         const double above = zr ? __ldg(p + idx + sxy) : 0.0;
@@ -294,17 +295,20 @@ __global__ void __launch_bounds__(JB_X* JB_Y) jacobi_sweep_kernel(Grid g, const 
     const int j = blockIdx.y * JB_Y + threadIdx.y;
     double md = 0.0;
     if (i >= 1 && i + 1 < g.nx && j >= 1 && j + 1 < g.ny) {
-        const long long sxy = (long long)g.nx * g.ny;
+        // 32-bit offsets (the host rejects grids of 2^31 points or more)
+        const int sxy = g.nx * g.ny;
         const int kb = max(1, (int)blockIdx.z * zchunk);
         const int ke = min(g.nz - 1, (int)(blockIdx.z + 1) * zchunk);
         if (kb < ke) {
-            long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
-            double below = cur[idx - sxy];
-            double c = cur[idx];
+            int idx = kb * sxy + j * g.nx + i;
+            double below = __ldg(cur + idx - sxy);
+            double c = __ldg(cur + idx);
+            // unrolled so that the loads of several planes are in flight together
+#pragma unroll 4
             for (int k = kb; k < ke; ++k, idx += sxy) {
-                const double above = cur[idx + sxy];
-                const double sx = __dadd_rn(cur[idx - 1], cur[idx + 1]);
-                const double sy = __dadd_rn(cur[idx - g.nx], cur[idx + g.nx]);
+                const double above = __ldg(cur + idx + sxy);
+                const double sx = __dadd_rn(__ldg(cur + idx - 1), __ldg(cur + idx + 1));
+                const double sy = __dadd_rn(__ldg(cur + idx - g.nx), __ldg(cur + idx + g.nx));
                 const double sz = __dadd_rn(below, above);
                 double acc = __dadd_rn(__dmul_rn(g.ix2, sx), __dmul_rn(g.iy2, sy));
                 acc = __dadd_rn(acc, __dmul_rn(g.iz2, sz));
