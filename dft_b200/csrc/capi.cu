@@ -124,8 +124,8 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
         NEED(ctx && key, "NULL argument");
         const std::string k(key);
         if (k == "jacobi_sweeps_per_launch") {
-            NEED(value == 0 || value == -1 || value == 1 || value == 2 || value == 4 || value == 8,
-                 "jacobi_sweeps_per_launch must be 0 (auto), -1 (persistent), 1, 2, 4 or 8");
+            NEED(value == 0 || value == -2 || value == -1 || value == 1 || value == 2 || value == 4 || value == 8,
+                 "jacobi_sweeps_per_launch must be 0 (auto), -2 (cluster), -1 (persistent), 1, 2, 4 or 8");
             ctx->jacobi_sweeps_per_launch = (int)value;
         } else {
             dftb::fail(DFT_INVALID_ARGUMENT, "unknown tuning key '%s'", key);

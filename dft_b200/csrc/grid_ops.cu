@@ -8,6 +8,8 @@
 // Every operator whose reference result is deterministic (H psi, Jacobi, density, the
 // nuclear potential, mixing) uses round-to-nearest intrinsics in the reference's operation
 // order (no FMA contraction), which makes it bit-identical to the reference.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -175,7 +177,6 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
     double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
     double cur = __ldg(p + idx);
     const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
-#pragma unroll 4
     for (int k = kb; k < ke; ++k, idx += sxy) {
         const bool zr = k + 1 < g.nz;
         const double above = zr ? __ldg(p + idx + sxy) : 0.0;
@@ -599,7 +600,163 @@ __global__ void __launch_bounds__(256) jacobi_persistent_kernel(Grid g, const do
     }
 }
 
+// ---- cluster-resident Jacobi: the whole grid in the shared memory of one thread-block cluster
+// Small grids (C1 is 48^3 = 110,592 points, 0.9 MB per field) fit in the distributed shared
+// memory of a 16-block cluster: block r keeps a z-slab of V, V' and rho in its own shared memory
+// and reads the two halo planes from its neighbours' shared memory (DSMEM).  One hardware
+// cluster barrier per sweep; after it every block reads the 16 per-block maxima, so all blocks
+// take the same stop decision.  Same arithmetic as jacobi_sweep_kernel (bit-identical).
+constexpr int JC_THREADS = 1024;
+
+struct JacobiClusterOut {
+    long long sweeps;
+    double last_diff;
+};
+
+__global__ void __launch_bounds__(JC_THREADS, 1)
+    jacobi_cluster_kernel(Grid g, const double* __restrict__ rho, double* __restrict__ vh, JacobiClusterOut* out,
+                          double den, double tol, long long cap, int pmax) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int nr = (int)cl.num_blocks();
+    const int r = (int)cl.block_rank();
+    extern __shared__ double sm[];
+    __shared__ double s_max[2];
+    __shared__ double red[JC_THREADS / 32];
+    __shared__ double s_d;
+    const int plane = g.nx * g.ny;
+    double* bufA = sm;
+    double* bufB = sm + (size_t)pmax * plane;
+    double* R = sm + 2 * (size_t)pmax * plane;
+    const int zlo = (int)(((long long)r * g.nz) / nr), zhi = (int)(((long long)(r + 1) * g.nz) / nr);
+    const int np = zhi - zlo;
+    const int zlo_prev = r > 0 ? (int)(((long long)(r - 1) * g.nz) / nr) : 0;
+    const int np_prev = zlo - zlo_prev;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < np * plane; e += JC_THREADS) {
+        const double v = vh[(size_t)zlo * plane + e];
+        bufA[e] = v;
+        bufB[e] = v;
+        R[e] = rho[(size_t)zlo * plane + e];
+    }
+    // neighbour slabs (never dereferenced at the outer faces: planes 0 and nz-1 are fixed)
+    double* A_prev = r > 0 ? cl.map_shared_rank(bufA, r - 1) : nullptr;
+    double* B_prev = r > 0 ? cl.map_shared_rank(bufB, r - 1) : nullptr;
+    double* A_next = r + 1 < nr ? cl.map_shared_rank(bufA, r + 1) : nullptr;
+    double* B_next = r + 1 < nr ? cl.map_shared_rank(bufB, r + 1) : nullptr;
+    cl.sync();
+    const double c4pi = 4.0 * xcf::PI;
+    long long fin = 0;
+    double d = 0.0;
+    for (long long s = 0; s < cap; ++s) {
+        const bool odd = s & 1;
+        const double* cur = odd ? bufB : bufA;
+        double* nxt = odd ? bufA : bufB;
+        const double* cprev = odd ? B_prev : A_prev;
+        const double* cnext = odd ? B_next : A_next;
+        double md = 0.0;
+        for (int lp = 0; lp < np; ++lp) {
+            const int z = zlo + lp;
+            if (z == 0 || z == g.nz - 1) continue;
+            const double* zm_plane = lp > 0 ? cur + (size_t)(lp - 1) * plane : cprev + (size_t)(np_prev - 1) * plane;
+            const double* zp_plane = lp + 1 < np ? cur + (size_t)(lp + 1) * plane : cnext;
+            const double* cp = cur + (size_t)lp * plane;
+            double* np_out = nxt + (size_t)lp * plane;
+            const double* rp = R + (size_t)lp * plane;
+            for (int q = tid; q < plane; q += JC_THREADS) {
+                const int j = q / g.nx, i = q - j * g.nx;
+                if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1) continue;
+                const double c = cp[q];
+                const double sx = __dadd_rn(cp[q - 1], cp[q + 1]);
+                const double sy = __dadd_rn(cp[q - g.nx], cp[q + g.nx]);
+                const double sz = __dadd_rn(zm_plane[q], zp_plane[q]);
+                double acc = __dadd_rn(__dmul_rn(g.ix2, sx), __dmul_rn(g.iy2, sy));
+                acc = __dadd_rn(acc, __dmul_rn(g.iz2, sz));
+                acc = __dadd_rn(acc, __dmul_rn(c4pi, rp[q]));
+                const double v = __ddiv_rn(acc, den);
+                np_out[q] = v;
+                md = fmax(md, fabs(v - c));
+            }
+        }
+        md = warp_max(md);
+        if ((tid & 31) == 0) red[tid >> 5] = md;
+        __syncthreads();
+        if (tid == 0) {
+            double m = red[0];
+            for (int w = 1; w < JC_THREADS / 32; ++w) m = fmax(m, red[w]);
+            s_max[s & 1] = m;
+        }
+        cl.sync();
+        if (tid == 0) {
+            double m = 0.0;
+            for (int q = 0; q < nr; ++q) m = fmax(m, *cl.map_shared_rank(&s_max[s & 1], q));
+            s_d = m;
+        }
+        __syncthreads();
+        d = s_d;
+        if (d < tol || s + 1 >= cap) {
+            fin = s + 1;
+            break;
+        }
+    }
+    const double* res = (fin & 1) ? bufB : bufA;
+    for (int e = tid; e < np * plane; e += JC_THREADS) vh[(size_t)zlo * plane + e] = res[e];
+    if (r == 0 && tid == 0) {
+        out->sweeps = fin;
+        out->last_diff = d;
+    }
+    cl.sync();  // no block leaves while a neighbour may still read its shared memory
+}
+
 }  // namespace
+
+// The whole solve inside one 16-block cluster's shared memory (grids of up to ~150k points).
+// Returns false (nothing launched) when the grid does not fit or the device cannot host the cluster.
+static bool hartree_cluster(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol,
+                            long max_sweeps, JacobiResult* res) {
+    const int nr = 16;
+    const int plane = g.nx * g.ny;
+    const int pmax = (g.nz + nr - 1) / nr;
+    const size_t smem = sizeof(double) * 3 * (size_t)pmax * plane;
+    if (g.nz < 2 * nr || smem > 200 * 1024) return false;
+    static int attr_ok = -1;
+    if (attr_ok < 0) {
+        attr_ok = cudaFuncSetAttribute(jacobi_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+                          cudaSuccess &&
+                      cudaFuncSetAttribute(jacobi_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           200 * 1024) == cudaSuccess
+                  ? 1
+                  : 0;
+        cudaGetLastError();
+    }
+    if (!attr_ok) return false;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nr);
+    cfg.blockDim = dim3(JC_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = nr;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, jacobi_cluster_kernel, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    JacobiClusterOut* o = (JacobiClusterOut*)ws_get(ctx, WS_CTRL, sizeof(JacobiClusterOut) + 64);
+    const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
+    DFT_CUDA(cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel, g, rho, vh, o, den, tol, (long long)max_sweeps, pmax));
+    count_launch(ctx);
+    JacobiClusterOut* h = (JacobiClusterOut*)pinned(ctx, (sizeof(JacobiClusterOut) + 7) / 8);
+    DFT_CUDA(cudaMemcpyAsync(h, o, sizeof(JacobiClusterOut), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    *res = {(long)h->sweeps, h->last_diff};
+    return true;
+}
 
 // The whole solve in one cooperative launch (small grids).
 static JacobiResult hartree_persistent(dft_context* ctx, const Grid& g, const double* rho, double* vh, double* buf1,
@@ -724,6 +881,11 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
     // launch shape: one persistent launch on small grids (launch-latency bound), one sweep per
     // launch otherwise; 2/4/8 select the temporally blocked kernel
     int tmax = ctx->jacobi_sweeps_per_launch;
+    if (tmax == 0 || tmax == -2) {
+        JacobiResult r;
+        if (hartree_cluster(ctx, g, rho, vh, tol, max_sweeps, &r)) return r;
+        if (tmax == -2) fail(DFT_INVALID_ARGUMENT, "grid does not fit the cluster-resident Jacobi");
+    }
     if (tmax == 0) tmax = g.N <= 64LL * 64 * 64 ? -1 : 1;
     if (tmax == -1) return hartree_persistent(ctx, g, rho, vh, buf1, tol, max_sweeps);
     if (tmax == 2 || tmax == 4 || tmax == 8) return hartree_tb(ctx, g, rho, vh, buf1, tol, max_sweeps, tmax);

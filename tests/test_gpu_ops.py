@@ -79,16 +79,20 @@ def test_hpsi_large_numpy_restatement(engine):
         assert np.array_equal(H[band], ref.ravel())
 
 
-@pytest.fixture(params=[0, -1, 1, 2, 4, 8], ids=lambda t: f"spl{t}")
+@pytest.fixture(params=[0, -2, -1, 1, 2, 4, 8], ids=lambda t: f"spl{t}")
 def sweeps_per_launch(request, engine):
-    """Every Jacobi launch shape (one sweep per launch, temporal blocks of 2/4/8, auto)."""
+    """Every Jacobi launch shape: auto, cluster-resident (-2), persistent (-1), one sweep per
+    launch (1), temporal blocks of 2/4/8."""
     engine.set_tuning("jacobi_sweeps_per_launch", request.param)
     yield request.param
     engine.set_tuning("jacobi_sweeps_per_launch", 0)
 
 
-@pytest.mark.parametrize("n,b", GRIDS[:3] + [((24, 24, 24), (-6.0, 6.0) * 3), ((40, 37, 70), (-6.0, 6.0) * 3)])
+@pytest.mark.parametrize("n,b", GRIDS + [((24, 24, 24), (-6.0, 6.0) * 3), ((40, 37, 70), (-6.0, 6.0) * 3),
+                                         ((33, 31, 35), (-6.0, 6.1, -6.0, 5.9, -5.5, 6.2))])
 def test_jacobi_bit_exact_and_sweeps(engine, port, n, b, sweeps_per_launch):
+    if sweeps_per_launch == -2 and n[2] < 32:
+        pytest.skip("the cluster-resident solver needs nz >= 32")
     na, nb = gaussian_density(n, b, 2)
     rho = na + nb
     ref = np.empty(rho.size)
@@ -109,7 +113,7 @@ def test_jacobi_bit_exact_and_sweeps(engine, port, n, b, sweeps_per_launch):
 def test_jacobi_cap(engine, port, sweeps_per_launch):
     """The silent sweep cap (HartreePotentialMolecule.cpp:207): stop after max_sweeps, with the
     iterate of exactly that sweep (37 is not a multiple of any block size)."""
-    n, b = (24, 24, 24), (-6.0, 6.0) * 3
+    n, b = (24, 24, 40), (-6.0, 6.0) * 3
     na, nb = gaussian_density(n, b, 4)
     d_rho, d_vh = engine.upload(na + nb), engine.array(na.size)
     sweeps, last = engine.hartree(G(n, b), d_rho, d_vh, tol=1e-8, max_sweeps=37)
