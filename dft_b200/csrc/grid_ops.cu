@@ -170,10 +170,10 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
     if (i >= g.nx || j >= g.ny) return;
     const double* __restrict__ p = psi + (long long)band * ld;
     double* __restrict__ o = out + (long long)band * ld;
-    const int sxy = g.nx * g.ny;  // 32-bit offsets within a band (host checks N < 2^31)
+    const long long sxy = (long long)g.nx * g.ny;
     const int kb = kc * zchunk;
     const int ke = min(g.nz, kb + zchunk);
-    int idx = kb * sxy + j * g.nx + i;
+    long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
     double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
     double cur = __ldg(p + idx);
     const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
@@ -687,10 +687,10 @@ __global__ void __launch_bounds__(JC_THREADS, 1)
             s_max[s & 1] = m;
         }
         cl.sync();
-        if (tid == 0) {
-            double m = 0.0;
-            for (int q = 0; q < nr; ++q) m = fmax(m, *cl.map_shared_rank(&s_max[s & 1], q));
-            s_d = m;
+        if (tid < 32) {  // one remote read per lane, then a shuffle max
+            double m = tid < nr ? *cl.map_shared_rank(&s_max[s & 1], tid) : 0.0;
+            m = warp_max(m);
+            if (tid == 0) s_d = m;
         }
         __syncthreads();
         d = s_d;
