@@ -37,7 +37,7 @@ class dft_grid(C.Structure):
 
 class dft_eig_opts(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iterations", C.c_int), ("max_subspace", C.c_int), ("verbose", C.c_int),
-                ("preconditioner", C.c_int)]
+                ("preconditioner", C.c_int), ("mixed_precision", C.c_int)]
 
 
 class dft_scf_opts(C.Structure):
@@ -105,6 +105,7 @@ _SIGS = {
     "dft_nuclear_potential_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.POINTER(C.c_int), _D, _P], C.c_int),
     "dft_solve_orbitals_dev": ([_P, C.POINTER(dft_grid), _P, C.c_int, C.c_int, _P, C.c_long, C.c_int, _D,
                                 C.POINTER(dft_eig_opts), C.POINTER(C.c_int)], C.c_int),
+    "dft_gram_dev": ([_P, C.POINTER(dft_grid), _P, C.c_long, C.c_int, _P, C.c_long, C.c_int, C.c_int, _D], C.c_int),
     "dft_scf_default_options": ([C.POINTER(dft_scf_opts)], None),
     "dft_scf_molecule": ([_P, C.POINTER(dft_grid), C.c_int, C.POINTER(C.c_int), _D, C.c_int, C.c_int, C.c_int,
                           C.POINTER(dft_scf_opts), C.POINTER(dft_scf_result)], C.c_int),
@@ -360,11 +361,17 @@ class Engine:
         _check(load().dft_nuclear_potential_dev(self.ctx, C.byref(g), len(Z), Z.ctypes.data_as(C.POINTER(C.c_int)),
                                                 _dp(xyz), _ptr(vext)))
 
+    def gram(self, grid, A, lda, ka, B, ldb, kb, precision=0) -> np.ndarray:
+        g = grid.c()
+        out = np.zeros((ka, kb))
+        _check(load().dft_gram_dev(self.ctx, C.byref(g), _ptr(A), lda, ka, _ptr(B), ldb, kb, int(precision), _dp(out)))
+        return out
+
     def solve_orbitals(self, grid, V, nocc, nbands, psi, ld, init=False, tol=1e-7, max_iterations=2000,
-                       max_subspace=3, verbose=False, preconditioner=4):
+                       max_subspace=3, verbose=False, preconditioner=4, mixed_precision=0):
         g = grid.c()
         eig = np.zeros(nbands)
-        o = dft_eig_opts(tol, max_iterations, max_subspace, int(verbose), int(preconditioner))
+        o = dft_eig_opts(tol, max_iterations, max_subspace, int(verbose), int(preconditioner), int(mixed_precision))
         it = C.c_int()
         _check(load().dft_solve_orbitals_dev(self.ctx, C.byref(g), _ptr(V), nocc, nbands, _ptr(psi), ld, int(init),
                                              _dp(eig), C.byref(o), C.byref(it)))

@@ -32,6 +32,7 @@ SOURCES = {
     "davidson.cu": [],
     "scf.cu": [],
     "radial.cu": ["-fmad=false"],
+    "gram_tc.cu": [],
     "eigh.cpp": [],
 }
 

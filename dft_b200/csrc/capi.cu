@@ -272,10 +272,24 @@ dft_status_t dft_solve_orbitals_dev(dft_context* ctx, const dft_grid* g, const d
             if (opts->max_iterations > 0) o.max_iterations = opts->max_iterations;
             if (opts->max_subspace >= 2) o.max_subspace = opts->max_subspace;
             o.precond_steps = opts->preconditioner;
+            o.mixed_precision = opts->mixed_precision;
             o.verbose = opts->verbose;
         }
         const int it = dftb::solve_orbitals(ctx, G, V, nocc, nbands, psi, ld, init != 0, eig, nullptr, o);
         if (iterations_out) *iterations_out = it;
+    });
+}
+
+dft_status_t dft_gram_dev(dft_context* ctx, const dft_grid* g, const double* A, long lda, int ka, const double* B,
+                          long ldb, int kb, int precision, double* C_host) {
+    return guard(ctx, [&] {
+        NEED(ctx && A && B && C_host, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        NEED(ka > 0 && kb > 0 && lda >= G.N && ldb >= G.N, "bad sizes");
+        std::vector<double> C;
+        if (precision == 1) dftb::gram_tc(ctx, G, A, lda, ka, B, ldb, kb, C);
+        else dftb::gram_fp64(ctx, G, A, lda, ka, B, ldb, kb, C);
+        std::copy(C.begin(), C.end(), C_host);
     });
 }
 

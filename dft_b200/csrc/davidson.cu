@@ -306,15 +306,24 @@ void rotate(dft_context* ctx, const Grid& g, const double* in, long long ldi, in
 
 // Orthonormalise the nt columns of T against V[0:k] and among themselves (dV inner product).
 // Dependent directions are dropped; returns the number kept (compacted to the front of T).
+// tc: Gram products on the tensor cores (TF32 hi+lo, ~1e-6 relative) instead of FP64
+void gram_any(bool tc, dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B,
+              long long ldb, int kb, std::vector<double>& C) {
+    if (tc) gram_tc(ctx, g, A, lda, ka, B, ldb, kb, C);
+    else gram(ctx, g, A, lda, ka, B, ldb, kb, C);
+}
+
 int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, double* T, int nt, long long ld,
-                   double* W) {
+                   double* W, bool tc = false) {
     std::vector<double> C, S, w, Z, Yk;
+    // directions below the Gram products' noise floor are dropped
+    const double floor_rel = tc ? 1e-8 : 1e-13;
     for (int pass = 0; pass < 2 && nt > 0; ++pass) {
         if (k > 0) {
-            gram(ctx, g, V, ld, k, T, ld, nt, C);  // k x nt
+            gram_any(tc, ctx, g, V, ld, k, T, ld, nt, C);  // k x nt
             rotate(ctx, g, V, ld, k, C, nt, T, ld, -1.0, 1.0);
         }
-        gram(ctx, g, T, ld, nt, T, ld, nt, S);
+        gram_any(tc, ctx, g, T, ld, nt, T, ld, nt, S);
         for (int i = 0; i < nt; ++i)
             for (int j = 0; j < i; ++j) S[(size_t)i * nt + j] = S[(size_t)j * nt + i] = 0.5 * (S[(size_t)i * nt + j] + S[(size_t)j * nt + i]);
         std::vector<double> Sc = S;
@@ -324,7 +333,7 @@ int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, doub
         // keep eigen-directions well above round-off; scale by lambda^{-1/2}
         std::vector<int> keep;
         for (int j = 0; j < nt; ++j)
-            if (w[j] > wmax * 1e-13 && w[j] > 1e-24) keep.push_back(j);
+            if (w[j] > wmax * floor_rel && w[j] > 1e-24) keep.push_back(j);
         const int nk = (int)keep.size();
         Yk.assign((size_t)nt * nk, 0.0);
         for (int i = 0; i < nt; ++i)
@@ -337,6 +346,11 @@ int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, doub
 }
 
 }  // namespace
+
+void gram_fp64(dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B,
+               long long ldb, int kb, std::vector<double>& C) {
+    gram(ctx, g, A, lda, ka, B, ldb, kb, C);
+}
 
 int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, int nbands, double* psi,
                    long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o) {
@@ -384,13 +398,17 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
     }
     apply_hamiltonian(ctx, g, V, Vb, AV, k, ld);
 
+    // Mixed precision: while the occupied residuals are above mixed_switch the Gram products run
+    // on the tensor cores (TF32 hi+lo); then the basis restarts from the Ritz block in FP64 and
+    // every later product (and the convergence test) is FP64.
+    bool tc_mode = o.mixed_precision != 0;
     std::vector<double> G;  // k x k, row-major, grows
     auto grow_G = [&](int k_old, int k_new) {
         std::vector<double> Gn((size_t)k_new * k_new, 0.0);
         for (int i = 0; i < k_old; ++i)
             for (int j = 0; j < k_old; ++j) Gn[(size_t)i * k_new + j] = G[(size_t)i * k_old + j];
         std::vector<double> C;
-        gram(ctx, g, Vb, ld, k_new, AV + (long long)k_old * ld, ld, k_new - k_old, C);  // k_new x (k_new-k_old)
+        gram_any(tc_mode, ctx, g, Vb, ld, k_new, AV + (long long)k_old * ld, ld, k_new - k_old, C);
         const int nn = k_new - k_old;
         for (int i = 0; i < k_new; ++i)
             for (int c = 0; c < nn; ++c) {
@@ -455,6 +473,21 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
             fprintf(stderr, "[davidson] it=%d k=%d active=%zu max_occ_res=%.3e theta0=%.10f\n", it, k, active.size(), mx,
                     theta[0]);
         }
+        if (tc_mode) {
+            double mx = 0.0;
+            for (int b = 0; b < nocc; ++b) mx = std::max(mx, rn[b]);
+            if (occ_conv || mx < o.mixed_switch) {
+                // switch to FP64: restart from the Ritz block, re-orthonormalised and re-projected
+                tc_mode = false;
+                DFT_CUDA(cudaMemcpyAsync(Vb, X, vecb * nb, cudaMemcpyDeviceToDevice, ctx->stream));
+                k = orthonormalise(ctx, g, Vb, 0, Vb, nb, ld, W);
+                if (k < nb) fail(DFT_NUMERICAL, "Ritz block lost rank at the FP64 switch");
+                apply_hamiltonian(ctx, g, V, Vb, AV, k, ld);
+                G.clear();
+                grow_G(0, k);
+                continue;
+            }
+        }
         if (occ_conv) {
             done = true;
             break;
@@ -506,13 +539,13 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
             if (cur != T)
                 DFT_CUDA(cudaMemcpyAsync(T, cur, vecb * na, cudaMemcpyDeviceToDevice, ctx->stream));
         }
-        int nt = orthonormalise(ctx, g, Vb, k, T, na, ld, W);
+        int nt = orthonormalise(ctx, g, Vb, k, T, na, ld, W, tc_mode);
         if (nt == 0) {
             // preconditioned directions fell into the basis: fall back to raw residuals
             for (int a = 0; a < na; ++a)
                 DFT_CUDA(cudaMemcpyAsync(T + (long long)a * ld, R + (long long)active[a] * ld, vecb,
                                          cudaMemcpyDeviceToDevice, ctx->stream));
-            nt = orthonormalise(ctx, g, Vb, k, T, na, ld, W);
+            nt = orthonormalise(ctx, g, Vb, k, T, na, ld, W, tc_mode);
             if (nt == 0) fail(DFT_NOT_CONVERGED, "La direccion de expansion Davidson es numericamente dependiente.");
         }
         apply_hamiltonian(ctx, g, V, T, AV + (long long)k * ld, nt, ld);

@@ -1,0 +1,280 @@
+// Mixed-precision Gram products on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// C (ka x kb) = dV * A^T B for tall-skinny band blocks (A_i, B_j contiguous over N grid points).
+// Each FP64 input x is split into two TF32 numbers, x ~ hi + lo (hi = TF32-rounded x,
+// lo = TF32(x - hi)), and the product is formed as hi*hi + hi*lo + lo*hi with FP32
+// accumulation in tensor memory (TMEM): relative error ~1e-6, the "FP32-level" precision the
+// block eigensolver uses while residuals are large.  Per block:
+//   * 128 threads stage a 32-point K slice of A (128 rows) and B (<= 256 rows) from HBM,
+//     split them and store hi/lo planes in shared memory in the canonical K-major layout
+//     (8-row x 16-byte core matrices, no swizzle), double-buffered;
+//   * one thread issues 12 tcgen05.mma.kind::tf32 (4 K=8 steps x 3 products) into a
+//     128 x N FP32 accumulator in TMEM and commits them to an mbarrier;
+//   * after its K range the block reads the accumulator back with tcgen05.ld (each warp its
+//     32 TMEM lanes) and writes FP64 partial sums; a deterministic FP64 reduction over blocks
+//     (gram_reduce_kernel in davidson.cu) finishes the product.
+// Every mbarrier wait is bounded; a block that gives up sets an error flag, waits (bounded)
+// for its own MMAs, frees its TMEM and returns.
+#include <cstdint>
+#include <vector>
+
+#include "ops.h"
+
+namespace dftb {
+
+namespace {
+
+constexpr int TC_THREADS = 128;
+constexpr int TC_M = 128;     // accumulator rows (A vectors per tile)
+constexpr int TC_KT = 32;     // points per K slice
+constexpr int TC_NMAX = 256;  // accumulator columns (B vectors per tile)
+constexpr long long TC_SPIN_LIMIT = 1LL << 22;  // try_wait polls before a block gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// canonical K-major, no-swizzle placement of element (row, k) of an R-row x 32-point slice:
+// core matrix (8 rows x 4 fp32) index = (k/4) * (R/8) + row/8, 128 bytes each
+__device__ __forceinline__ int kmajor_offset_words(int row, int k, int R) {
+    return (((k >> 2) * (R >> 3) + (row >> 3)) << 5) + ((row & 7) << 2) + (k & 3);
+}
+
+// UMMA shared-memory matrix descriptor (sm_100: version 1, no swizzle)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // version
+    return d;                // layout type 0 = SWIZZLE_NONE, base offset 0
+}
+
+// instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = n
+__host__ __device__ constexpr uint32_t idesc_tf32(int n) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// bounded wait for the phase with the given parity to complete; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (long long i = 0; i < TC_SPIN_LIMIT; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;  // no output lanes disabled
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+        ::"r"(tmem_c), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Gram tile.  grid = (ceil(ka/128), ceil(kb/nt), nchunks); dynamic smem = 2 stages x
+// (A hi, A lo: 128 x 32 fp32; B hi, B lo: ncols x 32 fp32) + 2 mbarriers.
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    gram_tc_kernel(const double* __restrict__ A, long long lda, int ka, const double* __restrict__ B, long long ldb,
+                   int kb, int nt, int ncols, long long n, long long chunk, double* __restrict__ partial,
+                   int* __restrict__ error) {
+    extern __shared__ __align__(1024) uint32_t sm[];
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t bar[2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TC_M, n0 = blockIdx.y * nt;
+    const int mrows = min(TC_M, ka - m0), nrows = min(nt, kb - n0);
+    const long long p0 = (long long)blockIdx.z * chunk, p1 = min(n, p0 + chunk);
+    const int a_words = TC_M * TC_KT, b_words = ncols * TC_KT;
+    const int stage_words = 2 * a_words + 2 * b_words;
+    // TMEM: ncols fp32 columns x 128 lanes, allocated by warp 0
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = idesc_tf32(ncols);
+    bool ok = true;
+    uint32_t phase[2] = {0, 0};
+    bool pending[2] = {false, false};
+    int step = 0;
+    for (long long ps = p0; ps < p1; ps += TC_KT, ++step) {
+        const int st = step & 1;
+        // the MMAs that last read this stage must be done before it is overwritten
+        if (pending[st]) {
+            if (!mbar_wait(&bar[st], phase[st])) ok = false;
+            phase[st] ^= 1;
+            pending[st] = false;
+        }
+        if (!__syncthreads_and(ok)) break;
+        uint32_t* ahi = sm + st * stage_words;
+        uint32_t* alo = ahi + a_words;
+        uint32_t* bhi = alo + a_words;
+        uint32_t* blo = bhi + b_words;
+        const int kvalid = (int)min((long long)TC_KT, p1 - ps);
+        // stage A: 128 rows x 32 points; a warp reads one row's 32 consecutive points
+        for (int r = warp; r < TC_M; r += TC_THREADS / 32) {
+            const double x = (r < mrows && lane < kvalid) ? __ldg(A + (long long)(m0 + r) * lda + ps + lane) : 0.0;
+            const uint32_t h = to_tf32((float)x);
+            const uint32_t l = to_tf32((float)(x - (double)__uint_as_float(h)));
+            const int o = kmajor_offset_words(r, lane, TC_M);
+            ahi[o] = h;
+            alo[o] = l;
+        }
+        for (int r = warp; r < ncols; r += TC_THREADS / 32) {
+            const double x = (r < nrows && lane < kvalid) ? __ldg(B + (long long)(n0 + r) * ldb + ps + lane) : 0.0;
+            const uint32_t h = to_tf32((float)x);
+            const uint32_t l = to_tf32((float)(x - (double)__uint_as_float(h)));
+            const int o = kmajor_offset_words(r, lane, ncols);
+            bhi[o] = h;
+            blo[o] = l;
+        }
+        // generic-proxy smem writes -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t lbo_a = (TC_M / 8) * 128, lbo_b = (uint32_t)(ncols / 8) * 128, sbo = 128;
+            const uint32_t sa_hi = smem_u32(ahi), sa_lo = smem_u32(alo), sb_hi = smem_u32(bhi), sb_lo = smem_u32(blo);
+#pragma unroll
+            for (int kk = 0; kk < TC_KT / 8; ++kk) {
+                // K = 8 tf32 = two 4-element core-matrix columns
+                const uint32_t oa = kk * 2 * lbo_a, ob = kk * 2 * lbo_b;
+                const uint64_t dah = smem_desc(sa_hi + oa, lbo_a, sbo), dal = smem_desc(sa_lo + oa, lbo_a, sbo);
+                const uint64_t dbh = smem_desc(sb_hi + ob, lbo_b, sbo), dbl = smem_desc(sb_lo + ob, lbo_b, sbo);
+                const uint32_t first = (step == 0 && kk == 0) ? 0u : 1u;
+                mma_tf32(tmem, dah, dbh, idesc, first);
+                mma_tf32(tmem, dah, dbl, idesc, 1u);
+                mma_tf32(tmem, dal, dbh, idesc, 1u);
+            }
+            mma_commit(&bar[st]);
+        }
+        pending[st] = true;
+    }
+    // drain: wait (bounded) for every stage that still has MMAs in flight
+    for (int st = 0; st < 2; ++st)
+        if (pending[st]) {
+            if (!mbar_wait(&bar[st], phase[st])) ok = false;
+            phase[st] ^= 1;
+        }
+    ok = __syncthreads_and(ok);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (tid == 0) atomicExch(error, 1);
+    } else if (step > 0) {
+        // accumulator row r = A vector m0 + r lives in TMEM lane r: warp w reads lanes 32w..32w+31
+        double* out = partial + (long long)blockIdx.z * ka * kb;
+        const int row = warp * 32 + lane;
+        for (int c0 = 0; c0 < ncols; c0 += 8) {
+            uint32_t v[8];
+            const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7])
+                         : "r"(addr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < mrows)
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (c0 + q < nrows) out[(long long)(m0 + row) * kb + (n0 + c0 + q)] = (double)__uint_as_float(v[q]);
+        }
+    } else {
+        // empty K range: this block contributes zeros
+        double* out = partial + (long long)blockIdx.z * ka * kb;
+        for (int e = tid; e < mrows * nrows; e += TC_THREADS)
+            out[(long long)(m0 + e / nrows) * kb + (n0 + e % nrows)] = 0.0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+__global__ void gram_tc_reduce_kernel(int nchunks, int nel, const double* __restrict__ partial, double scale,
+                                      double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    for (int e = blockIdx.x * warps + (threadIdx.x >> 5); e < nel; e += gridDim.x * warps) {
+        double s = 0.0;
+        for (int c = lane; c < nchunks; c += 32) s += partial[(long long)c * nel + e];
+        s = warp_sum(s);
+        if (lane == 0) out[e] = s * scale;
+    }
+}
+
+}  // namespace
+
+// C (ka x kb, host, row-major) = dV * A^T B on the tensor cores (TF32 hi+lo split).
+void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B, long long ldb,
+             int kb, std::vector<double>& C) {
+    C.assign((size_t)ka * kb, 0.0);
+    if (ka == 0 || kb == 0) return;
+    // N tile: up to 256 columns, a multiple of 16, TMEM allocation a power of two >= 32
+    const int ntiles = (kb + TC_NMAX - 1) / TC_NMAX;
+    const int nt = (kb + ntiles - 1) / ntiles;
+    int ncols = 32;
+    while (ncols < nt) ncols <<= 1;
+    const int mtiles = (ka + TC_M - 1) / TC_M;
+    const size_t smem = sizeof(uint32_t) * 2 * (size_t)(2 * TC_M * TC_KT + 2 * ncols * TC_KT);
+    // split K so that each block accumulates <= 8192 points in FP32 and the machine is covered
+    long long nch = std::max<long long>(1, (2LL * ctx->num_sms) / (mtiles * ntiles));
+    nch = std::max<long long>(nch, (g.N + 8191) / 8192);
+    long long chunk = (g.N + nch - 1) / nch;
+    chunk = ((chunk + TC_KT - 1) / TC_KT) * TC_KT;
+    nch = (g.N + chunk - 1) / chunk;
+    const size_t nel = (size_t)ka * kb;
+    double* partial = (double*)ws_get(ctx, WS_SMALL, sizeof(double) * (nel * nch + nel) + 64);
+    double* res = partial + nel * nch;
+    int* err = (int*)(res + nel);
+    static bool attr = false;
+    if (!attr) {
+        DFT_CUDA(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
+    }
+    DFT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+    gram_tc_kernel<<<dim3(mtiles, ntiles, (unsigned)nch), TC_THREADS, smem, ctx->stream>>>(
+        A, lda, ka, B, ldb, kb, nt, ncols, g.N, chunk, partial, err);
+    DFT_LAUNCH_CHECK();
+    const int rb = (int)std::min<size_t>((nel + 7) / 8, 4096);
+    gram_tc_reduce_kernel<<<rb, 256, 0, ctx->stream>>>((int)nch, (int)nel, partial, g.dV, res);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx, 2);
+    double* h = pinned(ctx, nel + 1);
+    DFT_CUDA(cudaMemcpyAsync(h, res, sizeof(double) * nel, cudaMemcpyDeviceToHost, ctx->stream));
+    DFT_CUDA(cudaMemcpyAsync(h + nel, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    if (*(int*)(h + nel)) fail(DFT_CUDA_ERROR, "tensor-core Gram: mbarrier wait timed out");
+    std::copy(h, h + nel, C.begin());
+}
+
+}  // namespace dftb

@@ -52,6 +52,13 @@ double kinetic_energy(dft_context* ctx, const Grid& g, const double* psi, int nb
 void kinetic_per_band(dft_context* ctx, const Grid& g, const double* psi, int nbands, long long ld, double* out_host);
 void nuclear_potential(dft_context* ctx, const Grid& g, int nnuc, const int* Z, const double* xyz, double* vext);
 
+// C (ka x kb, host) = dV A^T B: FP64 (davidson.cu) or on the tensor cores with a TF32 hi+lo
+// split (gram_tc.cu).
+void gram_fp64(dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B,
+               long long ldb, int kb, std::vector<double>& C);
+void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B, long long ldb,
+             int kb, std::vector<double>& C);
+
 // Block Davidson eigensolver (davidson.cu).
 struct EigOpts {
     double tol = 1e-7;
@@ -59,6 +66,8 @@ struct EigOpts {
     int max_subspace = 3;
     int verbose = 0;
     int precond_steps = 4;  // 0 = the reference's diagonal preconditioner
+    int mixed_precision = 0;       // 1 = tensor-core (TF32 hi+lo) Gram products while residuals are large
+    double mixed_switch = 1e-3;    // occupied residual below which the solver switches to FP64
 };
 int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, int nbands, double* psi,
                    long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o);

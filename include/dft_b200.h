@@ -145,7 +145,16 @@ typedef struct {
     int verbose;         /* 1: per-iteration lines on stderr */
     int preconditioner;  /* 0: the reference's diagonal (theta - diag)^-1 (EigenvalueSolverMolecule.cpp:521-555);
                             k > 0: k damped-Jacobi smoothing steps on (T + sigma) t = r (default 4) */
+    int mixed_precision; /* 1: Gram products on the tensor cores (TF32 hi+lo split, FP32 accumulation)
+                            until the occupied residuals fall below 1e-3, then FP64 to the end */
 } dft_eig_opts;
+
+/* dV * A^T B for band blocks A (ka x N, leading dimension lda) and B (kb x N), result in
+ * C_host (ka x kb, row-major).  precision 0 = FP64, 1 = tensor cores (TF32 hi+lo split).
+ * The block eigensolver's Gram product, exposed for testing; no counterpart in the reference
+ * (its dot products are EigenvalueSolverMolecule.cpp:35-47). */
+dft_status_t dft_gram_dev(dft_context* ctx, const dft_grid* g, const double* A, long lda, int ka, const double* B,
+                          long ldb, int kb, int precision, double* C_host);
 
 /* solveMolecularOrbitals (reference EigenvalueSolverMolecule.h:20-28,
  * EigenvalueSolverMolecule.cpp:1233-1300): the lowest nocc eigenpairs of H = -1/2 lap_h + V,

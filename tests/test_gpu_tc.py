@@ -1,0 +1,45 @@
+"""GPU: the tensor-core (tcgen05, TF32 hi+lo) Gram product and the mixed-precision eigensolver.
+
+Bars: the TF32 hi+lo Gram matches FP64 to 1e-5 of the largest |entry| (FP32 accumulation over
+chunks of <= 8192 points); the mixed-precision eigensolver, which switches to FP64 before its
+final iterations, gives the FP64 eigenvalues to 1e-9 Ha.
+"""
+import numpy as np
+import pytest
+
+import dft_b200
+from oracle.bindings import PZ81  # noqa: F401
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("ka,kb,n", [(12, 12, (40, 40, 40)), (50, 70, (64, 48, 33)), (130, 300, (32, 32, 40)),
+                                     (200, 69, (48, 48, 48)), (1, 3, (5, 7, 9))])
+def test_gram_tensor_cores_vs_fp64(engine, ka, kb, n):
+    g = dft_b200.CartesianGrid(*n, -3.0, 3.0, -2.0, 2.5, -1.5, 1.7)
+    N = g.getSize()
+    rng = np.random.default_rng(ka * 1000 + kb)
+    A = rng.standard_normal((ka, N))
+    B = A[: min(ka, kb)].copy() if kb <= ka else rng.standard_normal((kb, N))
+    B = B if B.shape[0] == kb else rng.standard_normal((kb, N))
+    dA, dB = engine.upload(A), engine.upload(B)
+    c64 = engine.gram(g, dA, N, ka, dB, N, kb, precision=0)
+    ctc = engine.gram(g, dA, N, ka, dB, N, kb, precision=1)
+    dV = g.getDx() * g.getDy() * g.getDz()
+    ref = A @ B.T * dV
+    assert np.max(np.abs(c64 - ref)) < 1e-10 * np.max(np.abs(ref))
+    assert np.max(np.abs(ctc - c64)) < 1e-5 * np.max(np.abs(c64))
+
+
+def test_mixed_precision_eigensolver(engine, port):
+    n, b = (32, 30, 28), (-5.0, 5.0, -4.6, 4.6, -4.2, 4.2)
+    g = dft_b200.CartesianGrid(*n, *b)
+    N = g.getSize()
+    Z, xyz = [8, 1, 1], np.array([0.05, 0.07, 0.03, 1.43, 0.07, 1.1, -1.43, 0.07, 1.1])
+    V = port.nuclear_potential(n, b, Z, xyz)
+    res = {}
+    for mixed in (0, 1):
+        psi = engine.array(8 * N)
+        eig, it = engine.solve_orbitals(g, engine.upload(V), 5, 8, psi, N, mixed_precision=mixed)
+        res[mixed] = eig
+    assert np.max(np.abs(res[1][:5] - res[0][:5])) < 1e-9
