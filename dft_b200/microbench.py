@@ -5,6 +5,7 @@
     python -m dft_b200.microbench xc     --n 128 --functional PBE96
     python -m dft_b200.microbench scf    --n 48  [--iterations 1]     # H2 at h = 0.3 (n = 48)
     python -m dft_b200.microbench radial                              # 60 atoms, one launch
+    python -m dft_b200.microbench gram   --n 64 --ka 64 --kb 64 --precision 1   # tcgen05 Gram
 
 Each mode prints one JSON line with the time and the achieved bandwidth for the
 operator's algorithmic bytes.  Used for roofline numbers and as the command under ncu.
@@ -43,7 +44,11 @@ def cube(n, h):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial"])
+    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram"])
+    ap.add_argument("--ka", type=int, default=64)
+    ap.add_argument("--kb", type=int, default=64)
+    ap.add_argument("--precision", type=int, default=0, help="gram: 0 = FP64, 1 = tensor cores (TF32 hi+lo)")
+    ap.add_argument("--mixed", type=int, default=0, help="scf: mixed-precision eigensolver")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--h", type=float, default=0.2)
     ap.add_argument("--bands", type=int, default=16)
@@ -110,6 +115,7 @@ def main():
         o = d.default_scf_options(max_iterations=a.iterations, extra_bands=w["extra_bands"], verbose=int(a.verbose),
                                   stop_abs_de=a.stop_abs_de)
         o.eig.verbose = int(a.verbose > 1)
+        o.eig.mixed_precision = a.mixed
         r = eng.scf_molecule(g, m, 0, w["multiplicity"], w["functional"], o)
         out.update(system=a.system, iterations=r.iterations, converged=r.converged, energy=r.total,
                    seconds=r.seconds, launches=eng.launches, eigenvalues=r.eigenvalues[:8],
@@ -117,6 +123,18 @@ def main():
                                                "ks_residual", "poisson_sweeps_in", "poisson_sweeps_out",
                                                "eig_iterations_alpha", "ms_hartree", "ms_xc", "ms_orbitals",
                                                "ms_density", "ms_energy", "ms_total")} for h in r.history])
+    elif a.mode == "gram":
+        g = cube(a.n, a.h)
+        N = g.getSize()
+        ka, kb = a.ka, a.kb
+        rng = np.random.default_rng(0)
+        A = eng.upload(rng.standard_normal(N * ka))
+        B = eng.upload(rng.standard_normal(N * kb))
+        t = _events(torch, stream, lambda: eng.gram(g, A, N, ka, B, N, kb, precision=a.precision), a.reps, flush)
+        ms = statistics.median(t)
+        flops = 2.0 * N * ka * kb
+        out.update(n=a.n, ka=ka, kb=kb, precision=a.precision, ms=ms, tflops=flops / (ms * 1e-3) / 1e12,
+                   gbs=8.0 * N * (ka + kb) / (ms * 1e-3) / 1e9)
     elif a.mode == "radial":
         Zs = list(range(1, 31)) * 2
         ks = ["PZ81"] * 30 + ["PBE96"] * 30
