@@ -44,7 +44,32 @@ class dft_scf_opts(C.Structure):
     _fields_ = [("max_iterations", C.c_int), ("energy_tol", C.c_double), ("density_tol", C.c_double),
                 ("ks_tol", C.c_double), ("stop_abs_de", C.c_double), ("poisson_tol", C.c_double),
                 ("poisson_max_sweeps", C.c_long), ("extra_bands", C.c_int), ("eig", dft_eig_opts),
-                ("verbose", C.c_int)]
+                ("verbose", C.c_int), ("poisson_start", C.c_int), ("poisson_net", C.c_void_p)]
+
+
+# dft_poisson_start
+POISSON_COLD, POISSON_PREVIOUS, POISSON_NETWORK, POISSON_COARSE, POISSON_HYBRID, POISSON_MULTIGRID = 0, 1, 2, 3, 4, 5
+
+
+class dft_poisson_start_info(C.Structure):
+    _fields_ = [("coarse_cycles", C.c_long), ("multigrid_cycles", C.c_int), ("residual", C.c_double),
+                ("scale", C.c_double)]
+
+
+class dft_pnet_train_opts(C.Structure):
+    _fields_ = [("samples", C.c_int), ("validation", C.c_int), ("epochs", C.c_int), ("batch", C.c_int),
+                ("lr", C.c_double), ("lr_min", C.c_double), ("seed", C.c_ulonglong), ("target_tol", C.c_double),
+                ("target_max_sweeps", C.c_long), ("ngrids", C.c_int), ("grids", dft_grid * 4), ("kmin", C.c_int),
+                ("kmax", C.c_int), ("wmin", C.c_double), ("wmax", C.c_double), ("ne_min", C.c_int),
+                ("ne_max", C.c_int), ("smooth_sweeps", C.c_int), ("mse_weight", C.c_double), ("verbose", C.c_int)]
+
+
+class dft_pnet_train_report(C.Structure):
+    _fields_ = [("steps", C.c_int), ("seconds_data", C.c_double), ("seconds_train", C.c_double),
+                ("ms_per_step", C.c_double), ("mean_target_sweeps", C.c_double),
+                ("train_loss_first_epoch", C.c_double), ("train_loss_last_epoch", C.c_double),
+                ("val_loss", C.c_double), ("val_loss_coarse", C.c_double), ("epoch_loss", C.POINTER(C.c_double)),
+                ("epoch_loss_capacity", C.c_int)]
 
 
 class dft_scf_iteration(C.Structure):
@@ -111,6 +136,21 @@ _SIGS = {
                           C.POINTER(dft_scf_opts), C.POINTER(dft_scf_result)], C.c_int),
     "dft_solve_atoms": ([_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_long, C.c_double,
                          C.POINTER(dft_atom_result)], C.c_int),
+    "dft_hartree_from_guess_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double, C.c_long, C.POINTER(C.c_long),
+                                    _D], C.c_int),
+    "dft_pnet_create": ([_P, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)], C.c_int),
+    "dft_pnet_destroy": ([_P], C.c_int),
+    "dft_pnet_num_params": ([_P, C.POINTER(C.c_size_t)], C.c_int),
+    "dft_pnet_get_params": ([_P, _P, C.POINTER(C.c_float), C.c_size_t], C.c_int),
+    "dft_pnet_set_params": ([_P, _P, C.POINTER(C.c_float), C.c_size_t], C.c_int),
+    "dft_pnet_loss_grad": ([_P, _P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), _D,
+                            C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+    "dft_poisson_start_dev": ([_P, C.POINTER(dft_grid), _P, _P, _P, C.c_int, C.POINTER(dft_poisson_start_info)],
+                              C.c_int),
+    "dft_synthetic_density_dev": ([_P, C.POINTER(dft_grid), C.c_ulonglong, C.c_int, C.c_int, C.c_double,
+                                   C.c_double, C.c_int, C.c_int, _P, C.POINTER(C.c_int)], C.c_int),
+    "dft_pnet_train_poisson": ([_P, _P, C.POINTER(dft_pnet_train_opts), C.POINTER(dft_pnet_train_report)],
+                               C.c_int),
 }
 
 _lib = None
@@ -326,6 +366,31 @@ class Engine:
                                       C.byref(ld)))
         return sw.value, ld.value
 
+    def hartree_from_guess(self, grid, rho, vh, tol=1e-8, max_sweeps=10000):
+        """Jacobi from the interior of vh (in/out) with the reference's stop rule."""
+        g = grid.c()
+        sw = C.c_long()
+        ld = C.c_double()
+        _check(load().dft_hartree_from_guess_dev(self.ctx, C.byref(g), _ptr(rho), _ptr(vh), tol, max_sweeps,
+                                                 C.byref(sw), C.byref(ld)))
+        return sw.value, ld.value
+
+    def poisson_start(self, grid, net, rho, out, multigrid_cycles=0) -> dict:
+        """Start values for the Jacobi solve into out (device): nested coarse grids, plus the
+        network's correction (net not None), then up to multigrid_cycles V-cycles."""
+        g = grid.c()
+        info = dft_poisson_start_info()
+        _check(load().dft_poisson_start_dev(self.ctx, C.byref(g), net.handle if net is not None else None, _ptr(rho),
+                                            _ptr(out), int(multigrid_cycles), C.byref(info)))
+        return {k: getattr(info, k) for k, _ in dft_poisson_start_info._fields_}
+
+    def synthetic_density(self, grid, seed, out, kmin=1, kmax=8, wmin=0.3, wmax=2.0, ne_min=2, ne_max=40) -> int:
+        g = grid.c()
+        ne = C.c_int()
+        _check(load().dft_synthetic_density_dev(self.ctx, C.byref(g), int(seed), kmin, kmax, wmin, wmax, ne_min,
+                                                ne_max, _ptr(out), C.byref(ne)))
+        return ne.value
+
     def hartree_energy(self, grid, rho, vh) -> float:
         g = grid.c()
         e = C.c_double()
@@ -411,6 +476,89 @@ class Engine:
         return [AtomResult.from_c(o) for o in out]
 
 
+class PoissonNet:
+    """The learned Poisson start's network (dft_pnet) on one engine."""
+
+    def __init__(self, engine: "Engine", seed: int = 1, in_channels: int = 2):
+        self.engine = engine
+        h = C.c_void_p()
+        _check(load().dft_pnet_create(engine.ctx, in_channels, int(seed), C.byref(h)))
+        self.handle = h.value
+
+    def close(self):
+        if self.handle:
+            load().dft_pnet_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_params(self) -> int:
+        n = C.c_size_t()
+        _check(load().dft_pnet_num_params(self.handle, C.byref(n)))
+        return n.value
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.num_params, dtype=np.float32)
+        _check(load().dft_pnet_get_params(self.engine.ctx, self.handle, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                          out.size))
+        return out
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(load().dft_pnet_set_params(self.engine.ctx, self.handle, p.ctypes.data_as(C.POINTER(C.c_float)),
+                                          p.size))
+
+    def save(self, path: str) -> None:
+        np.save(path, self.get_params())
+
+    def load(self, path: str) -> None:
+        self.set_params(np.load(path))
+
+    def loss_grad(self, shape, x, t):
+        """One forward/backward pass on a host volume: x (N, channels), t (N) -> (loss, grad, y)."""
+        nx, ny, nz = shape
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        grad = np.zeros(self.num_params, dtype=np.float32)
+        y = np.zeros(nx * ny * nz, dtype=np.float32)
+        loss = C.c_double()
+        fp = C.POINTER(C.c_float)
+        _check(load().dft_pnet_loss_grad(self.engine.ctx, self.handle, nx, ny, nz, x.ctypes.data_as(fp),
+                                         t.ctypes.data_as(fp), C.byref(loss), grad.ctypes.data_as(fp),
+                                         y.ctypes.data_as(fp)))
+        return loss.value, grad, y
+
+    def train(self, grids, samples=256, validation=32, epochs=10, batch=4, lr=2e-3, lr_min=5e-5, seed=2026,
+              target_tol=1e-10, target_max_sweeps=200000, kmin=1, kmax=8, wmin=0.3, wmax=2.0, ne_min=2, ne_max=40,
+              smooth_sweeps=64, mse_weight=0.1, verbose=False) -> dict:
+        o = dft_pnet_train_opts()
+        o.samples, o.validation, o.epochs, o.batch = samples, validation, epochs, batch
+        o.lr, o.lr_min, o.seed = lr, lr_min, seed
+        o.target_tol, o.target_max_sweeps = target_tol, target_max_sweeps
+        if not 1 <= len(grids) <= 4:
+            raise ValueError("1 to 4 training grids")
+        o.ngrids = len(grids)
+        for i, g in enumerate(grids):
+            o.grids[i] = g.c()
+        o.kmin, o.kmax, o.wmin, o.wmax, o.ne_min, o.ne_max = kmin, kmax, wmin, wmax, ne_min, ne_max
+        o.smooth_sweeps, o.mse_weight = smooth_sweeps, mse_weight
+        o.verbose = int(verbose)
+        r = dft_pnet_train_report()
+        hist = (C.c_double * epochs)()
+        r.epoch_loss = C.cast(hist, C.POINTER(C.c_double))
+        r.epoch_loss_capacity = epochs
+        _check(load().dft_pnet_train_poisson(self.engine.ctx, self.handle, C.byref(o), C.byref(r)))
+        out = {k: getattr(r, k) for k, _ in dft_pnet_train_report._fields_ if k not in ("epoch_loss",
+                                                                                      "epoch_loss_capacity")}
+        out["epoch_loss"] = list(hist)
+        return out
+
+
 def _ptr(x):
     if x is None:
         return None
@@ -427,6 +575,8 @@ def default_scf_options(**kw) -> dft_scf_opts:
     o = dft_scf_opts()
     load().dft_scf_default_options(C.byref(o))
     for k, v in kw.items():
+        if k == "poisson_net" and hasattr(v, "handle"):
+            v = v.handle
         if k.startswith("eig_"):
             setattr(o.eig, k[4:], v)
         else:

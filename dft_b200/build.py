@@ -33,6 +33,8 @@ SOURCES = {
     "scf.cu": [],
     "radial.cu": ["-fmad=false"],
     "gram_tc.cu": [],
+    "neural.cu": [],
+    "poisson_start.cu": [],
     "eigh.cpp": [],
 }
 

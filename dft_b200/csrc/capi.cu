@@ -3,6 +3,7 @@
 #include <cstring>
 #include <string>
 
+#include "neural.h"
 #include "ops.h"
 
 namespace {
@@ -190,6 +191,19 @@ dft_status_t dft_hartree_dev(dft_context* ctx, const dft_grid* g, const double* 
     });
 }
 
+dft_status_t dft_hartree_from_guess_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh,
+                                        double tol, long max_sweeps, long* sweeps_out, double* last_diff_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && rho && vh, "NULL argument");
+        NEED(rho != vh, "rho and vh must not alias");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::JacobiResult r = dftb::hartree(ctx, G, rho, vh, tol, max_sweeps, vh);
+        dftb::sync(ctx);
+        if (sweeps_out) *sweeps_out = r.sweeps;
+        if (last_diff_out) *last_diff_out = r.last_diff;
+    });
+}
+
 dft_status_t dft_hartree_noalloc_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
                                      long max_sweeps, long* sweeps_out, double* last_diff_out) {
     return guard(ctx, [&] {
@@ -331,3 +345,85 @@ dft_status_t dft_solve_atoms(dft_context* ctx, int nruns, const int* Z, const in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- learned Poisson start --
+dft_status_t dft_pnet_create(dft_context* ctx, int in_channels, unsigned long long seed, dft_pnet** out) {
+    return guard(ctx, [&] {
+        NEED(ctx && out, "NULL argument");
+        *out = dftb::pnet_create(ctx, in_channels, seed);
+    });
+}
+
+dft_status_t dft_pnet_destroy(dft_pnet* net) {
+    return guard(nullptr, [&] { dftb::pnet_destroy(net); });
+}
+
+dft_status_t dft_pnet_num_params(const dft_pnet* net, size_t* n) {
+    return guard(nullptr, [&] {
+        NEED(net && n, "NULL argument");
+        *n = dftb::pnet_num_params(net);
+    });
+}
+
+dft_status_t dft_pnet_get_params(dft_context* ctx, dft_pnet* net, float* host, size_t n) {
+    return guard(ctx, [&] {
+        NEED(ctx && net && host, "NULL argument");
+        NEED(n == dftb::pnet_num_params(net), "parameter count mismatch");
+        dftb::pnet_get_params(ctx, net, host);
+    });
+}
+
+dft_status_t dft_pnet_set_params(dft_context* ctx, dft_pnet* net, const float* host, size_t n) {
+    return guard(ctx, [&] {
+        NEED(ctx && net && host, "NULL argument");
+        NEED(n == dftb::pnet_num_params(net), "parameter count mismatch");
+        dftb::pnet_set_params(ctx, net, host);
+    });
+}
+
+dft_status_t dft_pnet_loss_grad(dft_context* ctx, dft_pnet* net, int nx, int ny, int nz, const float* x,
+                                const float* t, double* loss, float* grad, float* y) {
+    return guard(ctx, [&] {
+        NEED(ctx && net && x && t, "NULL argument");
+        dftb::pnet_loss_grad(ctx, net, nx, ny, nz, x, t, loss, grad, y);
+    });
+}
+
+dft_status_t dft_poisson_start_dev(dft_context* ctx, const dft_grid* g, dft_pnet* net, const double* rho,
+                                   double* vstart, int multigrid_cycles, dft_poisson_start_info* info) {
+    return guard(ctx, [&] {
+        NEED(ctx && rho && vstart, "NULL argument");
+        NEED(rho != vstart, "rho and vstart must not alias");
+        NEED(multigrid_cycles >= 0, "multigrid_cycles must be >= 0");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::PoissonGuessInfo pi;
+        dftb::poisson_start(ctx, net, G, rho, vstart, multigrid_cycles, &pi);
+        dftb::sync(ctx);
+        if (info) {
+            info->coarse_cycles = pi.coarse_cycles;
+            info->multigrid_cycles = pi.cycles;
+            info->residual = pi.residual;
+            info->scale = pi.scale;
+        }
+    });
+}
+
+dft_status_t dft_synthetic_density_dev(dft_context* ctx, const dft_grid* g, unsigned long long seed, int kmin,
+                                       int kmax, double wmin, double wmax, int ne_min, int ne_max, double* rho,
+                                       int* ne_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && rho, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        const int ne = dftb::synthetic_density(ctx, G, seed, kmin, kmax, wmin, wmax, ne_min, ne_max, rho);
+        dftb::sync(ctx);
+        if (ne_out) *ne_out = ne;
+    });
+}
+
+dft_status_t dft_pnet_train_poisson(dft_context* ctx, dft_pnet* net, const dft_pnet_train_opts* opts,
+                                    dft_pnet_train_report* report) {
+    return guard(ctx, [&] {
+        NEED(ctx && net && opts && report, "NULL argument");
+        dftb::pnet_train_poisson(ctx, net, opts, report);
+    });
+}

@@ -126,6 +126,11 @@ enum WsSlot {
     WS_DAV6 = 16,    // Davidson per-band scalars on device
     WS_SCF2 = 17,
     WS_SCF3 = 18,
+    WS_PG0 = 19,     // coarse-grid Poisson start (neural.cu)
+    WS_PG1 = 20,
+    WS_PG2 = 21,
+    WS_PG3 = 22,
+    WS_PG4 = 23,
     WS_NUM = 24,
 };
 

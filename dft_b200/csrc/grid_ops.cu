@@ -234,16 +234,19 @@ struct JacobiCtrl {
     double last_diff;              // max |dV| of the last completed sweep
 };
 
-// Boundary fill, reference HartreePotentialMolecule.cpp:37-95 and :171-202.  Interior = 0.
-// x_i = xmin + i*dx exactly as CartesianGrid::getX; Q is the total charge.
-__global__ void jacobi_init_kernel(Grid g, double Q, double* a, double* b) {
+// Boundary fill, reference HartreePotentialMolecule.cpp:37-95 and :171-202.  Interior = 0
+// (the reference's cold start, :152-155) or, for a warm start, the interior of `guess`
+// (which may alias `a`).  x_i = xmin + i*dx exactly as CartesianGrid::getX; Q is the total charge.
+__global__ void jacobi_init_kernel(Grid g, double Q, double* a, double* b, const double* guess) {
     const long long n = g.N;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(p % g.nx);
         const int j = (int)((p / g.nx) % g.ny);
         const int k = (int)(p / ((long long)g.nx * g.ny));
         double v = 0.0;
-        if (i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz) {
+        const bool face = i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz;
+        if (!face && guess) v = guess[p];
+        if (face) {
             const double x = __dadd_rn(g.xmin, __dmul_rn((double)i, g.dx));
             const double y = __dadd_rn(g.ymin, __dmul_rn((double)j, g.dy));
             const double z = __dadd_rn(g.zmin, __dmul_rn((double)k, g.dz));
@@ -850,15 +853,20 @@ static JacobiResult hartree_tb(dft_context* ctx, const Grid& g, const double* rh
     return {(long)hc->sweep, hc->last_diff};
 }
 
-JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol, long max_sweeps) {
+bool faces_exact(const Grid& g) {
+    return (g.xmin + (double)(g.nx - 1) * g.dx == g.xmax) && (g.ymin + (double)(g.ny - 1) * g.dy == g.ymax) &&
+           (g.zmin + (double)(g.nz - 1) * g.dz == g.zmax);
+}
+
+JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol, long max_sweeps,
+                     const double* guess, bool zero_faces) {
     if (max_sweeps < 0) fail(DFT_INVALID_ARGUMENT, "max_sweeps must be >= 0");
     double* buf1 = (double*)ws_get(ctx, WS_JACOBI, sizeof(double) * (size_t)g.N);
     JacobiCtrl* ctrl = (JacobiCtrl*)ws_get(ctx, WS_CTRL, sizeof(JacobiCtrl) + 64);
     // Boundary values are Q/|r| only on faces whose last node misses the bound by rounding
     // (reference :60-79); on every grid whose x_{n-1} == xmax they are all zero and Q is unused.
-    const bool exact_faces = (g.xmin + (double)(g.nx - 1) * g.dx == g.xmax) &&
-                             (g.ymin + (double)(g.ny - 1) * g.dy == g.ymax) &&
-                             (g.zmin + (double)(g.nz - 1) * g.dz == g.zmax);
+    // zero_faces forces the zero boundary (Q = 0) whatever the rounding.
+    const bool exact_faces = zero_faces || faces_exact(g);
     double Q = 0.0;
     if (!exact_faces) {
         double* q = (double*)ws_get(ctx, WS_TMP2, sizeof(double));
@@ -870,7 +878,7 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
         sync(ctx);
         Q = h[0];
     }
-    jacobi_init_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, Q, vh, buf1);
+    jacobi_init_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, Q, vh, buf1, guess);
     DFT_LAUNCH_CHECK();
     count_launch(ctx);
     DFT_CUDA(cudaMemsetAsync(ctrl, 0, sizeof(JacobiCtrl), ctx->stream));
@@ -981,7 +989,7 @@ JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho,
         DFT_CUDA(cudaMemcpyAsync(&Q, qslot, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         sync(ctx);
     }
-    jacobi_init_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, Q, vh, buf1);
+    jacobi_init_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, Q, vh, buf1, nullptr);
     DFT_LAUNCH_CHECK();
     count_launch(ctx);
     // the array keeps the previous call's control words: clear them

@@ -17,7 +17,12 @@ struct JacobiResult {
     long sweeps;
     double last_diff;
 };
-JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol, long max_sweeps);
+// guess: nullptr = the reference's cold start; otherwise the interior start values (may be vh).
+// zero_faces: zero boundary values even where the reference's rule would give Q/|r|.
+JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol, long max_sweeps,
+                     const double* guess = nullptr, bool zero_faces = false);
+// true when every face's last node lands exactly on the bound (the reference's boundary is then zero)
+bool faces_exact(const Grid& g);
 // The same solve on the library's fixed scratch array: no device allocation (grid_ops.cu).
 JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol,
                              long max_sweeps);

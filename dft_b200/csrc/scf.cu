@@ -8,6 +8,7 @@
 #include <limits>
 #include <vector>
 
+#include "neural.h"
 #include "ops.h"
 
 namespace dftb {
@@ -75,7 +76,35 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     eo.mixed_precision = o.eig.mixed_precision;
     eo.verbose = o.eig.verbose;
 
+    const int pstart = o.poisson_start;
+    if (pstart < DFT_POISSON_COLD || pstart > DFT_POISSON_MULTIGRID)
+        fail(DFT_INVALID_ARGUMENT, "unknown poisson_start %d", pstart);
+    if (pstart == DFT_POISSON_NETWORK && !o.poisson_net)
+        fail(DFT_INVALID_ARGUMENT, "poisson_start DFT_POISSON_NETWORK needs poisson_net");
+
     DevBuf vext(N), da(N), db(N), rho(N), vh(N), vxa(N), vxb(N), va(N), vb(N), oa(N), ob(N), orho(N), ovh(N);
+    DevBuf vstart(pstart >= DFT_POISSON_NETWORK ? (size_t)N : 0);
+    dft_pnet* net = pstart == DFT_POISSON_COARSE ? nullptr : o.poisson_net;
+    // Poisson solve of density d into v with the chosen start; `have_prev` says whether v
+    // still holds this slot's potential from the previous iteration.
+    auto poisson = [&](const double* d, double* v, bool have_prev) {
+        const double* start = nullptr;
+        if (pstart == DFT_POISSON_MULTIGRID) {
+            if (have_prev) {
+                DFT_CUDA(cudaMemcpyAsync(vstart.p, v, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+                multigrid(ctx, g, d, vstart.p, 0.5 * o.poisson_tol, 40, nullptr);
+            } else {
+                poisson_start(ctx, net, g, d, vstart.p, 40, nullptr);
+            }
+            start = vstart.p;
+        } else if ((pstart == DFT_POISSON_PREVIOUS || pstart == DFT_POISSON_HYBRID) && have_prev) {
+            start = v;
+        } else if (pstart >= DFT_POISSON_NETWORK) {
+            poisson_start(ctx, net, g, d, vstart.p, 0, nullptr);
+            start = vstart.p;
+        }
+        return hartree(ctx, g, d, v, o.poisson_tol, o.poisson_max_sweeps, start);
+    };
     DevBuf psia((size_t)bands_a * ld), psib(closed ? 0 : (size_t)bands_b * ld);
     std::vector<double> eiga(bands_a), eigb(bands_b), resa(bands_a), resb(bands_b);
     std::vector<double> occa(bands_a, 0.0), occb(bands_b, 0.0);
@@ -123,7 +152,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         // n -> V_H(n) (MolecularSCFIteration.cpp:45-66)
         auto t0 = Clock::now();
         add2(ctx, N, da.p, db.p, rho.p);
-        JacobiResult jin = hartree(ctx, g, rho.p, vh.p, o.poisson_tol, o.poisson_max_sweeps);
+        JacobiResult jin = poisson(rho.p, vh.p, it > 1);
         sync(ctx);
         rec.ms_hartree = ms_since(t0);
         rec.poisson_sweeps_in = jin.sweeps;
@@ -146,7 +175,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         if (closed) DFT_CUDA(cudaMemcpyAsync(ob.p, oa.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
         else spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), ob.p);
         add2(ctx, N, oa.p, ob.p, orho.p);
-        JacobiResult jout = hartree(ctx, g, orho.p, ovh.p, o.poisson_tol, o.poisson_max_sweeps);
+        JacobiResult jout = poisson(orho.p, ovh.p, it > 1);
         sync(ctx);
         rec.ms_density = ms_since(t0);
         rec.poisson_sweeps_out = jout.sweeps;

@@ -49,6 +49,7 @@ typedef struct {
 } dft_grid;
 
 typedef struct dft_context dft_context;
+typedef struct dft_pnet dft_pnet; /* learned Poisson start network (see the end of this header) */
 
 const char* dft_last_error_message(void);
 const char* dft_version(void);
@@ -170,6 +171,17 @@ dft_status_t dft_solve_orbitals_dev(dft_context* ctx, const dft_grid* g, const d
 
 /* ---- SCF drivers (host in, host out) ------------------------------------------------- */
 
+typedef enum {
+    DFT_POISSON_COLD = 0,     /* zero interior, as HartreePotentialMolecule.cpp:152-155 */
+    DFT_POISSON_PREVIOUS = 1, /* the previous SCF iteration's potential for the same density slot */
+    DFT_POISSON_NETWORK = 2,  /* coarse-grid solve plus the network's correction (dft_poisson_start_dev) */
+    DFT_POISSON_COARSE = 3,   /* coarse-grid solve alone */
+    DFT_POISSON_HYBRID = 4,   /* DFT_POISSON_NETWORK (coarse alone when poisson_net is NULL) for the
+                                 first solve of each density slot, DFT_POISSON_PREVIOUS afterwards */
+    DFT_POISSON_MULTIGRID = 5 /* multigrid cycles from the previous potential (first solve: from the
+                                 coarse or network start), then Jacobi with the unchanged stop rule */
+} dft_poisson_start;
+
 typedef struct {
     int max_iterations;      /* 250 (DFTConstants.h:13) */
     double energy_tol;       /* 1e-11 (DFTConstants.h:16) */
@@ -181,6 +193,10 @@ typedef struct {
     int extra_bands;         /* unoccupied buffer bands per spin in the block eigensolver */
     dft_eig_opts eig;        /* eigensolver options (tol = 1e-7 reproduces the reference) */
     int verbose;             /* 1: one line per SCF iteration on stderr */
+    /* Start of each Poisson solve (no counterpart in the reference, which always starts
+     * from zero): DFT_POISSON_COLD reproduces the reference. */
+    int poisson_start;       /* dft_poisson_start */
+    dft_pnet* poisson_net;   /* network for DFT_POISSON_NETWORK (not owned) */
 } dft_scf_opts;
 
 /* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)
@@ -240,6 +256,89 @@ typedef struct {
  * persistent kernel launch, one thread block per run.  results: host array of nruns. */
 dft_status_t dft_solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, long points, double rmax,
                              dft_atom_result* results);
+
+/* ---- learned Poisson start (no counterpart in the reference) ------------------------- */
+/* A coarse grid with the same bounds and about a quarter of the points per axis carries the
+ * long-range part of V_H: the density is restricted to it with the transposed trilinear
+ * weights (charge-conserving), solved there by the same Jacobi kernels and interpolated back.
+ * A 3-level convolutional network (BF16 activations, FP32 accumulation, about 1.5e5
+ * parameters) predicts the remaining short-range correction from the density and the
+ * interpolated coarse potential.  Jacobi then runs from that start with the unchanged stop
+ * rule.  Parameters are FP32 on the host side of these calls. */
+
+dft_status_t dft_pnet_create(dft_context* ctx, int in_channels, unsigned long long seed, dft_pnet** out);
+dft_status_t dft_pnet_destroy(dft_pnet* net);
+dft_status_t dft_pnet_num_params(const dft_pnet* net, size_t* n);
+dft_status_t dft_pnet_get_params(dft_context* ctx, dft_pnet* net, float* host, size_t n);
+dft_status_t dft_pnet_set_params(dft_context* ctx, dft_pnet* net, const float* host, size_t n);
+
+/* One forward and backward pass on an (nx, ny, nz) volume: input x[N][in_channels] and
+ * target t[N] (host, x fastest), loss = mean over interior points of (y - t)^2.  Returns the
+ * loss, the parameter gradient (host, num_params, may be NULL) and y (host, N, may be NULL).
+ * Inputs are rounded to BF16 as the network stores them. */
+dft_status_t dft_pnet_loss_grad(dft_context* ctx, dft_pnet* net, int nx, int ny, int nz, const float* x,
+                                const float* t, double* loss, float* grad, float* y);
+
+typedef struct {
+    long coarse_cycles;   /* multigrid cycles spent on the coarse levels */
+    int multigrid_cycles; /* V-cycles run */
+    double residual;      /* size of the next Jacobi update after them */
+    double scale;         /* max |first coarse level's potential|: the network's input/output scale */
+} dft_poisson_start_info;
+
+/* Start values for the Jacobi solve of density rho (device): the nested coarse-grid solution
+ * (full multigrid over grids of about half the points per axis each) interpolated to g, plus the network's correction when net is not NULL, then up to
+ * multigrid_cycles V(2,2) cycles (stopping once the next Jacobi update would be below
+ * 0.5e-8).  vstart: device, N doubles, faces zero (grids whose last nodes land on the bounds).
+ * info may be NULL. */
+dft_status_t dft_poisson_start_dev(dft_context* ctx, const dft_grid* g, dft_pnet* net, const double* rho,
+                                   double* vstart, int multigrid_cycles, dft_poisson_start_info* info);
+
+/* calculateHartreePotential from a given start: the interior of vh (device, in/out) is the
+ * first iterate, the faces get the reference's boundary values; same stop rule and cap. */
+dft_status_t dft_hartree_from_guess_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh,
+                                        double tol, long max_sweeps, long* sweeps_out, double* last_diff_out);
+
+/* Seeded synthetic density: kmin..kmax Gaussians with centres uniform in the box, widths
+ * uniform in [wmin, wmax] bohr, positive random weights, normalised so sum rho dV is an
+ * electron count drawn from ne_min..ne_max (returned in ne_out, may be NULL). */
+dft_status_t dft_synthetic_density_dev(dft_context* ctx, const dft_grid* g, unsigned long long seed, int kmin,
+                                       int kmax, double wmin, double wmax, int ne_min, int ne_max, double* rho,
+                                       int* ne_out);
+
+typedef struct {
+    int samples;             /* synthetic densities, each solved to target_tol */
+    int validation;          /* of which the last ones are held out */
+    int epochs;
+    int batch;               /* samples per optimiser step */
+    double lr, lr_min;       /* Adam step size, cosine-decayed from lr to lr_min */
+    unsigned long long seed;
+    double target_tol;       /* Jacobi tolerance of the targets */
+    long target_max_sweeps;
+    int ngrids;              /* 1..4 grids, used in turn */
+    dft_grid grids[4];
+    int kmin, kmax;          /* Gaussians per density */
+    double wmin, wmax;       /* widths (bohr) */
+    int ne_min, ne_max;      /* electrons per density */
+    int smooth_sweeps;       /* k: the loss adds mean((J^k e)^2), J a Jacobi sweep on the error e */
+    double mse_weight;       /* weight of the plain mean(e^2) term */
+    int verbose;
+} dft_pnet_train_opts;
+
+typedef struct {
+    int steps;
+    double seconds_data, seconds_train, ms_per_step;
+    double mean_target_sweeps;
+    double train_loss_first_epoch, train_loss_last_epoch;
+    double val_loss;         /* network */
+    double val_loss_coarse;  /* zero correction: the coarse start alone */
+    double* epoch_loss;      /* optional host array, epoch_loss_capacity entries */
+    int epoch_loss_capacity;
+} dft_pnet_train_report;
+
+/* Trains the network on the device with its own forward, backward and Adam kernels. */
+dft_status_t dft_pnet_train_poisson(dft_context* ctx, dft_pnet* net, const dft_pnet_train_opts* opts,
+                                    dft_pnet_train_report* report);
 
 #ifdef __cplusplus
 }
