@@ -35,6 +35,7 @@ SOURCES = {
     "gram_tc.cu": [],
     "neural.cu": [],
     "poisson_start.cu": [],
+    "precond_mg.cu": [],
     "eigh.cpp": [],
 }
 

@@ -309,7 +309,9 @@ void rotate(dft_context* ctx, const Grid& g, const double* in, long long ldi, in
 // tc: Gram products on the tensor cores (TF32 hi+lo, ~1e-6 relative) instead of FP64
 void gram_any(bool tc, dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B,
               long long ldb, int kb, std::vector<double>& C) {
-    if (tc) gram_tc(ctx, g, A, lda, ka, B, ldb, kb, C);
+    // the tensor-core product pays only when both blocks are wide enough to fill its tiles;
+    // narrow products (few bands) are latency-bound either way and stay in FP64
+    if (tc && (long long)ka * kb >= 2048) gram_tc(ctx, g, A, lda, ka, B, ldb, kb, C);
     else gram(ctx, g, A, lda, ka, B, ldb, kb, C);
 }
 
@@ -510,10 +512,18 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         }
         double* T = Vb + (long long)k * ld;
         DFT_CUDA(cudaMemcpyAsync(dsrc, active.data(), sizeof(int) * na, cudaMemcpyHostToDevice, ctx->stream));
-        if (o.precond_steps <= 0) {
+        // auto (-2): one multigrid cycle on large grids, where a few smoothing steps no longer
+        // reach the long-wavelength part of the residual; 4 smoothing steps otherwise
+        const int pc = o.precond_steps == -2 ? (g.N >= 80LL * 80 * 80 ? -1 : 4) : o.precond_steps;
+        if (pc == 0) {
             precond_kernel<<<dim3(eb, na), 256, 0, ctx->stream>>>(R, V, dsrc, dtheta, T, ld, g.N, kin);
             DFT_LAUNCH_CHECK();
             count_launch(ctx);
+        } else if (pc < 0) {
+            // one multigrid cycle for (T + sigma_b) t = r_b, sigma_b = max(-theta_b, 1 Ha)
+            std::vector<double> sig(na);
+            for (int a = 0; a < na; ++a) sig[a] = std::max(-theta[active[a]], 1.0);
+            precondition_multigrid(ctx, g, R, dsrc, na, sig.data(), T, ld);
         } else {
             // (T + sigma_b) t = r_b with sigma_b = max(-theta_b, 1 Ha): the far-field (V ~ 0) form of
             // (H - theta_b) for bound states; t0 = r/d, then damped-Jacobi steps (w = 2/3)
@@ -529,13 +539,13 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
             dim3 sgrid(sbx, sby, na * nzc2), sblock(32, 8);
             kinetic_smooth_kernel<<<sgrid, sblock, 0, ctx->stream>>>(g, nullptr, R, dsrc, dsigma, T, ld, zc, nzc2, 1.0);
             double *cur = T, *nxt = W;
-            for (int s = 0; s < o.precond_steps; ++s) {
+            for (int s = 0; s < pc; ++s) {
                 kinetic_smooth_kernel<<<sgrid, sblock, 0, ctx->stream>>>(g, cur, R, dsrc, dsigma, nxt, ld, zc, nzc2,
                                                                          2.0 / 3.0);
                 std::swap(cur, nxt);
             }
             DFT_LAUNCH_CHECK();
-            count_launch(ctx, 1 + o.precond_steps);
+            count_launch(ctx, 1 + pc);
             if (cur != T)
                 DFT_CUDA(cudaMemcpyAsync(T, cur, vecb * na, cudaMemcpyDeviceToDevice, ctx->stream));
         }

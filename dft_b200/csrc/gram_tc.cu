@@ -5,9 +5,10 @@
 // lo = TF32(x - hi)), and the product is formed as hi*hi + hi*lo + lo*hi with FP32
 // accumulation in tensor memory (TMEM): relative error ~1e-6, the "FP32-level" precision the
 // block eigensolver uses while residuals are large.  Per block:
-//   * 128 threads stage a 32-point K slice of A (128 rows) and B (<= 256 rows) from HBM,
+//   * 256 threads stage a 32-point K slice of A (128 rows) and B (<= 256 rows) from HBM,
 //     split them and store hi/lo planes in shared memory in the canonical K-major layout
-//     (8-row x 16-byte core matrices, no swizzle), double-buffered;
+//     (8-row x 16-byte core matrices, no swizzle), double-buffered; the next slice's FP64
+//     values are loaded into registers while the tensor cores consume the current one;
 //   * one thread issues 12 tcgen05.mma.kind::tf32 (4 K=8 steps x 3 products) into a
 //     128 x N FP32 accumulator in TMEM and commits them to an mbarrier;
 //   * after its K range the block reads the accumulator back with tcgen05.ld (each warp its
@@ -24,7 +25,7 @@ namespace dftb {
 
 namespace {
 
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 256;
 constexpr int TC_M = 128;     // accumulator rows (A vectors per tile)
 constexpr int TC_KT = 32;     // points per K slice
 constexpr int TC_NMAX = 256;  // accumulator columns (B vectors per tile)
@@ -95,24 +96,29 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 }
 
 // Gram tile.  grid = (ceil(ka/128), ceil(kb/nt), nchunks); dynamic smem = 2 stages x
-// (A hi, A lo: 128 x 32 fp32; B hi, B lo: ncols x 32 fp32) + 2 mbarriers.
+// (A hi, A lo: 128 x 32 fp32; B hi, B lo: NC x 32 fp32).  Row r of a slice is read by warp
+// r % 8 (one point per lane); each thread holds the next slice's raw FP64 values in
+// registers, loaded while the tensor cores work on the current slice.
+template <int NC>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     gram_tc_kernel(const double* __restrict__ A, long long lda, int ka, const double* __restrict__ B, long long ldb,
-                   int kb, int nt, int ncols, long long n, long long chunk, double* __restrict__ partial,
+                   int kb, int nt, long long n, long long chunk, double* __restrict__ partial,
                    int* __restrict__ error) {
     extern __shared__ __align__(1024) uint32_t sm[];
     __shared__ uint32_t s_tmem;
     __shared__ __align__(8) uint64_t bar[2];
+    constexpr int NW = TC_THREADS / 32;
+    constexpr int RA = TC_M / NW, RB = NC / NW;  // rows per warp
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * TC_M, n0 = blockIdx.y * nt;
     const int mrows = min(TC_M, ka - m0), nrows = min(nt, kb - n0);
     const long long p0 = (long long)blockIdx.z * chunk, p1 = min(n, p0 + chunk);
-    const int a_words = TC_M * TC_KT, b_words = ncols * TC_KT;
-    const int stage_words = 2 * a_words + 2 * b_words;
-    // TMEM: ncols fp32 columns x 128 lanes, allocated by warp 0
+    constexpr int a_words = TC_M * TC_KT, b_words = NC * TC_KT;
+    constexpr int stage_words = 2 * a_words + 2 * b_words;
+    // TMEM: NC fp32 columns x 128 lanes, allocated by warp 0
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(ncols));
+                     "r"(NC));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
@@ -124,7 +130,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    const uint32_t idesc = idesc_tf32(ncols);
+    const uint32_t idesc = idesc_tf32(NC);
+    double xa[RA], xb[RB];
+    auto load = [&](long long ps) {
+        const bool pv = ps + lane < p1;
+#pragma unroll
+        for (int i = 0; i < RA; ++i) {
+            const int r = warp + i * NW;
+            xa[i] = (r < mrows && pv) ? __ldg(A + (long long)(m0 + r) * lda + ps + lane) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < RB; ++i) {
+            const int r = warp + i * NW;
+            xb[i] = (r < nrows && pv) ? __ldg(B + (long long)(n0 + r) * ldb + ps + lane) : 0.0;
+        }
+    };
+    if (p0 < p1) load(p0);
     bool ok = true;
     uint32_t phase[2] = {0, 0};
     bool pending[2] = {false, false};
@@ -142,21 +163,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         uint32_t* alo = ahi + a_words;
         uint32_t* bhi = alo + a_words;
         uint32_t* blo = bhi + b_words;
-        const int kvalid = (int)min((long long)TC_KT, p1 - ps);
-        // stage A: 128 rows x 32 points; a warp reads one row's 32 consecutive points
-        for (int r = warp; r < TC_M; r += TC_THREADS / 32) {
-            const double x = (r < mrows && lane < kvalid) ? __ldg(A + (long long)(m0 + r) * lda + ps + lane) : 0.0;
-            const uint32_t h = to_tf32((float)x);
-            const uint32_t l = to_tf32((float)(x - (double)__uint_as_float(h)));
+#pragma unroll
+        for (int i = 0; i < RA; ++i) {
+            const int r = warp + i * NW;
+            const uint32_t h = to_tf32((float)xa[i]);
+            const uint32_t l = to_tf32((float)(xa[i] - (double)__uint_as_float(h)));
             const int o = kmajor_offset_words(r, lane, TC_M);
             ahi[o] = h;
             alo[o] = l;
         }
-        for (int r = warp; r < ncols; r += TC_THREADS / 32) {
-            const double x = (r < nrows && lane < kvalid) ? __ldg(B + (long long)(n0 + r) * ldb + ps + lane) : 0.0;
-            const uint32_t h = to_tf32((float)x);
-            const uint32_t l = to_tf32((float)(x - (double)__uint_as_float(h)));
-            const int o = kmajor_offset_words(r, lane, ncols);
+#pragma unroll
+        for (int i = 0; i < RB; ++i) {
+            const int r = warp + i * NW;
+            const uint32_t h = to_tf32((float)xb[i]);
+            const uint32_t l = to_tf32((float)(xb[i] - (double)__uint_as_float(h)));
+            const int o = kmajor_offset_words(r, lane, NC);
             bhi[o] = h;
             blo[o] = l;
         }
@@ -165,7 +186,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         __syncthreads();
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t lbo_a = (TC_M / 8) * 128, lbo_b = (uint32_t)(ncols / 8) * 128, sbo = 128;
+            constexpr uint32_t lbo_a = (TC_M / 8) * 128, lbo_b = (uint32_t)(NC / 8) * 128, sbo = 128;
             const uint32_t sa_hi = smem_u32(ahi), sa_lo = smem_u32(alo), sb_hi = smem_u32(bhi), sb_lo = smem_u32(blo);
 #pragma unroll
             for (int kk = 0; kk < TC_KT / 8; ++kk) {
@@ -181,6 +202,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             mma_commit(&bar[st]);
         }
         pending[st] = true;
+        // the next slice's loads overlap the MMAs just issued
+        if (ps + TC_KT < p1) load(ps + TC_KT);
     }
     // drain: wait (bounded) for every stage that still has MMAs in flight
     for (int st = 0; st < 2; ++st)
@@ -193,12 +216,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (!ok) {
         if (tid == 0) atomicExch(error, 1);
     } else if (step > 0) {
-        // accumulator row r = A vector m0 + r lives in TMEM lane r: warp w reads lanes 32w..32w+31
+        // accumulator row r = A vector m0 + r lives in TMEM lane r: warp w reads lanes
+        // 32 (w % 4) .. +31; warps w and w + 4 split the columns
         double* out = partial + (long long)blockIdx.z * ka * kb;
-        const int row = warp * 32 + lane;
-        for (int c0 = 0; c0 < ncols; c0 += 8) {
+        const int q4 = warp & 3, half = warp >> 2;
+        const int row = q4 * 32 + lane;
+        constexpr int CH = NC / (NW / 4);
+        for (int c0 = half * CH; c0 < half * CH + CH; c0 += 8) {
             uint32_t v[8];
-            const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            const uint32_t addr = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)c0;
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
                            "=r"(v[7])
@@ -217,7 +243,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NC));
 }
 
 __global__ void gram_tc_reduce_kernel(int nchunks, int nel, const double* __restrict__ partial, double scale,
@@ -258,12 +284,32 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
     int* err = (int*)(res + nel);
     static bool attr = false;
     if (!attr) {
-        DFT_CUDA(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        DFT_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        DFT_CUDA(cudaFuncSetAttribute(gram_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        DFT_CUDA(cudaFuncSetAttribute(gram_tc_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        DFT_CUDA(cudaFuncSetAttribute(gram_tc_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr = true;
     }
     DFT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
-    gram_tc_kernel<<<dim3(mtiles, ntiles, (unsigned)nch), TC_THREADS, smem, ctx->stream>>>(
-        A, lda, ka, B, ldb, kb, nt, ncols, g.N, chunk, partial, err);
+    const dim3 grid(mtiles, ntiles, (unsigned)nch);
+    switch (ncols) {
+        case 32:
+            gram_tc_kernel<32><<<grid, TC_THREADS, smem, ctx->stream>>>(A, lda, ka, B, ldb, kb, nt, g.N, chunk,
+                                                                        partial, err);
+            break;
+        case 64:
+            gram_tc_kernel<64><<<grid, TC_THREADS, smem, ctx->stream>>>(A, lda, ka, B, ldb, kb, nt, g.N, chunk,
+                                                                        partial, err);
+            break;
+        case 128:
+            gram_tc_kernel<128><<<grid, TC_THREADS, smem, ctx->stream>>>(A, lda, ka, B, ldb, kb, nt, g.N, chunk,
+                                                                         partial, err);
+            break;
+        default:
+            gram_tc_kernel<256><<<grid, TC_THREADS, smem, ctx->stream>>>(A, lda, ka, B, ldb, kb, nt, g.N, chunk,
+                                                                         partial, err);
+            break;
+    }
     DFT_LAUNCH_CHECK();
     const int rb = (int)std::min<size_t>((nel + 7) / 8, 4096);
     gram_tc_reduce_kernel<<<rb, 256, 0, ctx->stream>>>((int)nch, (int)nel, partial, g.dV, res);

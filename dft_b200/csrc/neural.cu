@@ -1157,7 +1157,11 @@ void pnet_train_poisson(dft_context* ctx, dft_pnet* n, const dft_pnet_train_opts
                           o->wmax, o->ne_min, o->ne_max, r);
         double* sdev = nullptr;
         coarse_start(ctx, slab.get(coarse_slab_doubles(g)), g, r, u, &sdev);
-        target_sweeps += hartree(ctx, g, r, v, o->target_tol, o->target_max_sweeps, u).sweeps;
+        // target: the Jacobi fixed point to target_tol, reached by multigrid cycles from the
+        // coarse start and finished by Jacobi sweeps under the stop rule
+        DFT_CUDA(cudaMemcpyAsync(v, u, sizeof(double) * (size_t)g.N, cudaMemcpyDeviceToDevice, ctx->stream));
+        multigrid(ctx, g, r, v, 0.5 * o->target_tol, 100, nullptr);
+        target_sweeps += hartree(ctx, g, r, v, o->target_tol, o->target_max_sweeps, v).sweeps;
         bf16* x = smp->x.get((size_t)g.N * 2);
         float* t = smp->t.get((size_t)g.N);
         net_input(ctx, n, g, r, u, sdev, x);

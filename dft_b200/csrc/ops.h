@@ -65,6 +65,12 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
              int kb, std::vector<double>& C);
 
 // Block Davidson eigensolver (davidson.cu).
+// One multigrid V(2,2) cycle from zero for (T + sigma_a) t_a = r_{src[a]} per band a (T the
+// kinetic operator with psi = 0 outside the box), into T[a*ld ..] (precond_mg.cu).
+// src_dev: device band indices into R; sigma_host: nb shifts (host).
+void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb,
+                            const double* sigma_host, double* T, long long ld);
+
 struct EigOpts {
     double tol = 1e-7;
     int max_iterations = 2000;

@@ -343,8 +343,8 @@ inline int mg_blocks(dft_context* ctx, long long n) {
 
 // ---------------------------------------------------------------- multigrid solve ------
 // V(2,2) cycles with weighted Jacobi (omega = 0.8) on the nested coarse grids, the same
-// charge-conserving restriction and trilinear interpolation, and an exact-enough coarsest
-// solve in shared memory.  Faces of every level are held at zero (the boundary of every grid
+// charge-conserving restriction and trilinear interpolation, and a coarsest-level Jacobi
+// solve in one block's shared memory.  Faces of every level are held at zero (the boundary of every grid
 // whose last nodes land on the bounds).
 struct MGLevel {
     Grid g;
@@ -415,7 +415,9 @@ void vcycle(dft_context* ctx, std::vector<MGLevel>& L, size_t i, double sscale) 
     MGLevel& l = L[i];
     if (i + 1 == L.size()) {
         const size_t sm = sizeof(double) * 2 * (size_t)l.g.N;
-        mg_coarsest_kernel<<<1, 1024, sm, ctx->stream>>>(l.g, l.src, l.v, 4 * (l.g.nx + l.g.ny + l.g.nz) * 4);
+        // the coarsest grid (at most 9 points on its shortest axis) needs only a few hundredths of
+        // its error removed per cycle: 8 sweeps per point of the longest axis
+        mg_coarsest_kernel<<<1, 1024, sm, ctx->stream>>>(l.g, l.src, l.v, 8 * std::max({l.g.nx, l.g.ny, l.g.nz}));
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
         return;

@@ -1,0 +1,293 @@
+// Multigrid preconditioner for the block eigensolver: one V(2,2) cycle from zero for
+// (T + sigma_a) t_a = r_a per correction band, T = -1/2 lap_h with psi = 0 outside the box
+// (the kinetic operator of applyMolecularKohnShamHamiltonian, KohnShamHamiltonianMolecule.cpp:90-166),
+// sigma_a = max(-theta_a, 1 Ha).  All bands advance together: every kernel takes the band
+// index from blockIdx.y.  The reference preconditions with the diagonal of H - theta
+// (EigenvalueSolverMolecule.cpp:521-555); this is an option of the block solver, not the
+// reference's behaviour.
+//
+// Per level the equation is (den + c_a) t_p - sum_nb w_d t_nb = s * src_p over every grid point
+// (neighbours outside the box are zero), with den = 2 (ix2 + iy2 + iz2), w_d = 1/h_d^2,
+// c_a = 2 sigma_a and s = 2 on the finest level (the residual r), 1 on coarse levels.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "neural.h"
+#include "ops.h"
+
+namespace dftb {
+namespace {
+
+__device__ __forceinline__ double nb_sum_open(const Grid& g, const double* v, long long p) {
+    const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((long long)g.nx * g.ny));
+    const long long sxy = (long long)g.nx * g.ny;
+    double s = 0.0;
+    if (i > 0) s += g.ix2 * v[p - 1];
+    if (i + 1 < g.nx) s += g.ix2 * v[p + 1];
+    if (j > 0) s += g.iy2 * v[p - g.nx];
+    if (j + 1 < g.ny) s += g.iy2 * v[p + g.nx];
+    if (k > 0) s += g.iz2 * v[p - sxy];
+    if (k + 1 < g.nz) s += g.iz2 * v[p + sxy];
+    return s;
+}
+
+// out = v + omega ((sum + s src) / (den + c) - v); v == nullptr means v = 0
+__global__ void pc_smooth_kernel(Grid g, long long ld, const double* __restrict__ src, double s,
+                                 const double* __restrict__ shift, const double* __restrict__ v,
+                                 double* __restrict__ out, double omega) {
+    const int a = blockIdx.y;
+    const double d = 2.0 * (g.ix2 + g.iy2 + g.iz2) + shift[a];
+    const double* sa = src + (long long)a * ld;
+    const double* va = v ? v + (long long)a * ld : nullptr;
+    double* oa = out + (long long)a * ld;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        if (!va) {
+            oa[p] = omega * s * sa[p] / d;
+        } else {
+            const double vj = (nb_sum_open(g, va, p) + s * sa[p]) / d;
+            oa[p] = va[p] + omega * (vj - va[p]);
+        }
+    }
+}
+
+// r = s src - ((den + c) v - sum)
+__global__ void pc_residual_kernel(Grid g, long long ld, const double* __restrict__ src, double s,
+                                   const double* __restrict__ shift, const double* __restrict__ v,
+                                   double* __restrict__ r) {
+    const int a = blockIdx.y;
+    const double d = 2.0 * (g.ix2 + g.iy2 + g.iz2) + shift[a];
+    const double* sa = src + (long long)a * ld;
+    const double* va = v + (long long)a * ld;
+    double* ra = r + (long long)a * ld;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x)
+        ra[p] = s * sa[p] - (d * va[p] - nb_sum_open(g, va, p));
+}
+
+// Restriction along one axis (transposed trilinear weights times h/H), per band.
+__global__ void pc_restrict_axis_kernel(const double* __restrict__ in, long long in_ld, double* __restrict__ out,
+                                        long long out_ld, int n0, int n1, int n2, int ax, int nc, double h,
+                                        double H) {
+    const int a = blockIdx.y;
+    in += (long long)a * in_ld;
+    out += (long long)a * out_ld;
+    int od[3] = {n0, n1, n2};
+    const int nf = od[ax];
+    od[ax] = nc;
+    const long long nout = (long long)od[0] * od[1] * od[2];
+    const long long s_in[3] = {1, n0, (long long)n0 * n1};
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nout; q += (long long)gridDim.x * blockDim.x) {
+        int idx[3];
+        idx[0] = (int)(q % od[0]);
+        idx[1] = (int)((q / od[0]) % od[1]);
+        idx[2] = (int)(q / ((long long)od[0] * od[1]));
+        const int I = idx[ax];
+        const double X = I * H;
+        const int flo = max(0, (int)ceil((X - H) / h));
+        const int fhi = min(nf - 1, (int)floor((X + H) / h));
+        long long b = 0;
+        for (int d = 0; d < 3; ++d)
+            if (d != ax) b += idx[d] * s_in[d];
+        double acc = 0.0;
+        for (int fi = flo; fi <= fhi; ++fi) {
+            const double wgt = 1.0 - fabs(fi * h - X) / H;
+            if (wgt > 0.0) acc += wgt * in[b + fi * s_in[ax]];
+        }
+        out[q] = acc * (h / H);
+    }
+}
+
+// v += trilinear interpolation of the coarse correction e, at every fine point
+__global__ void pc_prolong_add_kernel(Grid f, long long fld, Grid c, long long cld, const double* __restrict__ e,
+                                      double* __restrict__ v) {
+    const int a = blockIdx.y;
+    e += (long long)a * cld;
+    v += (long long)a * fld;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < f.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % f.nx), j = (int)((p / f.nx) % f.ny), k = (int)(p / ((long long)f.nx * f.ny));
+        const double u[3] = {i * f.dx / c.dx, j * f.dy / c.dy, k * f.dz / c.dz};
+        const int m[3] = {c.nx, c.ny, c.nz};
+        int I[3];
+        double w[3];
+        for (int d = 0; d < 3; ++d) {
+            I[d] = min(max((int)floor(u[d]), 0), m[d] - 2);
+            w[d] = fmin(fmax(u[d] - I[d], 0.0), 1.0);
+        }
+        double acc = 0.0;
+        for (int t = 0; t < 8; ++t) {
+            const int x = t & 1, y = (t >> 1) & 1, z = t >> 2;
+            const double wt = (x ? w[0] : 1.0 - w[0]) * (y ? w[1] : 1.0 - w[1]) * (z ? w[2] : 1.0 - w[2]);
+            acc += wt * e[((long long)(I[2] + z) * c.ny + (I[1] + y)) * c.nx + (I[0] + x)];
+        }
+        v[p] += acc;
+    }
+}
+
+// Coarsest level: `sweeps` Jacobi sweeps from zero, one block per band, in shared memory.
+constexpr int PC_COARSEST_MAX = 12288;
+__global__ void __launch_bounds__(1024) pc_coarsest_kernel(Grid g, long long ld, const double* __restrict__ src,
+                                                           double s, const double* __restrict__ shift,
+                                                           double* __restrict__ e, int sweeps) {
+    extern __shared__ double sm[];
+    const int a = blockIdx.x;
+    const int n = (int)g.N;
+    src += (long long)a * ld;
+    e += (long long)a * ld;
+    double* x = sm;
+    double* y = sm + n;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) x[p] = 0.0;
+    __syncthreads();
+    const double d = 2.0 * (g.ix2 + g.iy2 + g.iz2) + shift[a];
+    for (int s = 0; s < sweeps; ++s) {
+        const double* cur = (s & 1) ? y : x;
+        double* nxt = (s & 1) ? x : y;
+        for (int p = threadIdx.x; p < n; p += blockDim.x) nxt[p] = (nb_sum_open(g, cur, p) + s * src[p]) / d;
+        __syncthreads();
+    }
+    const double* res = (sweeps & 1) ? y : x;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) e[p] = res[p];
+}
+
+__global__ void pc_gather_kernel(long long n, long long ld, const double* __restrict__ R, const int* __restrict__ srcmap,
+                                 double* __restrict__ out) {
+    const int a = blockIdx.y;
+    const double* r = R + (long long)srcmap[a] * ld;
+    double* o = out + (long long)a * ld;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        o[p] = r[p];
+}
+
+struct PCLevel {
+    Grid g;
+    long long ld;
+    double *src, *v, *tmp, *res, *t1, *t2;
+};
+
+Grid pc_coarse(const Grid& g) {
+    dft_grid d{coarse_points(g.nx), coarse_points(g.ny), coarse_points(g.nz), g.xmin, g.xmax, g.ymin,
+               g.ymax,          g.zmin,          g.zmax};
+    return make_grid(&d);
+}
+
+inline dim3 pc_grid(dft_context* ctx, long long n, int nb) {
+    long long bx = (n + 255) / 256;
+    const long long cap = std::max<long long>(1, (long long)ctx->num_sms * 8 / std::max(nb, 1));
+    bx = std::max<long long>(1, std::min(bx, std::max<long long>(cap, 4)));
+    return dim3((unsigned)bx, (unsigned)nb);
+}
+
+void pc_smooth(dft_context* ctx, PCLevel& l, double s, const double* shift, int nb, int n, bool from_zero) {
+    for (int k = 0; k < n; ++k) {
+        const double* v = (from_zero && k == 0) ? nullptr : l.v;
+        pc_smooth_kernel<<<pc_grid(ctx, l.g.N, nb), 256, 0, ctx->stream>>>(l.g, l.ld, l.src, s, shift, v, l.tmp, 0.8);
+        std::swap(l.v, l.tmp);
+    }
+    count_launch(ctx, n);
+}
+
+void pc_vcycle(dft_context* ctx, std::vector<PCLevel>& L, size_t i, double s, const double* shift, int nb) {
+    PCLevel& l = L[i];
+    if (i + 1 == L.size()) {
+        pc_coarsest_kernel<<<nb, 1024, sizeof(double) * 2 * (size_t)l.g.N, ctx->stream>>>(
+            l.g, l.ld, l.src, s, shift, l.v, 8 * std::max({l.g.nx, l.g.ny, l.g.nz}));
+        count_launch(ctx);
+        return;
+    }
+    pc_smooth(ctx, l, s, shift, nb, 2, true);
+    pc_residual_kernel<<<pc_grid(ctx, l.g.N, nb), 256, 0, ctx->stream>>>(l.g, l.ld, l.src, s, shift, l.v, l.res);
+    PCLevel& c = L[i + 1];
+    const Grid& f = l.g;
+    pc_restrict_axis_kernel<<<pc_grid(ctx, (long long)f.nz * f.ny * c.g.nx, nb), 256, 0, ctx->stream>>>(
+        l.res, l.ld, l.t1, (long long)f.nz * f.ny * c.g.nx, f.nx, f.ny, f.nz, 0, c.g.nx, f.dx, c.g.dx);
+    pc_restrict_axis_kernel<<<pc_grid(ctx, (long long)f.nz * c.g.ny * c.g.nx, nb), 256, 0, ctx->stream>>>(
+        l.t1, (long long)f.nz * f.ny * c.g.nx, l.t2, (long long)f.nz * c.g.ny * c.g.nx, c.g.nx, f.ny, f.nz, 1, c.g.ny,
+        f.dy, c.g.dy);
+    pc_restrict_axis_kernel<<<pc_grid(ctx, c.g.N, nb), 256, 0, ctx->stream>>>(
+        l.t2, (long long)f.nz * c.g.ny * c.g.nx, c.src, c.ld, c.g.nx, c.g.ny, f.nz, 2, c.g.nz, f.dz, c.g.dz);
+    count_launch(ctx, 4);
+    pc_vcycle(ctx, L, i + 1, 1.0, shift, nb);
+    pc_prolong_add_kernel<<<pc_grid(ctx, f.N, nb), 256, 0, ctx->stream>>>(f, l.ld, c.g, c.ld, c.v, l.v);
+    count_launch(ctx);
+    pc_smooth(ctx, l, s, shift, nb, 2, false);
+    DFT_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb,
+                            const double* sigma_host, double* T, long long ld) {
+    if (nb <= 0) return;
+    std::vector<PCLevel> L;
+    PCLevel f{};
+    f.g = g;
+    f.ld = ld;
+    L.push_back(f);
+    Grid cur = g;
+    while (cur.N > PC_COARSEST_MAX || std::min({cur.nx, cur.ny, cur.nz}) > 9) {
+        const Grid c = pc_coarse(cur);
+        if (c.nx == cur.nx && c.ny == cur.ny && c.nz == cur.nz) break;
+        PCLevel l{};
+        l.g = c;
+        l.ld = c.N;
+        L.push_back(l);
+        cur = c;
+        if (L.size() >= 10) break;
+    }
+    if (L.back().g.N > PC_COARSEST_MAX) fail(DFT_INVALID_ARGUMENT, "grid too small or anisotropic for multigrid");
+    // slab: per band, fine tmp/res and src copy; coarse levels src/v/tmp/res; restriction temps
+    size_t per_band = 3 * (size_t)ld + 16;
+    for (size_t i = 0; i < L.size(); ++i) {
+        if (i > 0) per_band += 4 * (size_t)L[i].g.N + 8;
+        if (i + 1 < L.size()) {
+            const Grid& a = L[i].g;
+            const Grid& c = L[i + 1].g;
+            per_band += (size_t)a.nz * a.ny * c.nx + (size_t)a.nz * c.ny * c.nx + 8;
+        }
+    }
+    double* slab = (double*)ws_get(ctx, WS_PG2, sizeof(double) * (per_band * nb + 64));
+    double* p = slab;
+    auto take = [&](size_t n) {
+        double* q = p;
+        p += (n * nb + 1) / 2 * 2;
+        return q;
+    };
+    L[0].src = take((size_t)ld);
+    L[0].tmp = take((size_t)ld);
+    L[0].res = take((size_t)ld);
+    L[0].v = T;
+    for (size_t i = 0; i < L.size(); ++i) {
+        if (i > 0) {
+            L[i].src = take((size_t)L[i].g.N);
+            L[i].v = take((size_t)L[i].g.N);
+            L[i].tmp = take((size_t)L[i].g.N);
+            L[i].res = take((size_t)L[i].g.N);
+        }
+        if (i + 1 < L.size()) {
+            const Grid& a = L[i].g;
+            const Grid& c = L[i + 1].g;
+            L[i].t1 = take((size_t)a.nz * a.ny * c.nx);
+            L[i].t2 = take((size_t)a.nz * c.ny * c.nx);
+        }
+    }
+    static bool attr = false;
+    if (!attr) {
+        DFT_CUDA(cudaFuncSetAttribute(pc_coarsest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(double) * 2 * PC_COARSEST_MAX)));
+        attr = true;
+    }
+    // shifts c_a = 2 sigma_a, on the device next to the slab
+    double* shift = (double*)ws_get(ctx, WS_PG3, sizeof(double) * (size_t)nb + 64);
+    std::vector<double> hs(sigma_host, sigma_host + nb);
+    for (double& x : hs) x *= 2.0;
+    DFT_CUDA(cudaMemcpyAsync(shift, hs.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, ctx->stream));
+    pc_gather_kernel<<<pc_grid(ctx, g.N, nb), 256, 0, ctx->stream>>>(g.N, ld, R, src_dev, L[0].src);
+    count_launch(ctx);
+    pc_vcycle(ctx, L, 0, 2.0, shift, nb);
+    if (L[0].v != T)
+        DFT_CUDA(cudaMemcpy2DAsync(T, sizeof(double) * ld, L[0].v, sizeof(double) * ld, sizeof(double) * g.N, nb,
+                                   cudaMemcpyDeviceToDevice, ctx->stream));
+    sync(ctx);  // hs must outlive its copy
+}
+
+}  // namespace dftb

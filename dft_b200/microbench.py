@@ -6,6 +6,8 @@
     python -m dft_b200.microbench scf    --n 48  [--iterations 1]     # H2 at h = 0.3 (n = 48)
     python -m dft_b200.microbench radial                              # 60 atoms, one launch
     python -m dft_b200.microbench gram   --n 64 --ka 64 --kb 64 --precision 1   # tcgen05 Gram
+    python -m dft_b200.microbench poisson --n 128 --poisson multigrid [--train 32]
+    python -m dft_b200.microbench scf --system h2o_128 --poisson multigrid --mixed 1 --stop-abs-de 1e-6
 
 Each mode prints one JSON line with the time and the achieved bandwidth for the
 operator's algorithmic bytes.  Used for roofline numbers and as the command under ncu.
@@ -37,6 +39,17 @@ def _events(torch, stream, fn, reps, flush=None):
     return times
 
 
+POISSON = {"cold": 0, "previous": 1, "network": 2, "coarse": 3, "hybrid": 4, "multigrid": 5}
+
+
+def train_net(eng, grid, samples):
+    """A network trained on the device on synthetic densities on `grid` (untimed setup)."""
+    net = d.PoissonNet(eng, seed=7)
+    rep = net.train([grid], samples=samples, validation=max(2, samples // 8), epochs=10, batch=4, lr=3e-3,
+                    lr_min=1e-4, seed=2027, smooth_sweeps=0, mse_weight=1.0)
+    return net, rep
+
+
 def cube(n, h):
     half = 0.5 * h * (n - 1)
     return d.CartesianGrid(n, n, n, -half, half, -half, half, -half, half)
@@ -44,11 +57,17 @@ def cube(n, h):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram"])
+    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram", "poisson"])
     ap.add_argument("--ka", type=int, default=64)
     ap.add_argument("--kb", type=int, default=64)
     ap.add_argument("--precision", type=int, default=0, help="gram: 0 = FP64, 1 = tensor cores (TF32 hi+lo)")
     ap.add_argument("--mixed", type=int, default=0, help="scf: mixed-precision eigensolver")
+    ap.add_argument("--poisson", default="cold", choices=sorted(POISSON),
+                    help="scf/poisson: start of each Poisson solve")
+    ap.add_argument("--precond", type=int, default=4,
+                    help="scf: eigensolver preconditioner (0 diagonal, k > 0 smoothing steps, -1 multigrid)")
+    ap.add_argument("--train", type=int, default=0,
+                    help="scf/poisson with a network start: train on this many synthetic densities first")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--h", type=float, default=0.2)
     ap.add_argument("--bands", type=int, default=16)
@@ -112,17 +131,48 @@ def main():
         m = d.Molecule()
         for z, p in zip(w["Z"], w["xyz"]):
             m.addNucleus(z, *p)
+        net, rep = (None, None)
+        if a.train:
+            net, rep = train_net(eng, g, a.train)
+            out["train"] = {k: rep[k] for k in ("steps", "seconds_data", "seconds_train", "val_loss",
+                                                "val_loss_coarse")}
         o = d.default_scf_options(max_iterations=a.iterations, extra_bands=w["extra_bands"], verbose=int(a.verbose),
-                                  stop_abs_de=a.stop_abs_de)
+                                  stop_abs_de=a.stop_abs_de, poisson_start=POISSON[a.poisson])
+        if net is not None:
+            o.poisson_net = net.handle
         o.eig.verbose = int(a.verbose > 1)
         o.eig.mixed_precision = a.mixed
+        o.eig.preconditioner = a.precond
         r = eng.scf_molecule(g, m, 0, w["multiplicity"], w["functional"], o)
-        out.update(system=a.system, iterations=r.iterations, converged=r.converged, energy=r.total,
+        out.update(system=a.system, poisson=a.poisson, mixed=a.mixed, precond=a.precond, iterations=r.iterations,
+                   converged=r.converged,
+                   energy=r.total,
                    seconds=r.seconds, launches=eng.launches, eigenvalues=r.eigenvalues[:8],
                    history=[{k: h[k] for k in ("iteration", "energy", "energy_difference", "density_difference",
                                                "ks_residual", "poisson_sweeps_in", "poisson_sweeps_out",
                                                "eig_iterations_alpha", "ms_hartree", "ms_xc", "ms_orbitals",
                                                "ms_density", "ms_energy", "ms_total")} for h in r.history])
+    elif a.mode == "poisson":
+        g = cube(a.n, a.h)
+        N = g.getSize()
+        rho, v = eng.array(N), eng.array(N)
+        eng.synthetic_density(g, 5, rho)
+        net = train_net(eng, g, a.train)[0] if a.train else None
+        res = {}
+
+        def run():
+            if a.poisson == "cold":
+                res["s"] = eng.hartree(g, rho, v)[0]
+                res["c"] = 0
+            else:
+                cyc = 40 if a.poisson == "multigrid" else 0
+                info = eng.poisson_start(g, net, rho, v, multigrid_cycles=cyc)
+                res["c"] = info["multigrid_cycles"] + info["coarse_cycles"]
+                res["s"] = eng.hartree_from_guess(g, rho, v)[0]
+
+        t = _events(torch, stream, run, a.reps)
+        out.update(n=a.n, poisson=a.poisson, network=bool(net), ms=statistics.median(t), sweeps=res["s"],
+                   cycles=res["c"])
     elif a.mode == "gram":
         g = cube(a.n, a.h)
         N = g.getSize()

@@ -145,7 +145,9 @@ typedef struct {
     int max_subspace;    /* basis size cap in multiples of nbands (>= 2) */
     int verbose;         /* 1: per-iteration lines on stderr */
     int preconditioner;  /* 0: the reference's diagonal (theta - diag)^-1 (EigenvalueSolverMolecule.cpp:521-555);
-                            k > 0: k damped-Jacobi smoothing steps on (T + sigma) t = r (default 4) */
+                            k > 0: k damped-Jacobi smoothing steps on (T + sigma) t = r (default 4);
+                            -1: one multigrid V(2,2) cycle on (T + sigma) t = r, all bands batched;
+                            -2: -1 on grids of 80^3 points or more, 4 below */
     int mixed_precision; /* 1: Gram products on the tensor cores (TF32 hi+lo split, FP32 accumulation)
                             until the occupied residuals fall below 1e-3, then FP64 to the end */
 } dft_eig_opts;
@@ -313,7 +315,7 @@ typedef struct {
     int batch;               /* samples per optimiser step */
     double lr, lr_min;       /* Adam step size, cosine-decayed from lr to lr_min */
     unsigned long long seed;
-    double target_tol;       /* Jacobi tolerance of the targets */
+    double target_tol;       /* Jacobi stop tolerance of the targets (reached via multigrid cycles) */
     long target_max_sweeps;
     int ngrids;              /* 1..4 grids, used in turn */
     dft_grid grids[4];
@@ -328,7 +330,7 @@ typedef struct {
 typedef struct {
     int steps;
     double seconds_data, seconds_train, ms_per_step;
-    double mean_target_sweeps;
+    double mean_target_sweeps;  /* Jacobi sweeps that finished each target after the cycles */
     double train_loss_first_epoch, train_loss_last_epoch;
     double val_loss;         /* network */
     double val_loss_coarse;  /* zero correction: the coarse start alone */

@@ -235,7 +235,7 @@ def test_nuclear_potential(engine, port):
     assert ei.value.status == dft_b200.DFT_SINGULAR
 
 
-@pytest.mark.parametrize("precond", [0, 4], ids=["diag", "kinetic4"])
+@pytest.mark.parametrize("precond", [0, 4, -1], ids=["diag", "kinetic4", "multigrid"])
 @pytest.mark.parametrize("case", ["h2o_11", "h2_16"])
 def test_block_davidson_vs_reference_algorithm(engine, port, case, precond):
     """Eigenpairs of the block solver vs the reference's state-by-state Davidson (oracle)."""
