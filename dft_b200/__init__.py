@@ -130,6 +130,8 @@ _SIGS = {
     "dft_nuclear_potential_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.POINTER(C.c_int), _D, _P], C.c_int),
     "dft_solve_orbitals_dev": ([_P, C.POINTER(dft_grid), _P, C.c_int, C.c_int, _P, C.c_long, C.c_int, _D,
                                 C.POINTER(dft_eig_opts), C.POINTER(C.c_int)], C.c_int),
+    "dft_rotate_dev": ([_P, C.POINTER(dft_grid), _P, C.c_long, C.c_int, _D, C.c_int, _P, C.c_long, C.c_int],
+                       C.c_int),
     "dft_gram_dev": ([_P, C.POINTER(dft_grid), _P, C.c_long, C.c_int, _P, C.c_long, C.c_int, C.c_int, _D], C.c_int),
     "dft_scf_default_options": ([C.POINTER(dft_scf_opts)], None),
     "dft_scf_molecule": ([_P, C.POINTER(dft_grid), C.c_int, C.POINTER(C.c_int), _D, C.c_int, C.c_int, C.c_int,
@@ -431,6 +433,13 @@ class Engine:
         out = np.zeros((ka, kb))
         _check(load().dft_gram_dev(self.ctx, C.byref(g), _ptr(A), lda, ka, _ptr(B), ldb, kb, int(precision), _dp(out)))
         return out
+
+    def rotate(self, grid, V, ldv, k, Y, X, ldx, precision=0):
+        """X = V * Y for band blocks (Y: k x m host matrix)."""
+        g = grid.c()
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        _check(load().dft_rotate_dev(self.ctx, C.byref(g), _ptr(V), ldv, k, _dp(Y), Y.shape[1], _ptr(X), ldx,
+                                     int(precision)))
 
     def solve_orbitals(self, grid, V, nocc, nbands, psi, ld, init=False, tol=1e-7, max_iterations=2000,
                        max_subspace=3, verbose=False, preconditioner=4, mixed_precision=0):

@@ -294,6 +294,20 @@ dft_status_t dft_solve_orbitals_dev(dft_context* ctx, const dft_grid* g, const d
     });
 }
 
+dft_status_t dft_rotate_dev(dft_context* ctx, const dft_grid* g, const double* V, long ldv, int k, const double* Y,
+                            int m, double* X, long ldx, int precision) {
+    return guard(ctx, [&] {
+        NEED(ctx && V && Y && X, "NULL argument");
+        NEED(k >= 0 && m >= 0, "k and m must be >= 0");
+        const dftb::Grid G = dftb::make_grid(g);
+        NEED(ldv >= G.N && ldx >= G.N, "leading dimensions must be >= N");
+        std::vector<double> Yv(Y, Y + (size_t)k * m);
+        if (precision) dftb::rotate_tc(ctx, G, V, ldv, k, Yv, m, X, ldx);
+        else dftb::rotate(ctx, G, V, ldv, k, Yv, m, X, ldx, 1.0, 0.0);
+        dftb::sync(ctx);
+    });
+}
+
 dft_status_t dft_gram_dev(dft_context* ctx, const dft_grid* g, const double* A, long lda, int ka, const double* B,
                           long ldb, int kb, int precision, double* C_host) {
     return guard(ctx, [&] {

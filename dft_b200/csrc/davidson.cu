@@ -277,6 +277,8 @@ void gram(dft_context* ctx, const Grid& g, const double* A, long long lda, int k
     std::memcpy(C.data(), h, sizeof(double) * nel);
 }
 
+}  // namespace
+
 // out = beta*out + alpha * in * Y   (Y: k x m host row-major)
 void rotate(dft_context* ctx, const Grid& g, const double* in, long long ldi, int k, const std::vector<double>& Y, int m,
             double* out, long long ldo, double alpha, double beta) {
@@ -303,6 +305,8 @@ void rotate(dft_context* ctx, const Grid& g, const double* in, long long ldi, in
     DFT_LAUNCH_CHECK();
     count_launch(ctx);
 }
+
+namespace {
 
 // Orthonormalise the nt columns of T against V[0:k] and among themselves (dV inner product).
 // Dependent directions are dropped; returns the number kept (compacted to the front of T).
@@ -430,6 +434,11 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
     };
     grow_G(0, k);
 
+    // out = in * Y: on the tensor cores in mixed-precision mode when the block is wide enough
+    auto rot = [&](const double* in, int kin, const std::vector<double>& Ym, int m, double* out) {
+        if (tc_mode && kin >= 32 && (long long)kin * m >= 2048) rotate_tc(ctx, g, in, ld, kin, Ym, m, out, ld);
+        else rotate(ctx, g, in, ld, kin, Ym, m, out, ld, 1.0, 0.0);
+    };
     double* dtheta = (double*)ws_get(ctx, WS_DAV6, sizeof(double) * 2 * nb + sizeof(int) * nb + 64);
     double* dsigma = dtheta + nb;
     int* dsrc = (int*)(dsigma + nb);
@@ -445,8 +454,8 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         for (int i = 0; i < k; ++i)
             for (int j = 0; j < nb; ++j) Y[(size_t)i * nb + j] = Z[(size_t)i * k + j];
         for (int j = 0; j < nb; ++j) theta[j] = w[j];
-        rotate(ctx, g, Vb, ld, k, Y, nb, X, ld, 1.0, 0.0);
-        rotate(ctx, g, AV, ld, k, Y, nb, AX, ld, 1.0, 0.0);
+        rot(Vb, k, Y, nb, X);
+        rot(AV, k, Y, nb, AX);
         // ---- residuals --------------------------------------------------------------------
         DFT_CUDA(cudaMemcpyAsync(dtheta, theta.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, ctx->stream));
         double* partial = (double*)ws_get(ctx, WS_REDUCE, sizeof(double) * ((size_t)eb * nb + nb));
@@ -502,9 +511,9 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
             std::vector<double> Zk((size_t)k * keep);
             for (int i = 0; i < k; ++i)
                 for (int j = 0; j < keep; ++j) Zk[(size_t)i * keep + j] = Z[(size_t)i * k + j];
-            rotate(ctx, g, Vb, ld, k, Zk, keep, W, ld, 1.0, 0.0);
+            rot(Vb, k, Zk, keep, W);
             DFT_CUDA(cudaMemcpyAsync(Vb, W, vecb * keep, cudaMemcpyDeviceToDevice, ctx->stream));
-            rotate(ctx, g, AV, ld, k, Zk, keep, W, ld, 1.0, 0.0);
+            rot(AV, k, Zk, keep, W);
             DFT_CUDA(cudaMemcpyAsync(AV, W, vecb * keep, cudaMemcpyDeviceToDevice, ctx->stream));
             k = keep;
             G.assign((size_t)k * k, 0.0);

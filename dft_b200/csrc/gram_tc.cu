@@ -131,18 +131,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
     const uint32_t idesc = idesc_tf32(NC);
+    // Thread (warp, lane) owns element (row 8 rg + lane / 4, point 4 kg + lane % 4) of core
+    // matrix cm = warp + 8 i (rg = cm / 8, kg = cm % 8): a warp writes one whole 128-byte core
+    // matrix per store, so the shared-memory stores are free of bank conflicts.
     double xa[RA], xb[RB];
+    const int lr = lane >> 2, lk = lane & 3;
     auto load = [&](long long ps) {
-        const bool pv = ps + lane < p1;
 #pragma unroll
         for (int i = 0; i < RA; ++i) {
-            const int r = warp + i * NW;
-            xa[i] = (r < mrows && pv) ? __ldg(A + (long long)(m0 + r) * lda + ps + lane) : 0.0;
+            const int cm = warp + i * NW, r = (cm >> 3) * 8 + lr;
+            const long long pt = ps + (cm & 7) * 4 + lk;
+            xa[i] = (r < mrows && pt < p1) ? __ldg(A + (long long)(m0 + r) * lda + pt) : 0.0;
         }
 #pragma unroll
         for (int i = 0; i < RB; ++i) {
-            const int r = warp + i * NW;
-            xb[i] = (r < nrows && pv) ? __ldg(B + (long long)(n0 + r) * ldb + ps + lane) : 0.0;
+            const int cm = warp + i * NW, r = (cm >> 3) * 8 + lr;
+            const long long pt = ps + (cm & 7) * 4 + lk;
+            xb[i] = (r < nrows && pt < p1) ? __ldg(B + (long long)(n0 + r) * ldb + pt) : 0.0;
         }
     };
     if (p0 < p1) load(p0);
@@ -165,19 +170,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         uint32_t* blo = bhi + b_words;
 #pragma unroll
         for (int i = 0; i < RA; ++i) {
-            const int r = warp + i * NW;
+            const int cm = warp + i * NW;
             const uint32_t h = to_tf32((float)xa[i]);
             const uint32_t l = to_tf32((float)(xa[i] - (double)__uint_as_float(h)));
-            const int o = kmajor_offset_words(r, lane, TC_M);
+            const int o = (((cm & 7) * (TC_M / 8) + (cm >> 3)) << 5) + lane;  // = kmajor_offset_words(row, k, TC_M)
             ahi[o] = h;
             alo[o] = l;
         }
 #pragma unroll
         for (int i = 0; i < RB; ++i) {
-            const int r = warp + i * NW;
+            const int cm = warp + i * NW;
             const uint32_t h = to_tf32((float)xb[i]);
             const uint32_t l = to_tf32((float)(xb[i] - (double)__uint_as_float(h)));
-            const int o = kmajor_offset_words(r, lane, NC);
+            const int o = (((cm & 7) * (NC / 8) + (cm >> 3)) << 5) + lane;
             bhi[o] = h;
             blo[o] = l;
         }
@@ -258,6 +263,148 @@ __global__ void gram_tc_reduce_kernel(int nchunks, int nel, const double* __rest
     }
 }
 
+// Rotation tile: X[n][p] = sum_k V[k][p] Y[k][n] for a 128-point tile (TMEM lanes = points)
+// and NC output bands (TMEM columns).  A = the V tile transposed (points x bands), B = Y^T
+// (bands-out x bands-in); both split into TF32 hi + lo in shared memory per 32-band slice.
+// grid = (ceil(N/128), ceil(m/nt)).
+template <int NC>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    rotate_tc_kernel(const double* __restrict__ V, long long ldv, int k, const double* __restrict__ Y, int m,
+                     int nt, double* __restrict__ X, long long ldx, long long n, int* __restrict__ error) {
+    extern __shared__ __align__(1024) uint32_t sm[];
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t bar[2];
+    constexpr int NW = TC_THREADS / 32;
+    constexpr int CA = TC_M * TC_KT / 32 / NW;  // core matrices of the V slice per warp (16)
+    constexpr int EB = NC * TC_KT / 32 / NW;    // core matrices of the Y slice per warp
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long p0 = (long long)blockIdx.x * TC_M;
+    const int j0 = blockIdx.y * nt, ncols = min(nt, m - j0);
+    constexpr int a_words = TC_M * TC_KT, b_words = NC * TC_KT;
+    constexpr int stage_words = 2 * a_words + 2 * b_words;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(NC));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = idesc_tf32(NC);
+    // as in the Gram kernel: thread (warp, lane) owns element (row 8 rg + lane / 4,
+    // k 4 kg + lane % 4) of core matrix cm = warp + 8 i; rows are points (V) or output bands (Y)
+    double xa[CA], xb[EB];
+    const int lr = lane >> 2, lk = lane & 3;
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int i = 0; i < CA; ++i) {
+            const int cm = warp + i * NW;
+            const long long p = p0 + (cm >> 3) * 8 + lr;
+            const int kk = k0 + (cm & 7) * 4 + lk;
+            xa[i] = (kk < k && p < n) ? __ldg(V + (long long)kk * ldv + p) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < EB; ++i) {
+            const int cm = warp + i * NW;
+            const int c = (cm >> 3) * 8 + lr, kk = k0 + (cm & 7) * 4 + lk;
+            xb[i] = (kk < k && c < ncols) ? __ldg(Y + (long long)kk * m + j0 + c) : 0.0;
+        }
+    };
+    load(0);
+    bool ok = true;
+    uint32_t phase[2] = {0, 0};
+    bool pending[2] = {false, false};
+    int step = 0;
+    for (int k0 = 0; k0 < k; k0 += TC_KT, ++step) {
+        const int st = step & 1;
+        if (pending[st]) {
+            if (!mbar_wait(&bar[st], phase[st])) ok = false;
+            phase[st] ^= 1;
+            pending[st] = false;
+        }
+        if (!__syncthreads_and(ok)) break;
+        uint32_t* ahi = sm + st * stage_words;
+        uint32_t* alo = ahi + a_words;
+        uint32_t* bhi = alo + a_words;
+        uint32_t* blo = bhi + b_words;
+#pragma unroll
+        for (int i = 0; i < CA; ++i) {
+            const int cm = warp + i * NW;
+            const uint32_t h = to_tf32((float)xa[i]);
+            const uint32_t l = to_tf32((float)(xa[i] - (double)__uint_as_float(h)));
+            const int o = (((cm & 7) * (TC_M / 8) + (cm >> 3)) << 5) + lane;
+            ahi[o] = h;
+            alo[o] = l;
+        }
+#pragma unroll
+        for (int i = 0; i < EB; ++i) {
+            const int cm = warp + i * NW;
+            const uint32_t h = to_tf32((float)xb[i]);
+            const uint32_t l = to_tf32((float)(xb[i] - (double)__uint_as_float(h)));
+            const int o = (((cm & 7) * (NC / 8) + (cm >> 3)) << 5) + lane;
+            bhi[o] = h;
+            blo[o] = l;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            constexpr uint32_t lbo_a = (TC_M / 8) * 128, lbo_b = (uint32_t)(NC / 8) * 128, sbo = 128;
+            const uint32_t sa_hi = smem_u32(ahi), sa_lo = smem_u32(alo), sb_hi = smem_u32(bhi), sb_lo = smem_u32(blo);
+#pragma unroll
+            for (int kk = 0; kk < TC_KT / 8; ++kk) {
+                const uint32_t oa = kk * 2 * lbo_a, ob = kk * 2 * lbo_b;
+                const uint64_t dah = smem_desc(sa_hi + oa, lbo_a, sbo), dal = smem_desc(sa_lo + oa, lbo_a, sbo);
+                const uint64_t dbh = smem_desc(sb_hi + ob, lbo_b, sbo), dbl = smem_desc(sb_lo + ob, lbo_b, sbo);
+                const uint32_t first = (step == 0 && kk == 0) ? 0u : 1u;
+                mma_tf32(tmem, dah, dbh, idesc, first);
+                mma_tf32(tmem, dah, dbl, idesc, 1u);
+                mma_tf32(tmem, dal, dbh, idesc, 1u);
+            }
+            mma_commit(&bar[st]);
+        }
+        pending[st] = true;
+        if (k0 + TC_KT < k) load(k0 + TC_KT);
+    }
+    for (int st = 0; st < 2; ++st)
+        if (pending[st]) {
+            if (!mbar_wait(&bar[st], phase[st])) ok = false;
+            phase[st] ^= 1;
+        }
+    ok = __syncthreads_and(ok);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (tid == 0) atomicExch(error, 1);
+    } else {
+        // TMEM lane = point p0 + row; warps w and w + 4 split the columns
+        const int q4 = warp & 3, half = warp >> 2;
+        const long long p = p0 + q4 * 32 + lane;
+        constexpr int CH = NC / (NW / 4);
+        for (int c0 = half * CH; c0 < half * CH + CH; c0 += 8) {
+            uint32_t v[8];
+            const uint32_t addr = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7])
+                         : "r"(addr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (p < n)
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (c0 + q < ncols) X[(long long)(j0 + c0 + q) * ldx + p] = (double)__uint_as_float(v[q]);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NC));
+}
+
 }  // namespace
 
 // C (ka x kb, host, row-major) = dV * A^T B on the tensor cores (TF32 hi+lo split).
@@ -321,6 +468,57 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
     sync(ctx);
     if (*(int*)(h + nel)) fail(DFT_CUDA_ERROR, "tensor-core Gram: mbarrier wait timed out");
     std::copy(h, h + nel, C.begin());
+}
+
+// X (m bands, leading dimension ldx) = V (k bands, ldv) * Y (k x m, host row-major) on the
+// tensor cores (TF32 hi+lo split, FP32 accumulation over k <= 4096 bands).
+void rotate_tc(dft_context* ctx, const Grid& g, const double* V, long long ldv, int k, const std::vector<double>& Y,
+               int m, double* X, long long ldx) {
+    if (m == 0) return;
+    if (k == 0) {
+        for (int j = 0; j < m; ++j)
+            DFT_CUDA(cudaMemsetAsync(X + (long long)j * ldx, 0, sizeof(double) * (size_t)g.N, ctx->stream));
+        return;
+    }
+    if (k > 4096) fail(DFT_INVALID_ARGUMENT, "rotation over more than 4096 bands");
+    const int ntiles = (m + TC_NMAX - 1) / TC_NMAX;
+    const int nt = (m + ntiles - 1) / ntiles;
+    int ncols = 32;
+    while (ncols < nt) ncols <<= 1;
+    const size_t smem = sizeof(uint32_t) * 2 * (size_t)(2 * TC_M * TC_KT + 2 * ncols * TC_KT);
+    double* dy = (double*)ws_get(ctx, WS_TMP, sizeof(double) * (size_t)k * m);
+    int* err = (int*)ws_get(ctx, WS_TMP2, 64);
+    DFT_CUDA(cudaMemcpyAsync(dy, Y.data(), sizeof(double) * (size_t)k * m, cudaMemcpyHostToDevice, ctx->stream));
+    DFT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+    static bool attr = false;
+    if (!attr) {
+        DFT_CUDA(cudaFuncSetAttribute(rotate_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        DFT_CUDA(cudaFuncSetAttribute(rotate_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        DFT_CUDA(cudaFuncSetAttribute(rotate_tc_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        DFT_CUDA(cudaFuncSetAttribute(rotate_tc_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
+    }
+    const dim3 grid((unsigned)((g.N + TC_M - 1) / TC_M), (unsigned)ntiles);
+    switch (ncols) {
+        case 32:
+            rotate_tc_kernel<32><<<grid, TC_THREADS, smem, ctx->stream>>>(V, ldv, k, dy, m, nt, X, ldx, g.N, err);
+            break;
+        case 64:
+            rotate_tc_kernel<64><<<grid, TC_THREADS, smem, ctx->stream>>>(V, ldv, k, dy, m, nt, X, ldx, g.N, err);
+            break;
+        case 128:
+            rotate_tc_kernel<128><<<grid, TC_THREADS, smem, ctx->stream>>>(V, ldv, k, dy, m, nt, X, ldx, g.N, err);
+            break;
+        default:
+            rotate_tc_kernel<256><<<grid, TC_THREADS, smem, ctx->stream>>>(V, ldv, k, dy, m, nt, X, ldx, g.N, err);
+            break;
+    }
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+    int* h = (int*)pinned(ctx, 1);
+    DFT_CUDA(cudaMemcpyAsync(h, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);  // also keeps Y alive until its copy has run
+    if (*h) fail(DFT_CUDA_ERROR, "tensor-core rotation: mbarrier wait timed out");
 }
 
 }  // namespace dftb

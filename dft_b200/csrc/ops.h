@@ -59,6 +59,13 @@ void nuclear_potential(dft_context* ctx, const Grid& g, int nnuc, const int* Z, 
 
 // C (ka x kb, host) = dV A^T B: FP64 (davidson.cu) or on the tensor cores with a TF32 hi+lo
 // split (gram_tc.cu).
+// out = beta*out + alpha * in * Y (Y: k x m host row-major), FP64 (davidson.cu)
+void rotate(dft_context* ctx, const Grid& g, const double* in, long long ldi, int k, const std::vector<double>& Y, int m,
+            double* out, long long ldo, double alpha, double beta);
+// X (m bands) = V (k bands) * Y (k x m, host row-major) on the tensor cores, TF32 hi+lo split
+// (gram_tc.cu).
+void rotate_tc(dft_context* ctx, const Grid& g, const double* V, long long ldv, int k, const std::vector<double>& Y,
+               int m, double* X, long long ldx);
 void gram_fp64(dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B,
                long long ldb, int kb, std::vector<double>& C);
 void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B, long long ldb,

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <limits>
 #include <vector>
 
@@ -90,12 +91,21 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     auto poisson = [&](const double* d, double* v, bool have_prev) {
         const double* start = nullptr;
         if (pstart == DFT_POISSON_MULTIGRID) {
+            const auto t0 = Clock::now();
+            int cyc = 0;
+            double res = 0.0;
             if (have_prev) {
                 DFT_CUDA(cudaMemcpyAsync(vstart.p, v, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
-                multigrid(ctx, g, d, vstart.p, 0.5 * o.poisson_tol, 40, nullptr);
+                cyc = multigrid(ctx, g, d, vstart.p, 0.5 * o.poisson_tol, 40, &res);
             } else {
-                poisson_start(ctx, net, g, d, vstart.p, 40, nullptr);
+                PoissonGuessInfo info;
+                poisson_start(ctx, net, g, d, vstart.p, 40, &info);
+                cyc = info.cycles;
+                res = info.residual;
             }
+            if (o.verbose > 1)
+                fprintf(stderr, "[poisson] multigrid %d cycles, next Jacobi update %.3e, %.2f ms\n", cyc, res,
+                        ms_since(t0));
             start = vstart.p;
         } else if ((pstart == DFT_POISSON_PREVIOUS || pstart == DFT_POISSON_HYBRID) && have_prev) {
             start = v;

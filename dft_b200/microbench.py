@@ -140,7 +140,7 @@ def main():
                                   stop_abs_de=a.stop_abs_de, poisson_start=POISSON[a.poisson])
         if net is not None:
             o.poisson_net = net.handle
-        o.eig.verbose = int(a.verbose > 1)
+        o.eig.verbose = int(a.verbose > 2)
         o.eig.mixed_precision = a.mixed
         o.eig.preconditioner = a.precond
         r = eng.scf_molecule(g, m, 0, w["multiplicity"], w["functional"], o)

@@ -152,6 +152,13 @@ typedef struct {
                             until the occupied residuals fall below 1e-3, then FP64 to the end */
 } dft_eig_opts;
 
+/* X (m x N, leading dimension ldx, device) = V (k x N, ldv, device) * Y (k x m, host,
+ * row-major).  precision 0 = FP64, 1 = tensor cores (TF32 hi+lo split).  The block
+ * eigensolver's subspace rotation, exposed for testing; no counterpart in the reference (its
+ * combinations are EigenvalueSolverMolecule.cpp:451-481). */
+dft_status_t dft_rotate_dev(dft_context* ctx, const dft_grid* g, const double* V, long ldv, int k, const double* Y,
+                            int m, double* X, long ldx, int precision);
+
 /* dV * A^T B for band blocks A (ka x N, leading dimension lda) and B (kb x N), result in
  * C_host (ka x kb, row-major).  precision 0 = FP64, 1 = tensor cores (TF32 hi+lo split).
  * The block eigensolver's Gram product, exposed for testing; no counterpart in the reference

@@ -43,3 +43,21 @@ def test_mixed_precision_eigensolver(engine, port):
         eig, it = engine.solve_orbitals(g, engine.upload(V), 5, 8, psi, N, mixed_precision=mixed)
         res[mixed] = eig
     assert np.max(np.abs(res[1][:5] - res[0][:5])) < 1e-9
+
+
+@pytest.mark.parametrize("k,m,n", [(40, 12, (40, 40, 40)), (207, 69, (33, 30, 28)), (64, 300, (20, 21, 22)),
+                                   (5, 3, (7, 9, 11))])
+def test_rotation_tensor_cores_vs_fp64(engine, k, m, n):
+    g = dft_b200.CartesianGrid(*n, -3.0, 3.0, -2.0, 2.5, -1.5, 1.7)
+    N = g.getSize()
+    rng = np.random.default_rng(k * 7 + m)
+    V = rng.standard_normal((k, N))
+    Y = rng.standard_normal((k, m))
+    dV = engine.upload(V)
+    X64, Xtc = engine.array(m * N), engine.array(m * N)
+    engine.rotate(g, dV, N, k, Y, X64, N, precision=0)
+    engine.rotate(g, dV, N, k, Y, Xtc, N, precision=1)
+    ref = Y.T @ V
+    a, b = X64.to_host((m, N)), Xtc.to_host((m, N))
+    assert np.max(np.abs(a - ref)) < 1e-11 * np.max(np.abs(ref))
+    assert np.max(np.abs(b - a)) < 2e-6 * np.max(np.abs(a))
