@@ -44,7 +44,8 @@ class dft_scf_opts(C.Structure):
     _fields_ = [("max_iterations", C.c_int), ("energy_tol", C.c_double), ("density_tol", C.c_double),
                 ("ks_tol", C.c_double), ("stop_abs_de", C.c_double), ("poisson_tol", C.c_double),
                 ("poisson_max_sweeps", C.c_long), ("extra_bands", C.c_int), ("eig", dft_eig_opts),
-                ("verbose", C.c_int), ("poisson_start", C.c_int), ("poisson_net", C.c_void_p)]
+                ("verbose", C.c_int), ("poisson_start", C.c_int), ("poisson_net", C.c_void_p), ("mixer", C.c_int),
+                ("pulay_depth", C.c_int), ("pulay_beta", C.c_double), ("eig_tol_adaptive", C.c_int)]
 
 
 # dft_poisson_start

@@ -107,6 +107,7 @@ dft_status_t dft_context_destroy(dft_context* ctx) {
         for (auto& w : ctx->ws)
             if (w.ptr) cudaFree(w.ptr);
         if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+        if (ctx->gram_ticket) cudaFree(ctx->gram_ticket);
         cudaStreamDestroy(ctx->stream);
     });
     delete ctx;
@@ -128,6 +129,9 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
             NEED(value == 0 || value == -2 || value == -1 || value == 1 || value == 2 || value == 4 || value == 8,
                  "jacobi_sweeps_per_launch must be 0 (auto), -2 (cluster), -1 (persistent), 1, 2, 4 or 8");
             ctx->jacobi_sweeps_per_launch = (int)value;
+        } else if (k == "network_tensor_cores") {
+            NEED(value == 0 || value == 1, "network_tensor_cores must be 0 or 1");
+            ctx->net_tensor_cores = (int)value;
         } else {
             dftb::fail(DFT_INVALID_ARGUMENT, "unknown tuning key '%s'", key);
         }

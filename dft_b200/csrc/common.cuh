@@ -98,10 +98,12 @@ struct dft_context {
     int num_sms = 148;
     // tuning knobs (dft_context_set_tuning)
     int jacobi_sweeps_per_launch = 0;  // 0 = auto, 1 = one sweep per launch, 2/4/8 = temporal blocking
+    int net_tensor_cores = 1;          // network convolutions on tcgen05 (1) or FP32 CUDA cores (0)
     // named scratch buffers (reductions, Jacobi ping-pong, XC intermediates, Davidson)
     dftb::Workspace ws[24];
     double* host_pinned = nullptr;  // small pinned staging area for scalars
     size_t host_pinned_bytes = 0;
+    void* gram_ticket = nullptr;    // block counter of the one-launch narrow Gram product
 };
 
 namespace dftb {

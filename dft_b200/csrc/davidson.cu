@@ -248,11 +248,102 @@ struct Blocks {
     long long ld;
 };
 
+// Narrow Gram products (ka <= 64, kb <= KB): one launch.  Warp w of every block owns rows
+// i = w, w + 8, ... of A (RPW of them) and all kb columns; its lanes stride the points and
+// keep RPW x KB sums in registers.  Block partials go to `partial`; the last block to finish
+// (ticket) adds them in block order (deterministic) and writes dV * C.
+template <int RPW, int KB>
+__global__ void __launch_bounds__(256) gram_small_kernel(const double* __restrict__ A, long long lda, int ka,
+                                                         const double* __restrict__ B, long long ldb, int kb,
+                                                         long long n, double scale, double* __restrict__ partial,
+                                                         unsigned int* __restrict__ ticket, double* __restrict__ out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double acc[RPW][KB];
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+        for (int j = 0; j < KB; ++j) acc[r][j] = 0.0;
+    for (long long p = (long long)blockIdx.x * 32 + lane; p < n; p += (long long)gridDim.x * 32) {
+        double b[KB];
+#pragma unroll
+        for (int j = 0; j < KB; ++j) b[j] = j < kb ? __ldg(B + (long long)j * ldb + p) : 0.0;
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const int i = warp + 8 * r;
+            const double a = i < ka ? __ldg(A + (long long)i * lda + p) : 0.0;
+#pragma unroll
+            for (int j = 0; j < KB; ++j) acc[r][j] = fma(a, b[j], acc[r][j]);
+        }
+    }
+    const int nel = ka * kb;
+    double* mine = partial + (long long)blockIdx.x * nel;
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+        for (int j = 0; j < KB; ++j) {
+            const double v = warp_sum(acc[r][j]);
+            const int i = warp + 8 * r;
+            if (lane == 0 && i < ka && j < kb) mine[i * kb + j] = v;
+        }
+    // last block: sum the partials in block order
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int e = warp; e < nel; e += 8) {
+        double v = 0.0;
+        for (int c = lane; c < (int)gridDim.x; c += 32) v += __ldcg(partial + (long long)c * nel + e);
+        v = warp_sum(v);
+        if (lane == 0) out[e] = v * scale;
+    }
+    if (threadIdx.x == 0) *ticket = 0;  // ready for the next call
+}
+
 // C (ka x kb, host, row-major) = dV * A^T B
 void gram(dft_context* ctx, const Grid& g, const double* A, long long lda, int ka, const double* B, long long ldb,
           int kb, std::vector<double>& C) {
     C.assign((size_t)ka * kb, 0.0);
     if (ka == 0 || kb == 0) return;
+    const int rpw = ka <= 8 ? 1 : ka <= 16 ? 2 : ka <= 32 ? 4 : 8;
+    const int kbt = kb <= 4 ? 4 : kb <= 8 ? 8 : 16;
+    if (ka <= 64 && kb <= 16 && rpw * kbt <= 64) {
+        // narrow product: one launch, the last block reduces
+        const size_t nel = (size_t)ka * kb;
+        const int nblk = (int)std::max<long long>(1, std::min<long long>(2LL * ctx->num_sms, (g.N + 1023) / 1024));
+        double* partial = (double*)ws_get(ctx, WS_SMALL, sizeof(double) * (nel * nblk + nel) + 64);
+        double* res = partial + nel * nblk;
+        if (!ctx->gram_ticket) {
+            DFT_CUDA(cudaMalloc(&ctx->gram_ticket, 64));
+            DFT_CUDA(cudaMemsetAsync(ctx->gram_ticket, 0, 64, ctx->stream));
+        }
+        unsigned int* tk = (unsigned int*)ctx->gram_ticket;
+#define DFT_GS(R, K)                                                                                          \
+    gram_small_kernel<R, K><<<nblk, 256, 0, ctx->stream>>>(A, lda, ka, B, ldb, kb, g.N, g.dV, partial, tk, res)
+        switch (rpw * 100 + kbt) {
+            case 104: DFT_GS(1, 4); break;
+            case 108: DFT_GS(1, 8); break;
+            case 116: DFT_GS(1, 16); break;
+            case 204: DFT_GS(2, 4); break;
+            case 208: DFT_GS(2, 8); break;
+            case 216: DFT_GS(2, 16); break;
+            case 404: DFT_GS(4, 4); break;
+            case 408: DFT_GS(4, 8); break;
+            case 416: DFT_GS(4, 16); break;
+            case 804: DFT_GS(8, 4); break;
+            default: DFT_GS(8, 8); break;
+        }
+#undef DFT_GS
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+        double* h = pinned(ctx, nel);
+        DFT_CUDA(cudaMemcpyAsync(h, res, sizeof(double) * nel, cudaMemcpyDeviceToHost, ctx->stream));
+        sync(ctx);
+        std::memcpy(C.data(), h, sizeof(double) * nel);
+        return;
+    }
     const int tx = (ka + GT - 1) / GT, ty = (kb + GT - 1) / GT;
     long long target = 4LL * ctx->num_sms;
     long long nch = std::max<long long>(1, target / (tx * ty));
@@ -408,6 +499,8 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
     // on the tensor cores (TF32 hi+lo); then the basis restarts from the Ritz block in FP64 and
     // every later product (and the convergence test) is FP64.
     bool tc_mode = o.mixed_precision != 0;
+    double tc_best = INFINITY;  // best occupied residual seen in tensor-core mode, and when
+    int tc_best_it = 0;
     std::vector<double> G;  // k x k, row-major, grows
     auto grow_G = [&](int k_old, int k_new) {
         std::vector<double> Gn((size_t)k_new * k_new, 0.0);
@@ -487,7 +580,14 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         if (tc_mode) {
             double mx = 0.0;
             for (int b = 0; b < nocc; ++b) mx = std::max(mx, rn[b]);
-            if (occ_conv || mx < o.mixed_switch) {
+            // also leave the tensor cores when the residuals stop falling: the TF32 hi+lo
+            // products have a noise floor that grows with |theta| and the band count
+            if (mx < 0.8 * tc_best) {
+                tc_best = mx;
+                tc_best_it = it;
+            }
+            const bool stalled = it - tc_best_it >= 15;
+            if (occ_conv || mx < o.mixed_switch || stalled) {
                 // switch to FP64: restart from the Ritz block, re-orthonormalised and re-projected
                 tc_mode = false;
                 DFT_CUDA(cudaMemcpyAsync(Vb, X, vecb * nb, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -530,9 +630,7 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
             count_launch(ctx);
         } else if (pc < 0) {
             // one multigrid cycle for (T + sigma_b) t = r_b, sigma_b = max(-theta_b, 1 Ha)
-            std::vector<double> sig(na);
-            for (int a = 0; a < na; ++a) sig[a] = std::max(-theta[active[a]], 1.0);
-            precondition_multigrid(ctx, g, R, dsrc, na, sig.data(), T, ld);
+            precondition_multigrid(ctx, g, R, dsrc, na, dtheta, T, ld);
         } else {
             // (T + sigma_b) t = r_b with sigma_b = max(-theta_b, 1 Ha): the far-field (V ~ 0) form of
             // (H - theta_b) for bound states; t0 = r/d, then damped-Jacobi steps (w = 2/3)

@@ -1382,4 +1382,49 @@ void nuclear_potential(dft_context* ctx, const Grid& g, int nnuc, const int* Z, 
     if (*h) fail(DFT_SINGULAR, "NuclearPotential is singular at a nuclear position.");
 }
 
+
+// =============================================================== Pulay mixing support
+namespace {
+struct LinComb {
+    const double* a[16];
+    const double* r[16];
+    double c[16];
+    int m;
+};
+// out = max(0, sum_i c_i (a_i + beta r_i))
+__global__ void lincomb_kernel(long long n, LinComb L, double beta, double* __restrict__ out) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int i = 0; i < L.m; ++i) s += L.c[i] * (L.a[i][p] + beta * L.r[i][p]);
+        out[p] = s > 0.0 ? s : 0.0;
+    }
+}
+__global__ void sub_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
+                           double* __restrict__ out) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        out[p] = a[p] - b[p];
+}
+}  // namespace
+
+void pulay_combine(dft_context* ctx, long long n, int m, const double* const* a, const double* const* r,
+                   const double* c, double beta, double* out) {
+    if (m < 1 || m > 16) fail(DFT_INVALID_ARGUMENT, "Pulay history of %d entries", m);
+    LinComb L{};
+    L.m = m;
+    for (int i = 0; i < m; ++i) {
+        L.a[i] = a[i];
+        L.r[i] = r[i];
+        L.c[i] = c[i];
+    }
+    lincomb_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, L, beta, out);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
+void sub(dft_context* ctx, long long n, const double* a, const double* b, double* out) {
+    sub_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, a, b, out);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
 }  // namespace dftb

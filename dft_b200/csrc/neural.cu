@@ -235,6 +235,183 @@ __global__ void __launch_bounds__(C3_THREADS) conv3_kernel(Vol v, const TIN* __r
     }
 }
 
+// ---------------------------------------------------------------- tensor-core 3x3x3 ----
+// Forward convolution as an implicit GEMM on the 5th-generation tensor cores: per block a
+// 128-point tile (16 x 8 x 1) of outputs, D[point][cout] = sum over 27 taps and CIN channels
+// of in[point + tap][ci] w[tap][ci][co], BF16 operands (tcgen05.mma kind::f16, A and B both
+// BF16), FP32 accumulator in TMEM.  The halo tile (18 x 10 x 3 points) is staged once; for
+// each group of taps the shifted input rows are copied into the canonical K-major,
+// no-swizzle layout (core matrix = 8 rows x 16 bytes) and one thread issues CIN/16 MMAs per
+// tap.  Weights for all taps are staged once per block in the same layout.  Every mbarrier
+// wait is bounded; a block that gives up flags the error, drains its MMAs and frees TMEM.
+constexpr int TCC_THREADS = 256;
+constexpr int TCC_X = 16, TCC_Y = 8, TCC_M = 128;
+constexpr int TCC_HX = TCC_X + 2, TCC_HY = TCC_Y + 2, TCC_HZ = 3;
+constexpr long long TCC_SPIN_LIMIT = 1LL << 22;
+
+__device__ __forceinline__ uint32_t tcc_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool tcc_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = tcc_smem(bar);
+    for (long long i = 0; i < TCC_SPIN_LIMIT; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ uint64_t tcc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100; no swizzle, base offset 0
+    return d;
+}
+
+// D = F32, A = B = BF16, both K-major, M = 128
+__host__ __device__ constexpr uint32_t tcc_idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TCC_M >> 4) << 24);
+}
+
+// byte offset of element (row, k) in an R-row canonical K-major bf16 tile
+__device__ __forceinline__ int tcc_off(int row, int k, int R) {
+    return (((k >> 3) * (R >> 3) + (row >> 3)) << 7) + ((row & 7) << 4) + ((k & 7) << 1);
+}
+
+template <int CIN, int COUT>
+constexpr int tcc_group() { return CIN == 16 ? 27 : 9; }  // taps staged per MMA batch
+
+template <int CIN, int COUT>
+constexpr size_t tcc_smem_bytes() {
+    return (size_t)27 * COUT * CIN * 2                              // weights
+           + (size_t)tcc_group<CIN, COUT>() * TCC_M * CIN * 2       // A rows for a group of taps
+           + al16((size_t)TCC_HX * TCC_HY * TCC_HZ * CIN * 2);      // halo
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(TCC_THREADS, 1)
+    conv3_tc_kernel(Vol v, const bf16* __restrict__ in, const bf16* __restrict__ w, const float* __restrict__ bias,
+                    bf16* __restrict__ zout, bf16* __restrict__ aout, int* __restrict__ error) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t bar;
+    constexpr int G = tcc_group<CIN, COUT>();
+    constexpr int W_BYTES = 27 * COUT * CIN * 2, A_TAP = TCC_M * CIN * 2;
+    constexpr int NCOL = COUT < 32 ? 32 : COUT;  // TMEM columns (power of two >= 32)
+    unsigned char* wsm = smem;
+    unsigned char* asm_ = smem + W_BYTES;
+    bf16* halo = reinterpret_cast<bf16*>(smem + W_BYTES + G * A_TAP);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tcc_smem(&s_tmem)),
+                     "r"(NCOL));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tcc_smem(&bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // weights: tap t, element (co, ci) of the N x K operand
+    for (int e = tid; e < 27 * CIN * COUT; e += TCC_THREADS) {
+        const int co = e % COUT, ci = (e / COUT) % CIN, t = e / (COUT * CIN);
+        *reinterpret_cast<bf16*>(wsm + t * COUT * CIN * 2 + tcc_off(co, ci, COUT)) = w[e];
+    }
+    const int x0 = blockIdx.x * TCC_X, y0 = blockIdx.y * TCC_Y, z0 = blockIdx.z;
+    load_box<CIN>(v, in, halo, x0 - 1, y0 - 1, z0 - 1, TCC_HX, TCC_HY, TCC_HZ, tid, TCC_THREADS);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    constexpr uint32_t lbo_a = (TCC_M / 8) * 128, lbo_b = (COUT / 8) * 128, sbo = 128;
+    constexpr uint32_t idesc = tcc_idesc(COUT);
+    bool ok = true;
+    uint32_t phase = 0;
+    for (int t0 = 0; t0 < 27; t0 += G) {
+        if (t0 > 0) {  // the previous group's MMAs read the A buffers: wait before rewriting them
+            if (!tcc_wait(&bar, phase)) ok = false;
+            phase ^= 1;
+        }
+        if (!__syncthreads_and(ok)) break;
+        // A rows: for tap t0 + g, row m = output point (m % 16, m / 16), 16-byte chunks of 8 channels
+        constexpr int CH = CIN / 8;
+        for (int e = tid; e < G * TCC_M * CH; e += TCC_THREADS) {
+            const int c = e % CH, m = (e / CH) % TCC_M, gi = e / (CH * TCC_M);
+            const int t = t0 + gi, tz = t / 9, ty = (t / 3) % 3, tx = t % 3;
+            const int hx = (m % TCC_X) + tx, hy = (m / TCC_X) + ty;
+            const uint4 val = *reinterpret_cast<const uint4*>(halo + ((tz * TCC_HY + hy) * TCC_HX + hx) * CIN + c * 8);
+            *reinterpret_cast<uint4*>(asm_ + gi * A_TAP + (((c * (TCC_M / 8) + (m >> 3)) << 7) + ((m & 7) << 4))) = val;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int gi = 0; gi < G; ++gi) {
+                const uint32_t a0 = tcc_smem(asm_ + gi * A_TAP), b0 = tcc_smem(wsm + (t0 + gi) * COUT * CIN * 2);
+#pragma unroll
+                for (int kk = 0; kk < CIN / 16; ++kk) {
+                    const uint64_t da = tcc_desc(a0 + kk * 2 * lbo_a, lbo_a, sbo);
+                    const uint64_t db = tcc_desc(b0 + kk * 2 * lbo_b, lbo_b, sbo);
+                    const uint32_t acc = (t0 == 0 && gi == 0 && kk == 0) ? 0u : 1u;
+                    const uint32_t zero = 0;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+                        ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(zero));
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             tcc_smem(&bar))
+                         : "memory");
+        }
+    }
+    // the last group (or a group cut short by an error) still has MMAs in flight
+    if (!tcc_wait(&bar, phase)) ok = false;
+    ok = __syncthreads_and(ok);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (tid == 0) atomicExch(error, 1);
+    } else {
+        // lane = output point; warps w and w + 4 split the output channels
+        const int q4 = warp & 3, half = warp >> 2;
+        const int m = q4 * 32 + lane;
+        const int gx = x0 + (m % TCC_X), gy = y0 + (m / TCC_X);
+        constexpr int HC = COUT / 2;
+        float z[HC];
+#pragma unroll
+        for (int c0 = 0; c0 < HC; c0 += 8) {
+            uint32_t r[8];
+            const uint32_t addr = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(half * HC + c0);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(addr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 8; ++q) z[c0 + q] = __uint_as_float(r[q]) + bias[half * HC + c0 + q];
+        }
+        if (gx < v.nx && gy < v.ny) {
+            const long long p = ((long long)z0 * v.ny + gy) * v.nx + gx;
+            float a[HC];
+#pragma unroll
+            for (int c = 0; c < HC; ++c) a[c] = silu(z[c]);
+            strow<HC>(zout + p * COUT + half * HC, z);
+            strow<HC>(aout + p * COUT + half * HC, a);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL));
+}
+
 // wT[tap][co][ci] = w[26 - tap][ci][co]: the data gradient of a 3x3x3 convolution is the
 // convolution of the output gradient with the flipped, transposed kernel.
 __global__ void conv3_flip_kernel(int cin, int cout, const bf16* __restrict__ w, bf16* __restrict__ wT) {
@@ -751,6 +928,7 @@ struct dft_pnet {
     dftb::DBuf<__nv_bfloat16> x, z[12], a[12], wT;
     dftb::DBuf<float> y, dz[12], t, e0, e1, e2, dy;
     dftb::DBuf<double> red;
+    dftb::DBuf<int> tc_err;  // set by a tensor-core convolution block whose wait timed out
 };
 
 namespace dftb {
@@ -774,6 +952,21 @@ void launch_conv3(dft_context* ctx, Vol v, const TIN* in, const bf16* w, const f
     }
     dim3 grid((v.nx + C3_X - 1) / C3_X, (v.ny + C3_Y - 1) / C3_Y, (v.nz + C3_P - 1) / C3_P);
     conv3_kernel<CIN, COUT, TIN, BWD><<<grid, C3_THREADS, sm, ctx->stream>>>(v, in, w, bias, z, a, g, extra, zprev);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
+template <int CIN, int COUT>
+void launch_conv3_tc(dft_context* ctx, Vol v, const bf16* in, const bf16* w, const float* bias, bf16* z, bf16* a,
+                     int* err) {
+    constexpr size_t sm = tcc_smem_bytes<CIN, COUT>();
+    static bool once = false;
+    if (!once) {
+        set_smem(conv3_tc_kernel<CIN, COUT>, sm);
+        once = true;
+    }
+    dim3 grid((v.nx + TCC_X - 1) / TCC_X, (v.ny + TCC_Y - 1) / TCC_Y, v.nz);
+    conv3_tc_kernel<CIN, COUT><<<grid, TCC_THREADS, sm, ctx->stream>>>(v, in, w, bias, z, a, err);
     DFT_LAUNCH_CHECK();
     count_launch(ctx);
 }
@@ -852,25 +1045,34 @@ void forward(dft_context* ctx, PNet* n, Vol v0, const bf16* x) {
     auto W = [&](int i) { return P + n->L[i].w; };
     auto B = [&](int i) { return F + n->L[i].b; };
     const int ew = 256;
+    const bool tc = ctx->net_tensor_cores != 0;
+    int* err = n->tc_err.get(1);
+    auto c16 = [&](const bf16* in, int i) {
+        if (tc) launch_conv3_tc<16, 16>(ctx, v0, in, W(i), B(i), n->z[i].p, n->a[i].p, err);
+        else launch_conv3<16, 16, bf16, false>(ctx, v0, in, W(i), B(i), n->z[i].p, n->a[i].p, nullptr, nullptr, nullptr);
+    };
+    auto c32 = [&](Vol vv, const bf16* in, int i) {
+        if (tc) launch_conv3_tc<32, 32>(ctx, vv, in, W(i), B(i), n->z[i].p, n->a[i].p, err);
+        else launch_conv3<32, 32, bf16, false>(ctx, vv, in, W(i), B(i), n->z[i].p, n->a[i].p, nullptr, nullptr, nullptr);
+    };
     if (n->in_ch == 2)
         launch_conv3<2, 16, bf16, false>(ctx, v0, x, W(0), B(0), n->z[0].p, n->a[0].p, nullptr, nullptr, nullptr);
     else
         fail(DFT_INVALID_ARGUMENT, "the network takes 2 input channels");
-    launch_conv3<16, 16, bf16, false>(ctx, v0, n->a[0].p, W(1), B(1), n->z[1].p, n->a[1].p, nullptr, nullptr, nullptr);
+    c16(n->a[0].p, 1);
     down_fwd_kernel<16, 32><<<blocks_for(ctx, v1.n()), ew, 0, ctx->stream>>>(v0, v1, n->a[1].p, W(2), B(2), n->z[2].p,
                                                                              n->a[2].p);
-    launch_conv3<32, 32, bf16, false>(ctx, v1, n->a[2].p, W(3), B(3), n->z[3].p, n->a[3].p, nullptr, nullptr, nullptr);
+    c32(v1, n->a[2].p, 3);
     down_fwd_kernel<32, 32><<<blocks_for(ctx, v2.n()), ew, 0, ctx->stream>>>(v1, v2, n->a[3].p, W(4), B(4), n->z[4].p,
                                                                              n->a[4].p);
-    launch_conv3<32, 32, bf16, false>(ctx, v2, n->a[4].p, W(5), B(5), n->z[5].p, n->a[5].p, nullptr, nullptr, nullptr);
-    launch_conv3<32, 32, bf16, false>(ctx, v2, n->a[5].p, W(6), B(6), n->z[6].p, n->a[6].p, nullptr, nullptr, nullptr);
+    c32(v2, n->a[4].p, 5);
+    c32(v2, n->a[5].p, 6);
     up_fwd_kernel<32, 32><<<blocks_for(ctx, v1.n()), ew, 0, ctx->stream>>>(v1, v2, n->a[6].p, W(7), B(7), n->a[3].p,
                                                                            n->z[7].p, n->a[7].p);
-    launch_conv3<32, 32, bf16, false>(ctx, v1, n->a[7].p, W(8), B(8), n->z[8].p, n->a[8].p, nullptr, nullptr, nullptr);
+    c32(v1, n->a[7].p, 8);
     up_fwd_kernel<32, 16><<<blocks_for(ctx, v0.n()), ew, 0, ctx->stream>>>(v0, v1, n->a[8].p, W(9), B(9), n->a[1].p,
                                                                            n->z[9].p, n->a[9].p);
-    launch_conv3<16, 16, bf16, false>(ctx, v0, n->a[9].p, W(10), B(10), n->z[10].p, n->a[10].p, nullptr, nullptr,
-                                      nullptr);
+    c16(n->a[9].p, 10);
     head_fwd_kernel<16><<<blocks_for(ctx, v0.n()), ew, 0, ctx->stream>>>(v0.n(), n->a[10].p, W(11), B(11), n->y.p);
     DFT_LAUNCH_CHECK();
     count_launch(ctx, 5);
@@ -1013,6 +1215,14 @@ void backward(dft_context* ctx, PNet* n, Vol v0, const bf16* x, const float* t, 
     launch_wgrad<2, 16>(ctx, v0, x, n->dz[0].p, GW(0), GB(0));
 }
 
+// Reads the tensor-core convolutions' error flag (synchronises the stream).
+void check_tc(dft_context* ctx, PNet* n) {
+    int* h = (int*)pinned(ctx, 1);
+    DFT_CUDA(cudaMemcpyAsync(h, n->tc_err.get(1), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    if (*h) fail(DFT_CUDA_ERROR, "tensor-core convolution: mbarrier wait timed out");
+}
+
 void adam_step(dft_context* ctx, PNet* n, float lr, float gscale) {
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     n->step += 1;
@@ -1059,6 +1269,7 @@ dft_pnet* pnet_create(dft_context* ctx, int in_channels, unsigned long long seed
         n->m.get(n->np);
         n->v.get(n->np);
         n->pb.get(n->np);
+        DFT_CUDA(cudaMemsetAsync(n->tc_err.get(1), 0, sizeof(int), ctx->stream));
         DFT_CUDA(cudaMemsetAsync(n->m.p, 0, n->np * 4, ctx->stream));
         DFT_CUDA(cudaMemsetAsync(n->v.p, 0, n->np * 4, ctx->stream));
         pnet_set_params(ctx, n, h.data());
@@ -1107,6 +1318,7 @@ void pnet_loss_grad(dft_context* ctx, dft_pnet* n, int nx, int ny, int nz, const
     DFT_CUDA(cudaMemcpyAsync(h, n->red.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
     sync(ctx);
     if (loss) *loss = h[0];
+    check_tc(ctx, n);
 }
 
 void pnet_correct(dft_context* ctx, dft_pnet* net, const Grid& g, const double* rho, double* v,
@@ -1118,6 +1330,7 @@ void pnet_correct(dft_context* ctx, dft_pnet* net, const Grid& g, const double* 
     combine_kernel<<<blocks_for(ctx, g.N), 256, 0, ctx->stream>>>(g, v, net->y.p, scale_dev, v);
     DFT_LAUNCH_CHECK();
     count_launch(ctx);
+    check_tc(ctx, net);
 }
 
 void pnet_train_poisson(dft_context* ctx, dft_pnet* n, const dft_pnet_train_opts* o, dft_pnet_train_report* rep) {
@@ -1203,6 +1416,7 @@ void pnet_train_poisson(dft_context* ctx, dft_pnet* n, const dft_pnet_train_opts
         DFT_CUDA(cudaMemcpyAsync(h, n->red.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
         sync(ctx);
         const double el = h[0] / ntrain;
+        check_tc(ctx, n);
         if (ep == 0) rep->train_loss_first_epoch = el;
         rep->train_loss_last_epoch = el;
         if (rep->epoch_loss && ep < rep->epoch_loss_capacity) rep->epoch_loss[ep] = el;

@@ -34,6 +34,12 @@ void add3(dft_context* ctx, long long n, const double* a, const double* b, const
 // d = (1-m) d + m o   (mixDensity, MolecularSCFHelpers.cpp:27-44)
 void mix(dft_context* ctx, long long n, double* d, const double* o, double m);
 
+// out = max(0, sum_i c_i (a_i + beta r_i)) over m <= 16 history entries (Pulay mixing)
+void pulay_combine(dft_context* ctx, long long n, int m, const double* const* a, const double* const* r,
+                   const double* c, double beta, double* out);
+// out = a - b
+void sub(dft_context* ctx, long long n, const double* a, const double* b, double* out);
+
 // sum_p a[p]*b[p] (optionally * w[p]); deterministic block order
 double dot(dft_context* ctx, long long n, const double* a, const double* b);
 // sum_p a[p]*b[p]*c[p] evaluated as (a*b)*c per term
@@ -73,10 +79,10 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
 
 // Block Davidson eigensolver (davidson.cu).
 // One multigrid V(2,2) cycle from zero for (T + sigma_a) t_a = r_{src[a]} per band a (T the
-// kinetic operator with psi = 0 outside the box), into T[a*ld ..] (precond_mg.cu).
-// src_dev: device band indices into R; sigma_host: nb shifts (host).
+// kinetic operator with psi = 0 outside the box), into T[a*ld ..] (precond_mg.cu), with
+// sigma_a = max(-theta[src[a]], 1 Ha).  src_dev: device band indices into R and theta_dev.
 void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb,
-                            const double* sigma_host, double* T, long long ld);
+                            const double* theta_dev, double* T, long long ld);
 
 struct EigOpts {
     double tol = 1e-7;

@@ -149,6 +149,13 @@ __global__ void __launch_bounds__(1024) pc_coarsest_kernel(Grid g, long long ld,
     for (int p = threadIdx.x; p < n; p += blockDim.x) e[p] = res[p];
 }
 
+// c_a = 2 max(-theta[src[a]], 1 Ha): the shift of each correction band, from the Ritz values
+__global__ void pc_shift_kernel(int nb, const double* __restrict__ theta, const int* __restrict__ src,
+                                double* __restrict__ shift) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nb; a += gridDim.x * blockDim.x)
+        shift[a] = 2.0 * fmax(-theta[src[a]], 1.0);
+}
+
 __global__ void pc_gather_kernel(long long n, long long ld, const double* __restrict__ R, const int* __restrict__ srcmap,
                                  double* __restrict__ out) {
     const int a = blockIdx.y;
@@ -216,7 +223,7 @@ void pc_vcycle(dft_context* ctx, std::vector<PCLevel>& L, size_t i, double s, co
 }  // namespace
 
 void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb,
-                            const double* sigma_host, double* T, long long ld) {
+                            const double* theta_dev, double* T, long long ld) {
     if (nb <= 0) return;
     std::vector<PCLevel> L;
     PCLevel f{};
@@ -276,18 +283,16 @@ void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, co
                                       (int)(sizeof(double) * 2 * PC_COARSEST_MAX)));
         attr = true;
     }
-    // shifts c_a = 2 sigma_a, on the device next to the slab
+    // shifts c_a = 2 sigma_a, computed on the device (no host round trip)
     double* shift = (double*)ws_get(ctx, WS_PG3, sizeof(double) * (size_t)nb + 64);
-    std::vector<double> hs(sigma_host, sigma_host + nb);
-    for (double& x : hs) x *= 2.0;
-    DFT_CUDA(cudaMemcpyAsync(shift, hs.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, ctx->stream));
+    pc_shift_kernel<<<(nb + 127) / 128, 128, 0, ctx->stream>>>(nb, theta_dev, src_dev, shift);
     pc_gather_kernel<<<pc_grid(ctx, g.N, nb), 256, 0, ctx->stream>>>(g.N, ld, R, src_dev, L[0].src);
     count_launch(ctx);
     pc_vcycle(ctx, L, 0, 2.0, shift, nb);
     if (L[0].v != T)
         DFT_CUDA(cudaMemcpy2DAsync(T, sizeof(double) * ld, L[0].v, sizeof(double) * ld, sizeof(double) * g.N, nb,
                                    cudaMemcpyDeviceToDevice, ctx->stream));
-    sync(ctx);  // hs must outlive its copy
+    DFT_LAUNCH_CHECK();
 }
 
 }  // namespace dftb

@@ -144,6 +144,87 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), db.p);
     }
 
+    // ---- Pulay mixer state (option; the reference mixes linearly) -----------------------
+    const int ns = closed ? 1 : 2;
+    const int pdepth = o.pulay_depth > 0 ? std::min(o.pulay_depth, 16) : 8;
+    const double pbeta = o.pulay_beta > 0.0 ? o.pulay_beta : 0.2;
+    if (o.mixer != 0 && o.mixer != 1) fail(DFT_INVALID_ARGUMENT, "unknown mixer %d", o.mixer);
+    DevBuf phist(o.mixer == 1 ? (size_t)2 * pdepth * ns * N : 0);
+    std::vector<double> Bp((size_t)pdepth * pdepth, 0.0);
+    int pcount = 0, phead = 0;
+    auto pulay_mix = [&]() {
+        const int slot = phead;
+        double* hin = phist.p + (size_t)slot * 2 * ns * N;
+        double* hres = hin + (size_t)ns * N;
+        DFT_CUDA(cudaMemcpyAsync(hin, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+        sub(ctx, N, oa.p, da.p, hres);
+        if (!closed) {
+            DFT_CUDA(cudaMemcpyAsync(hin + N, db.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+            sub(ctx, N, ob.p, db.p, hres + N);
+        }
+        phead = (phead + 1) % pdepth;
+        pcount = std::min(pcount + 1, pdepth);
+        for (int j = 0; j < pcount; ++j) {
+            const double* rj = phist.p + (size_t)j * 2 * ns * N + (size_t)ns * N;
+            const double v = dot(ctx, (long long)ns * N, hres, rj);
+            Bp[(size_t)slot * pdepth + j] = Bp[(size_t)j * pdepth + slot] = v;
+        }
+        // minimise |sum c_i r_i| with sum c_i = 1: [B 1; 1 0][c; l] = [0; 1], Gaussian
+        // elimination with partial pivoting; a singular system falls back to the newest entry
+        const int m = pcount, M = m + 1;
+        std::vector<double> A((size_t)M * M, 0.0), rhs(M, 0.0);
+        double tr = 0.0;
+        for (int i = 0; i < m; ++i) tr += Bp[(size_t)i * pdepth + i];
+        for (int i = 0; i < m; ++i) {
+            for (int j = 0; j < m; ++j) A[(size_t)i * M + j] = Bp[(size_t)i * pdepth + j];
+            A[(size_t)i * M + i] += 1e-12 * tr;
+            A[(size_t)i * M + m] = A[(size_t)m * M + i] = 1.0;
+        }
+        rhs[m] = 1.0;
+        bool ok = true;
+        for (int c = 0; c < M && ok; ++c) {
+            int piv = c;
+            for (int r = c + 1; r < M; ++r)
+                if (std::fabs(A[(size_t)r * M + c]) > std::fabs(A[(size_t)piv * M + c])) piv = r;
+            if (!(std::fabs(A[(size_t)piv * M + c]) > 1e-300)) {
+                ok = false;
+                break;
+            }
+            if (piv != c) {
+                for (int k = 0; k < M; ++k) std::swap(A[(size_t)c * M + k], A[(size_t)piv * M + k]);
+                std::swap(rhs[c], rhs[piv]);
+            }
+            for (int r = c + 1; r < M; ++r) {
+                const double f = A[(size_t)r * M + c] / A[(size_t)c * M + c];
+                for (int k = c; k < M; ++k) A[(size_t)r * M + k] -= f * A[(size_t)c * M + k];
+                rhs[r] -= f * rhs[c];
+            }
+        }
+        std::vector<double> cf(M, 0.0);
+        if (ok) {
+            for (int r = M - 1; r >= 0; --r) {
+                double v = rhs[r];
+                for (int k = r + 1; k < M; ++k) v -= A[(size_t)r * M + k] * cf[k];
+                cf[r] = v / A[(size_t)r * M + r];
+            }
+            for (int i = 0; i < m; ++i) ok = ok && std::isfinite(cf[i]);
+        }
+        if (!ok) {
+            std::fill(cf.begin(), cf.end(), 0.0);
+            cf[slot] = 1.0;
+        }
+        for (int sp = 0; sp < ns; ++sp) {
+            const double* a[16];
+            const double* r[16];
+            for (int i = 0; i < m; ++i) {
+                a[i] = phist.p + (size_t)i * 2 * ns * N + (size_t)sp * N;
+                r[i] = a[i] + (size_t)ns * N;
+            }
+            pulay_combine(ctx, N, m, a, r, cf.data(), pbeta, sp == 0 ? da.p : db.p);
+        }
+        if (closed) DFT_CUDA(cudaMemcpyAsync(db.p, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+    };
+
     // ---- SCF loop, constants SelfConsistentFieldMolecule.cpp:27-31 ----------------------
     double prevE = std::numeric_limits<double>::infinity();
     double prevD = std::numeric_limits<double>::infinity();
@@ -175,9 +256,11 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         rec.ms_xc = ms_since(t0);
         // orbitals (:117-144), warm-started from the previous iteration
         t0 = Clock::now();
-        rec.eig_iterations_alpha = solve_orbitals(ctx, g, va.p, na, bands_a, psia.p, ld, true, eiga.data(), resa.data(), eo);
+        EigOpts ek = eo;
+        if (o.eig_tol_adaptive && std::isfinite(prevD)) ek.tol = std::max(eo.tol, std::min(1e-3, 0.1 * prevD));
+        rec.eig_iterations_alpha = solve_orbitals(ctx, g, va.p, na, bands_a, psia.p, ld, true, eiga.data(), resa.data(), ek);
         if (!closed)
-            rec.eig_iterations_beta = solve_orbitals(ctx, g, vb.p, nb, bands_b, psib.p, ld, true, eigb.data(), resb.data(), eo);
+            rec.eig_iterations_beta = solve_orbitals(ctx, g, vb.p, nb, bands_b, psib.p, ld, true, eigb.data(), resb.data(), ek);
         rec.ms_orbitals = ms_since(t0);
         // output densities (:160-187)
         t0 = Clock::now();
@@ -220,7 +303,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         rec.energy_difference = dE;
         rec.density_difference = effd;
         rec.ks_residual = resid;
-        rec.mixing = imix;
+        rec.mixing = o.mixer == 1 ? pbeta : imix;
         rec.ms_total = ms_since(t_it);
         if (res->history && res->history_len < res->history_capacity) res->history[res->history_len++] = rec;
         if (o.verbose)
@@ -235,8 +318,12 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             if (effd > prevD * 1.05) mixing = std::max(0.10, mixing * 0.75);
             else if (effd < prevD) mixing = std::min(0.50, mixing * 1.10);
         }
-        mix(ctx, N, da.p, oa.p, imix);
-        mix(ctx, N, db.p, ob.p, imix);
+        if (o.mixer == 1) {
+            pulay_mix();
+        } else {
+            mix(ctx, N, da.p, oa.p, imix);
+            mix(ctx, N, db.p, ob.p, imix);
+        }
         prevD = effd;
         prevE = E[5];
     }

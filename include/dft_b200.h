@@ -206,6 +206,12 @@ typedef struct {
      * from zero): DFT_POISSON_COLD reproduces the reference. */
     int poisson_start;       /* dft_poisson_start */
     dft_pnet* poisson_net;   /* network for DFT_POISSON_NETWORK (not owned) */
+    /* Density mixing and eigensolver tolerance (no counterpart in the reference; the defaults
+     * 0 keep its linear mixer, SelfConsistentFieldMolecule.cpp:447-484, and its fixed tolerance). */
+    int mixer;               /* 0: linear with the adaptive factor; 1: Pulay (DIIS) on n_out - n_in */
+    int pulay_depth;         /* history length for the Pulay mixer (0 = 8) */
+    double pulay_beta;       /* step along the extrapolated residual (0 = 0.2) */
+    int eig_tol_adaptive;    /* 1: eigensolver tolerance max(eig.tol, min(1e-3, 0.1 * previous dRho)) */
 } dft_scf_opts;
 
 /* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)

@@ -41,8 +41,10 @@ def test_param_count_matches_oracle(engine):
     assert np.array_equal(net.get_params(), p * 2)
 
 
+@pytest.mark.parametrize("tensor_cores", [1, 0], ids=["tcgen05", "cuda_cores"])
 @pytest.mark.parametrize("shape", [(10, 9, 7), (37, 34, 21)])
-def test_forward_and_gradient_vs_oracle(engine, shape):
+def test_forward_and_gradient_vs_oracle(engine, shape, tensor_cores):
+    engine.set_tuning("network_tensor_cores", tensor_cores)
     net = dft_b200.PoissonNet(engine)
     p = _random_params(11)
     net.set_params(p)
@@ -59,6 +61,7 @@ def test_forward_and_gradient_vs_oracle(engine, shape):
         n = R.TAPS[typ] * cin * cout
         assert _rel(grad[wo:wo + n], g_ref[wo:wo + n]) < 3e-2, (typ, cin, cout)
         assert _rel(grad[bo:bo + cout], g_ref[bo:bo + cout]) < 3e-2, (typ, cin, cout, "bias")
+    engine.set_tuning("network_tensor_cores", 1)
 
 
 def _h2_grid(n=48, half=7.05):
@@ -155,3 +158,30 @@ def test_scf_with_each_poisson_start(engine):
         assert abs(e - energies[dft_b200.POISSON_COLD]) < 2e-5, (mode, energies)
     assert sweeps[dft_b200.POISSON_HYBRID] < 0.6 * sweeps[dft_b200.POISSON_COLD], sweeps
     assert sweeps[dft_b200.POISSON_MULTIGRID] < 0.01 * sweeps[dft_b200.POISSON_COLD], sweeps
+
+
+@pytest.mark.parametrize("case", ["h2_closed", "h3_doublet"])
+def test_pulay_mixer_same_energy(engine, case):
+    """The Pulay mixer and the adaptive eigensolver tolerance reach the linear mixer's energy."""
+    g = dft_b200.CartesianGrid(28, 28, 28, -5.4, 5.4, -5.4, 5.4, -5.4, 5.4)
+    m = dft_b200.Molecule()
+    if case == "h2_closed":
+        m.addNucleus(1, -0.7, 0.0, 0.0)
+        m.addNucleus(1, 0.7, 0.0, 0.0)
+        mult = 1
+    else:
+        m.addNucleus(1, -1.6, 0.0, 0.0)
+        m.addNucleus(1, 0.0, 0.1, 0.0)
+        m.addNucleus(1, 1.6, 0.0, 0.0)
+        mult = 2
+    res = {}
+    for mixer, adaptive in ((0, 0), (1, 0), (1, 1)):
+        o = dft_b200.default_scf_options(stop_abs_de=1e-8, poisson_start=dft_b200.POISSON_MULTIGRID, mixer=mixer,
+                                         eig_tol_adaptive=adaptive)
+        r = engine.scf_molecule(g, m, 0, mult, "PBE96", o)
+        res[(mixer, adaptive)] = (r.total, r.iterations)
+    print(case, res)
+    e0 = res[(0, 0)][0]
+    for k, (e, it) in res.items():
+        assert abs(e - e0) < 1e-6, (k, res)
+    assert res[(1, 0)][1] <= res[(0, 0)][1]
