@@ -117,14 +117,15 @@ def scf_options(w, fast=False, net=None):
     """plain: the reference's method in FP64 (cold-start Jacobi, FP64 eigensolver).
     fast: multigrid cycles from the previous potential (the learned start for each density
     slot's first solve) before the same Jacobi stop rule, the mixed-precision eigensolver
-    (tcgen05 TF32 hi+lo Gram products, FP64 finish) and its multigrid preconditioner on large
-    grids."""
+    (tcgen05 TF32 hi+lo Gram products and rotations, FP64 finish) with its multigrid
+    preconditioner on large grids, Pulay density mixing and an eigensolver tolerance that
+    follows the density change."""
     import dft_b200
     if not fast:
         return dft_b200.default_scf_options(stop_abs_de=1e-6, extra_bands=w["extra_bands"])
     o = dft_b200.default_scf_options(stop_abs_de=1e-6, extra_bands=w["extra_bands"],
                                      poisson_start=dft_b200.POISSON_MULTIGRID, eig_mixed_precision=1,
-                                     eig_preconditioner=-2)
+                                     eig_preconditioner=-2, mixer=1, adaptive_eig_tol=1)
     if net is not None:
         o.poisson_net = net.handle
     return o
@@ -370,7 +371,7 @@ def main():
     # max|dV| < 1e-8 stops ~1e-8/(1 - rho) away from the Jacobi fixed point): the FP64 oracle
     # run for the energy error of the fast configuration
     import dft_b200 as _d
-    tight = _d.default_scf_options(stop_abs_de=1e-6, extra_bands=w["extra_bands"],
+    tight = _d.default_scf_options(stop_abs_de=1e-9, extra_bands=w["extra_bands"],
                                    poisson_tol=jacobi_tight_tol(w), poisson_max_sweeps=400000)
     tight_total, _, tight_res, _ = run(tight, 0, 1)
     opts = fast
@@ -410,7 +411,8 @@ def main():
                    "eig_iterations": [h["eig_iterations_alpha"] for h in last.history],
                    "method": "multigrid Poisson start from the previous potential (learned start for each density "
                              "slot's first solve), unchanged Jacobi stop rule; mixed-precision eigensolver "
-                             "(tcgen05 TF32 hi+lo Gram, FP64 finish)",
+                             "(tcgen05 TF32 hi+lo Gram and rotations, FP64 finish); Pulay mixing; eigensolver "
+                             "tolerance following the density change",
                    "poisson_sweeps": sum(h["poisson_sweeps_in"] + h["poisson_sweeps_out"] for h in last.history),
                    "network": train_info,
                    "plain_fp64": {"ms_per_step": plain_ms, "steps": plain_steps, "energy": plain_res[-1].total,

@@ -45,7 +45,8 @@ class dft_scf_opts(C.Structure):
                 ("ks_tol", C.c_double), ("stop_abs_de", C.c_double), ("poisson_tol", C.c_double),
                 ("poisson_max_sweeps", C.c_long), ("extra_bands", C.c_int), ("eig", dft_eig_opts),
                 ("verbose", C.c_int), ("poisson_start", C.c_int), ("poisson_net", C.c_void_p), ("mixer", C.c_int),
-                ("pulay_depth", C.c_int), ("pulay_beta", C.c_double), ("eig_tol_adaptive", C.c_int)]
+                ("pulay_depth", C.c_int), ("pulay_beta", C.c_double), ("adaptive_eig_tol", C.c_int),
+                ("smearing_kt", C.c_double)]
 
 
 # dft_poisson_start
@@ -584,10 +585,14 @@ def _ptr(x):
 def default_scf_options(**kw) -> dft_scf_opts:
     o = dft_scf_opts()
     load().dft_scf_default_options(C.byref(o))
+    scf_fields = {f for f, _ in dft_scf_opts._fields_}
+    eig_fields = {f for f, _ in dft_eig_opts._fields_}
     for k, v in kw.items():
         if k == "poisson_net" and hasattr(v, "handle"):
             v = v.handle
-        if k.startswith("eig_"):
+        if k not in scf_fields and not (k.startswith("eig_") and k[4:] in eig_fields):
+            raise TypeError(f"unknown SCF option {k!r}")
+        if k not in scf_fields:
             setattr(o.eig, k[4:], v)
         else:
             setattr(o, k, v)

@@ -144,6 +144,42 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), db.p);
     }
 
+    // ---- Fermi-Dirac occupations (option; the reference fills the lowest levels) --------
+    const double kt = o.smearing_kt;
+    if (kt < 0.0 || !std::isfinite(kt)) fail(DFT_INVALID_ARGUMENT, "smearing_kt must be >= 0");
+    // f_i = 1 / (1 + exp((e_i - mu) / kt)) with sum f_i = nel, mu by bisection; returns the
+    // number of bands to converge tightly (every band with f_i > 1e-8, at least nel)
+    auto fermi = [&](const std::vector<double>& e, int nel, std::vector<double>& f) {
+        const int m = (int)e.size();
+        if (nel >= m) {
+            std::fill(f.begin(), f.end(), 1.0);
+            return m;
+        }
+        double lo = *std::min_element(e.begin(), e.end()) - 40.0 * kt;
+        double hi = *std::max_element(e.begin(), e.end()) + 40.0 * kt;
+        auto count = [&](double mu) {
+            double c = 0.0;
+            for (int i = 0; i < m; ++i) {
+                const double x = (e[i] - mu) / kt;
+                c += x > 700.0 ? 0.0 : 1.0 / (1.0 + std::exp(x));
+            }
+            return c;
+        };
+        for (int k = 0; k < 200; ++k) {
+            const double mid = 0.5 * (lo + hi);
+            (count(mid) < nel ? lo : hi) = mid;
+        }
+        const double mu = 0.5 * (lo + hi);
+        int nconv = nel;
+        for (int i = 0; i < m; ++i) {
+            const double x = (e[i] - mu) / kt;
+            f[i] = x > 700.0 ? 0.0 : 1.0 / (1.0 + std::exp(x));
+            if (f[i] > 1e-8) nconv = std::max(nconv, i + 1);
+        }
+        return nconv;
+    };
+    int nconv_a = na, nconv_b = nb;
+
     // ---- Pulay mixer state (option; the reference mixes linearly) -----------------------
     const int ns = closed ? 1 : 2;
     const int pdepth = o.pulay_depth > 0 ? std::min(o.pulay_depth, 16) : 8;
@@ -257,10 +293,21 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         // orbitals (:117-144), warm-started from the previous iteration
         t0 = Clock::now();
         EigOpts ek = eo;
-        if (o.eig_tol_adaptive && std::isfinite(prevD)) ek.tol = std::max(eo.tol, std::min(1e-3, 0.1 * prevD));
-        rec.eig_iterations_alpha = solve_orbitals(ctx, g, va.p, na, bands_a, psia.p, ld, true, eiga.data(), resa.data(), ek);
+        if (o.adaptive_eig_tol && std::isfinite(prevD)) ek.tol = std::max(eo.tol, std::min(1e-3, 0.1 * prevD));
+        rec.eig_iterations_alpha =
+            solve_orbitals(ctx, g, va.p, nconv_a, bands_a, psia.p, ld, true, eiga.data(), resa.data(), ek);
         if (!closed)
-            rec.eig_iterations_beta = solve_orbitals(ctx, g, vb.p, nb, bands_b, psib.p, ld, true, eigb.data(), resb.data(), ek);
+            rec.eig_iterations_beta =
+                solve_orbitals(ctx, g, vb.p, nconv_b, bands_b, psib.p, ld, true, eigb.data(), resb.data(), ek);
+        if (kt > 0.0) {
+            nconv_a = fermi(eiga, na, occa);
+            if (closed) {
+                occb = occa;
+                nconv_b = nconv_a;
+            } else {
+                nconv_b = fermi(eigb, nb, occb);
+            }
+        }
         rec.ms_orbitals = ms_since(t0);
         // output densities (:160-187)
         t0 = Clock::now();
@@ -274,11 +321,19 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         rec.poisson_sweeps_out = jout.sweeps;
         // energies (TotalEnergyMolecule.cpp:237-333): orbitals alpha then beta in one sum
         t0 = Clock::now();
-        kinetic_per_band(ctx, g, psia.p, na, ld, Ta.data());
-        if (!closed) kinetic_per_band(ctx, g, psib.p, nb, ld, Tb.data());
         double T = 0.0;
-        for (int i = 0; i < na; ++i) T += 1.0 * Ta[i];
-        for (int i = 0; i < nb; ++i) T += 1.0 * (closed ? Ta[i] : Tb[i]);
+        if (kt > 0.0) {
+            // fractional occupations over every band that carries charge
+            kinetic_per_band(ctx, g, psia.p, nconv_a, ld, Ta.data());
+            if (!closed) kinetic_per_band(ctx, g, psib.p, nconv_b, ld, Tb.data());
+            for (int i = 0; i < nconv_a; ++i) T += occa[i] * Ta[i];
+            for (int i = 0; i < (closed ? nconv_a : nconv_b); ++i) T += occb[i] * (closed ? Ta[i] : Tb[i]);
+        } else {
+            kinetic_per_band(ctx, g, psia.p, na, ld, Ta.data());
+            if (!closed) kinetic_per_band(ctx, g, psib.p, nb, ld, Tb.data());
+            for (int i = 0; i < na; ++i) T += 1.0 * Ta[i];
+            for (int i = 0; i < nb; ++i) T += 1.0 * (closed ? Ta[i] : Tb[i]);
+        }
         const double eext = dot3(ctx, N, orho.p, vext.p, g.dV);
         const double eh = 0.5 * dot(ctx, N, orho.p, ovh.p) * g.dV;
         const double exc = xc(ctx, g, kind, oa.p, ob.p, nullptr, nullptr, true);

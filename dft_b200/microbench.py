@@ -66,6 +66,9 @@ def main():
                     help="scf/poisson: start of each Poisson solve")
     ap.add_argument("--precond", type=int, default=4,
                     help="scf: eigensolver preconditioner (0 diagonal, k > 0 smoothing steps, -1 multigrid)")
+    ap.add_argument("--mixer", type=int, default=0, help="scf: 0 linear (reference), 1 Pulay")
+    ap.add_argument("--adaptive", type=int, default=0, help="scf: adaptive eigensolver tolerance")
+    ap.add_argument("--smearing", type=float, default=0.0, help="scf: Fermi-Dirac temperature (Ha), 0 = aufbau")
     ap.add_argument("--train", type=int, default=0,
                     help="scf/poisson with a network start: train on this many synthetic densities first")
     ap.add_argument("--n", type=int, default=128)
@@ -137,7 +140,8 @@ def main():
             out["train"] = {k: rep[k] for k in ("steps", "seconds_data", "seconds_train", "val_loss",
                                                 "val_loss_coarse")}
         o = d.default_scf_options(max_iterations=a.iterations, extra_bands=w["extra_bands"], verbose=int(a.verbose),
-                                  stop_abs_de=a.stop_abs_de, poisson_start=POISSON[a.poisson])
+                                  stop_abs_de=a.stop_abs_de, poisson_start=POISSON[a.poisson], mixer=a.mixer,
+                                  adaptive_eig_tol=a.adaptive, smearing_kt=a.smearing)
         if net is not None:
             o.poisson_net = net.handle
         o.eig.verbose = int(a.verbose > 2)

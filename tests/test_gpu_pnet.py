@@ -177,7 +177,7 @@ def test_pulay_mixer_same_energy(engine, case):
     res = {}
     for mixer, adaptive in ((0, 0), (1, 0), (1, 1)):
         o = dft_b200.default_scf_options(stop_abs_de=1e-8, poisson_start=dft_b200.POISSON_MULTIGRID, mixer=mixer,
-                                         eig_tol_adaptive=adaptive)
+                                         adaptive_eig_tol=adaptive)
         r = engine.scf_molecule(g, m, 0, mult, "PBE96", o)
         res[(mixer, adaptive)] = (r.total, r.iterations)
     print(case, res)
@@ -185,3 +185,21 @@ def test_pulay_mixer_same_energy(engine, case):
     for k, (e, it) in res.items():
         assert abs(e - e0) < 1e-6, (k, res)
     assert res[(1, 0)][1] <= res[(0, 0)][1]
+
+
+def test_fermi_smearing_limits(engine):
+    """A small smearing temperature reproduces the integer-occupation energy of a gapped
+    molecule; a larger one still converges."""
+    g = dft_b200.CartesianGrid(28, 28, 28, -5.4, 5.4, -5.4, 5.4, -5.4, 5.4)
+    m = dft_b200.Molecule()
+    m.addNucleus(1, -0.7, 0.0, 0.0)
+    m.addNucleus(1, 0.7, 0.0, 0.0)
+    e = {}
+    for kt in (0.0, 1e-4, 2e-2):
+        o = dft_b200.default_scf_options(stop_abs_de=1e-8, poisson_start=dft_b200.POISSON_MULTIGRID, mixer=1,
+                                         smearing_kt=kt)
+        r = engine.scf_molecule(g, m, 0, 1, "PZ81", o)
+        e[kt] = (r.total, r.iterations)
+    print(e)
+    assert abs(e[1e-4][0] - e[0.0][0]) < 1e-6
+    assert np.isfinite(e[2e-2][0]) and e[2e-2][1] < 100
