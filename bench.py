@@ -196,9 +196,9 @@ def measure_jacobi(eng, torch, stream, w):
 
 
 def measure_gram(eng, torch, stream, w, ka, kb, reps=20):
-    """The eigensolver's FP64 Gram product (gram_kernel + gram_reduce_kernel) at the workload's
-    grid with the basis/new-block widths of its Davidson iterations.  Algorithmic bytes per
-    call = N (ka + kb) 8 (both blocks read once)."""
+    """The eigensolver's FP64 Gram product at the workload's grid with the basis/new-block
+    widths of its Davidson iterations (narrow blocks: gram_small_kernel, one launch with the
+    reduction done by the last block).  Algorithmic bytes per call = N (ka + kb) 8."""
     import dft_b200
     g = dft_b200.CartesianGrid(*w["n"], *w["bounds"])
     N = g.getSize()
@@ -431,7 +431,7 @@ def main():
                    "plain_energy_error_vs_tight": plain_res[-1].total - tight_res[-1].total},
         "gpu_launches": launches,
         "e2e": {"value": e2e_val, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "kernel": "gram_kernel + gram_reduce_kernel (FP64 Gram of the eigensolver)",
+        "roofline": {"bound": "hbm", "kernel": "gram_small_kernel (FP64 Gram of the eigensolver, one launch)",
                      "achieved": gr["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": gr["gbs"] / peaks["hbm_gbs"], "peak_source": peaks["source"], "traffic": None,
                      "bytes_per_call": gr["bytes"], "ms_per_call": gr["ms"], "ka": gr["ka"], "kb": gr["kb"],
