@@ -134,17 +134,13 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         }
 
     // ---- initial densities from orbitals in the bare V_ext (MolecularSCFHelpers.cpp:515-579) --
-    // With the adaptive tolerance these orbitals only seed the first density, which the SCF
-    // replaces at once: 1e-3 is enough.
-    EigOpts e0 = eo;
-    if (o.adaptive_eig_tol) e0.tol = std::max(eo.tol, 1e-3);
-    int it_a = solve_orbitals(ctx, g, vext.p, na, bands_a, psia.p, ld, false, eiga.data(), resa.data(), e0);
+    int it_a = solve_orbitals(ctx, g, vext.p, na, bands_a, psia.p, ld, false, eiga.data(), resa.data(), eo);
     (void)it_a;
     spin_density(ctx, N, psia.p, bands_a, ld, occa.data(), da.p);
     if (closed) {
         DFT_CUDA(cudaMemcpyAsync(db.p, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
     } else {
-        solve_orbitals(ctx, g, vext.p, nb, bands_b, psib.p, ld, false, eigb.data(), resb.data(), e0);
+        solve_orbitals(ctx, g, vext.p, nb, bands_b, psib.p, ld, false, eigb.data(), resb.data(), eo);
         spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), db.p);
     }
 
@@ -297,8 +293,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         // orbitals (:117-144), warm-started from the previous iteration
         t0 = Clock::now();
         EigOpts ek = eo;
-        if (o.adaptive_eig_tol)
-            ek.tol = std::max(eo.tol, std::isfinite(prevD) ? std::min(1e-3, 0.1 * prevD) : 1e-3);
+        if (o.adaptive_eig_tol && std::isfinite(prevD)) ek.tol = std::max(eo.tol, std::min(1e-3, 0.1 * prevD));
         rec.eig_iterations_alpha =
             solve_orbitals(ctx, g, va.p, nconv_a, bands_a, psia.p, ld, true, eiga.data(), resa.data(), ek);
         if (!closed)

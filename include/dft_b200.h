@@ -211,8 +211,7 @@ typedef struct {
     int mixer;               /* 0: linear with the adaptive factor; 1: Pulay (DIIS) on n_out - n_in */
     int pulay_depth;         /* history length for the Pulay mixer (0 = 8) */
     double pulay_beta;       /* step along the extrapolated residual (0 = 0.2) */
-    int adaptive_eig_tol;    /* 1: eigensolver tolerance max(eig.tol, min(1e-3, 0.1 * previous dRho)), and
-                                1e-3 for the initial orbitals and the first iteration */
+    int adaptive_eig_tol;    /* 1: eigensolver tolerance max(eig.tol, min(1e-3, 0.1 * previous dRho)) */
     double smearing_kt;      /* > 0: Fermi-Dirac occupations at this temperature (Ha) over the extra
                                 bands instead of the reference's integer aufbau (0) */
 } dft_scf_opts;
