@@ -6,6 +6,7 @@ h2o_128      H2O (O at the origin, O-H 1.81 bohr, HOH 104.5 deg), 128^3 grid, h 
 cluster20    20 nuclei with Z drawn from {1, 6, 7, 8}, positions uniform in a 24-bohr cube centred
              in a 192^3 grid (h = 0.2), minimum separation 2.0 bohr, no nucleus within 1e-12 of a
              node, neutral, multiplicity 1 + (N_e mod 2), PBE96 (seeded numpy generator)
+cluster20_clear  the same draw with every nucleus at least 0.08 bohr from the nearest node
 """
 from __future__ import annotations
 
@@ -35,7 +36,10 @@ def h2o_128(n=128, h=0.2):
                 desc=f"H2O PBE96 {n}^3 h={h}, multiplicity 1, 5 occupied + 7 extra bands")
 
 
-def cluster(natoms=20, n=192, h=0.2, box=24.0, min_sep=2.0, seed=20261203, extra_bands=8):
+def cluster(natoms=20, n=192, h=0.2, box=24.0, min_sep=2.0, seed=20261203, extra_bands=8, min_node_distance=0.0):
+    """min_node_distance > 0 also rejects nuclei closer than that (bohr) to the nearest grid node:
+    the point-nucleus potential -Z/r at a node 0.01 bohr from a nucleus is a single-node spike
+    (-76 Ha for hydrogen) that binds a spurious grid-scale state."""
     rng = np.random.default_rng(seed)
     grid_n, b = _cube(n, h)
     lo = b[0]
@@ -48,6 +52,8 @@ def cluster(natoms=20, n=192, h=0.2, box=24.0, min_sep=2.0, seed=20261203, extra
         f = (p - lo) / h
         if np.any(np.abs(f - np.round(f)) * h < 1e-12):
             continue
+        if min_node_distance > 0.0 and np.linalg.norm((f - np.round(f)) * h) < min_node_distance:
+            continue
         xyz.append(p)
         Z.append(int(rng.choice([1, 6, 7, 8])))
     ne = sum(Z)
@@ -56,7 +62,15 @@ def cluster(natoms=20, n=192, h=0.2, box=24.0, min_sep=2.0, seed=20261203, extra
                 desc=f"{natoms}-atom cluster (Z in {{1,6,7,8}}, seed {seed}), {ne} electrons, PBE96 {n}^3 h={h}")
 
 
-SYSTEMS = {"h2_48": h2_48, "h2o_128": h2o_128, "cluster20": cluster}
+def cluster_clear(**kw):
+    """cluster20 with every nucleus at least 0.08 bohr from the nearest grid node."""
+    w = cluster(min_node_distance=0.08, **kw)
+    w["name"] += "_clear"
+    w["desc"] += ", nuclei >= 0.08 bohr from grid nodes"
+    return w
+
+
+SYSTEMS = {"h2_48": h2_48, "h2o_128": h2o_128, "cluster20": cluster, "cluster20_clear": cluster_clear}
 
 
 def get(name, **kw):
