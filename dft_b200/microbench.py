@@ -7,6 +7,7 @@
     python -m dft_b200.microbench radial                              # 60 atoms, one launch
     python -m dft_b200.microbench gram   --n 64 --ka 64 --kb 64 --precision 1   # tcgen05 Gram
     python -m dft_b200.microbench poisson --n 128 --poisson multigrid [--train 32]
+    python -m dft_b200.microbench train --n 96 --tc 1                 # network training step
     python -m dft_b200.microbench scf --system h2o_128 --poisson multigrid --mixed 1 --stop-abs-de 1e-6
 
 Each mode prints one JSON line with the time and the achieved bandwidth for the
@@ -57,7 +58,8 @@ def cube(n, h):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram", "poisson"])
+    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram", "poisson", "train"])
+    ap.add_argument("--tc", type=int, default=1, help="network convolutions on the tensor cores (1) or CUDA cores (0)")
     ap.add_argument("--ka", type=int, default=64)
     ap.add_argument("--kb", type=int, default=64)
     ap.add_argument("--precision", type=int, default=0, help="gram: 0 = FP64, 1 = tensor cores (TF32 hi+lo)")
@@ -87,6 +89,7 @@ def main():
 
     eng = d.Engine(0)
     eng.set_tuning("jacobi_sweeps_per_launch", a.spl)
+    eng.set_tuning("network_tensor_cores", a.tc)
     stream = torch.cuda.ExternalStream(eng.stream)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     out = {"mode": a.mode}
@@ -177,6 +180,13 @@ def main():
         t = _events(torch, stream, run, a.reps)
         out.update(n=a.n, poisson=a.poisson, network=bool(net), ms=statistics.median(t), sweeps=res["s"],
                    cycles=res["c"])
+    elif a.mode == "train":
+        g = cube(a.n, a.h)
+        net = d.PoissonNet(eng, seed=7)
+        rep = net.train([g], samples=16, validation=4, epochs=3, batch=4, lr=3e-3, lr_min=1e-4, seed=5,
+                        smooth_sweeps=0, mse_weight=1.0)
+        out.update(n=a.n, tc=a.tc, ms_per_step=rep["ms_per_step"], samples_per_step=4, steps=rep["steps"],
+                   seconds_data=rep["seconds_data"], val_loss=rep["val_loss"], val_loss_coarse=rep["val_loss_coarse"])
     elif a.mode == "gram":
         g = cube(a.n, a.h)
         N = g.getSize()
