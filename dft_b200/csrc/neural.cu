@@ -296,10 +296,13 @@ constexpr size_t tcc_smem_bytes() {
            + al16((size_t)TCC_HX * TCC_HY * TCC_HZ * CIN * 2);      // halo
 }
 
-template <int CIN, int COUT>
+// BWD = true: data gradient of a convolution (w = flipped, transposed weights, in = the
+// output gradient rounded to BF16): g = sum * silu'(zprev), stored in FP32 to gout.
+template <int CIN, int COUT, bool BWD>
 __global__ void __launch_bounds__(TCC_THREADS, 1)
     conv3_tc_kernel(Vol v, const bf16* __restrict__ in, const bf16* __restrict__ w, const float* __restrict__ bias,
-                    bf16* __restrict__ zout, bf16* __restrict__ aout, int* __restrict__ error) {
+                    bf16* __restrict__ zout, bf16* __restrict__ aout, float* __restrict__ gout,
+                    const bf16* __restrict__ zprev, int* __restrict__ error) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint32_t s_tmem;
     __shared__ __align__(8) uint64_t bar;
@@ -396,15 +399,22 @@ __global__ void __launch_bounds__(TCC_THREADS, 1)
                          : "r"(addr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int q = 0; q < 8; ++q) z[c0 + q] = __uint_as_float(r[q]) + bias[half * HC + c0 + q];
+            for (int q = 0; q < 8; ++q) z[c0 + q] = __uint_as_float(r[q]) + (BWD ? 0.f : bias[half * HC + c0 + q]);
         }
         if (gx < v.nx && gy < v.ny) {
             const long long p = ((long long)z0 * v.ny + gy) * v.nx + gx;
-            float a[HC];
+            if constexpr (BWD) {
+                float zp[HC];
+                ldrow<HC>(zprev + p * COUT + half * HC, zp);
 #pragma unroll
-            for (int c = 0; c < HC; ++c) a[c] = silu(z[c]);
-            strow<HC>(zout + p * COUT + half * HC, z);
-            strow<HC>(aout + p * COUT + half * HC, a);
+                for (int c = 0; c < HC; ++c) gout[p * COUT + half * HC + c] = z[c] * dsilu(zp[c]);
+            } else {
+                float a[HC];
+#pragma unroll
+                for (int c = 0; c < HC; ++c) a[c] = silu(z[c]);
+                strow<HC>(zout + p * COUT + half * HC, z);
+                strow<HC>(aout + p * COUT + half * HC, a);
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -929,6 +939,7 @@ struct dft_pnet {
     dftb::DBuf<float> y, dz[12], t, e0, e1, e2, dy;
     dftb::DBuf<double> red;
     dftb::DBuf<int> tc_err;  // set by a tensor-core convolution block whose wait timed out
+    dftb::DBuf<__nv_bfloat16> dzb;  // output gradient rounded to BF16 for the tensor-core data gradient
 };
 
 namespace dftb {
@@ -962,13 +973,35 @@ void launch_conv3_tc(dft_context* ctx, Vol v, const bf16* in, const bf16* w, con
     constexpr size_t sm = tcc_smem_bytes<CIN, COUT>();
     static bool once = false;
     if (!once) {
-        set_smem(conv3_tc_kernel<CIN, COUT>, sm);
+        set_smem(conv3_tc_kernel<CIN, COUT, false>, sm);
         once = true;
     }
     dim3 grid((v.nx + TCC_X - 1) / TCC_X, (v.ny + TCC_Y - 1) / TCC_Y, v.nz);
-    conv3_tc_kernel<CIN, COUT><<<grid, TCC_THREADS, sm, ctx->stream>>>(v, in, w, bias, z, a, err);
+    conv3_tc_kernel<CIN, COUT, false><<<grid, TCC_THREADS, sm, ctx->stream>>>(v, in, w, bias, z, a, nullptr, nullptr,
+                                                                              err);
     DFT_LAUNCH_CHECK();
     count_launch(ctx);
+}
+
+// Data gradient on the tensor cores: the output gradient dz (FP32) is rounded to BF16, then
+// convolved with the flipped, transposed weights wT; gout = result * silu'(zprev).
+template <int C>
+void launch_conv3_tc_bwd(dft_context* ctx, PNet* n, Vol v, const float* dz, const bf16* wT, float* gout,
+                         const bf16* zprev, int* err) {
+    constexpr size_t sm = tcc_smem_bytes<C, C>();
+    static bool once = false;
+    if (!once) {
+        set_smem(conv3_tc_kernel<C, C, true>, sm);
+        once = true;
+    }
+    const long long cnt = v.n() * C;
+    bf16* dzb = n->dzb.get((size_t)cnt);
+    to_bf16_kernel<<<blocks_for(ctx, cnt), 256, 0, ctx->stream>>>(cnt, dz, dzb);
+    dim3 grid((v.nx + TCC_X - 1) / TCC_X, (v.ny + TCC_Y - 1) / TCC_Y, v.nz);
+    conv3_tc_kernel<C, C, true><<<grid, TCC_THREADS, sm, ctx->stream>>>(v, dzb, wT, nullptr, nullptr, nullptr, gout,
+                                                                       zprev, err);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx, 2);
 }
 
 template <int CIN, int COUT>
@@ -1147,6 +1180,17 @@ void backward(dft_context* ctx, PNet* n, Vol v0, const bf16* x, const float* t, 
     auto GW = [&](int i) { return G + n->L[i].w; };
     auto GB = [&](int i) { return G + n->L[i].b; };
     const int ew = 256;
+    const bool tc = ctx->net_tensor_cores != 0;
+    int* err = n->tc_err.get(1);
+    // data gradient of a square 3x3x3 layer (weights already flipped into n->wT)
+    auto conv_bwd16 = [&](Vol vv, const float* dzin, float* gout, const bf16* zprev) {
+        if (tc) launch_conv3_tc_bwd<16>(ctx, n, vv, dzin, n->wT.p, gout, zprev, err);
+        else launch_conv3<16, 16, float, true>(ctx, vv, dzin, n->wT.p, nullptr, nullptr, nullptr, gout, nullptr, zprev);
+    };
+    auto conv_bwd32 = [&](Vol vv, const float* dzin, float* gout, const bf16* zprev) {
+        if (tc) launch_conv3_tc_bwd<32>(ctx, n, vv, dzin, n->wT.p, gout, zprev, err);
+        else launch_conv3<32, 32, float, true>(ctx, vv, dzin, n->wT.p, nullptr, nullptr, nullptr, gout, nullptr, zprev);
+    };
     const long long nint = (long long)std::max(v0.nx - 2, 1) * std::max(v0.ny - 2, 1) * std::max(v0.nz - 2, 1);
     float* dy = n->dy.get((size_t)v0.n());
     loss_dy(ctx, n, v0, L, n->y.p, t, dy, n->red.p);
@@ -1157,8 +1201,7 @@ void backward(dft_context* ctx, PNet* n, Vol v0, const bf16* x, const float* t, 
     // c11: conv3 16->16 at level 0
     launch_wgrad<16, 16>(ctx, v0, n->a[9].p, n->dz[10].p, GW(10), GB(10));
     flip(ctx, 16, 16, W(10), n->wT.p);
-    launch_conv3<16, 16, float, true>(ctx, v0, n->dz[10].p, n->wT.p, nullptr, nullptr, nullptr, n->dz[9].p, nullptr,
-                                      n->z[9].p);
+    conv_bwd16(v0, n->dz[10].p, n->dz[9].p, n->z[9].p);
     // c10: up 32->16 (+ skip a1)
     pair_wgrad_kernel<32, 16, true><<<blocks_for(ctx, v1.n(), 16), 256, 0, ctx->stream>>>(v0, v1, n->a[8].p,
                                                                                           n->dz[9].p, GW(9), GB(9));
@@ -1169,8 +1212,7 @@ void backward(dft_context* ctx, PNet* n, Vol v0, const bf16* x, const float* t, 
     // c9: conv3 32->32 at level 1
     launch_wgrad<32, 32>(ctx, v1, n->a[7].p, n->dz[8].p, GW(8), GB(8));
     flip(ctx, 32, 32, W(8), n->wT.p);
-    launch_conv3<32, 32, float, true>(ctx, v1, n->dz[8].p, n->wT.p, nullptr, nullptr, nullptr, n->dz[7].p, nullptr,
-                                      n->z[7].p);
+    conv_bwd32(v1, n->dz[8].p, n->dz[7].p, n->z[7].p);
     // c8: up 32->32 (+ skip a3)
     pair_wgrad_kernel<32, 32, true><<<blocks_for(ctx, v2.n(), 16), 256, 0, ctx->stream>>>(v1, v2, n->a[6].p,
                                                                                           n->dz[7].p, GW(7), GB(7));
@@ -1181,12 +1223,10 @@ void backward(dft_context* ctx, PNet* n, Vol v0, const bf16* x, const float* t, 
     // c7, c6: conv3 32->32 at level 2
     launch_wgrad<32, 32>(ctx, v2, n->a[5].p, n->dz[6].p, GW(6), GB(6));
     flip(ctx, 32, 32, W(6), n->wT.p);
-    launch_conv3<32, 32, float, true>(ctx, v2, n->dz[6].p, n->wT.p, nullptr, nullptr, nullptr, n->dz[5].p, nullptr,
-                                      n->z[5].p);
+    conv_bwd32(v2, n->dz[6].p, n->dz[5].p, n->z[5].p);
     launch_wgrad<32, 32>(ctx, v2, n->a[4].p, n->dz[5].p, GW(5), GB(5));
     flip(ctx, 32, 32, W(5), n->wT.p);
-    launch_conv3<32, 32, float, true>(ctx, v2, n->dz[5].p, n->wT.p, nullptr, nullptr, nullptr, n->dz[4].p, nullptr,
-                                      n->z[4].p);
+    conv_bwd32(v2, n->dz[5].p, n->dz[4].p, n->z[4].p);
     // c5: down 32->32; a3 also feeds the skip of c8
     pair_wgrad_kernel<32, 32, false><<<blocks_for(ctx, v2.n(), 16), 256, 0, ctx->stream>>>(v1, v2, n->a[3].p,
                                                                                            n->dz[4].p, GW(4), GB(4));
@@ -1197,8 +1237,7 @@ void backward(dft_context* ctx, PNet* n, Vol v0, const bf16* x, const float* t, 
     // c4: conv3 32->32 at level 1
     launch_wgrad<32, 32>(ctx, v1, n->a[2].p, n->dz[3].p, GW(3), GB(3));
     flip(ctx, 32, 32, W(3), n->wT.p);
-    launch_conv3<32, 32, float, true>(ctx, v1, n->dz[3].p, n->wT.p, nullptr, nullptr, nullptr, n->dz[2].p, nullptr,
-                                      n->z[2].p);
+    conv_bwd32(v1, n->dz[3].p, n->dz[2].p, n->z[2].p);
     // c3: down 16->32; a1 also feeds the skip of c10
     pair_wgrad_kernel<16, 32, false><<<blocks_for(ctx, v1.n(), 16), 256, 0, ctx->stream>>>(v0, v1, n->a[1].p,
                                                                                            n->dz[2].p, GW(2), GB(2));
@@ -1209,8 +1248,7 @@ void backward(dft_context* ctx, PNet* n, Vol v0, const bf16* x, const float* t, 
     // c2: conv3 16->16 at level 0
     launch_wgrad<16, 16>(ctx, v0, n->a[0].p, n->dz[1].p, GW(1), GB(1));
     flip(ctx, 16, 16, W(1), n->wT.p);
-    launch_conv3<16, 16, float, true>(ctx, v0, n->dz[1].p, n->wT.p, nullptr, nullptr, nullptr, n->dz[0].p, nullptr,
-                                      n->z[0].p);
+    conv_bwd16(v0, n->dz[1].p, n->dz[0].p, n->z[0].p);
     // c1: weights only
     launch_wgrad<2, 16>(ctx, v0, x, n->dz[0].p, GW(0), GB(0));
 }
