@@ -58,11 +58,15 @@ const char* dft_version(void);
 dft_status_t dft_context_create(int device, dft_context** out);
 dft_status_t dft_context_destroy(dft_context* ctx);
 dft_status_t dft_context_synchronize(dft_context* ctx);
-/* Kernel-shape knobs (results do not depend on them).  Keys:
+/* Kernel-shape knobs.  Keys:
  *   "jacobi_sweeps_per_launch": 0 = auto (default), -2 = the whole solve in the shared memory
  *                               of one 16-block cluster (small grids), -1 = the whole solve in
  *                               one persistent (cooperative) launch, 1 = one sweep per launch,
- *                               2, 4 or 8 = temporally blocked sweeps per launch. */
+ *                               2, 4 or 8 = temporally blocked sweeps per launch (results are
+ *                               identical for every value).
+ *   "network_tensor_cores":     1 (default) = the Poisson-start network's 16- and 32-channel
+ *                               convolutions on tcgen05, 0 = FP32 CUDA cores (results agree to
+ *                               BF16 rounding, not bit for bit). */
 dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long value);
 /* The cudaStream_t the context launches on, as an opaque handle (for event timing). */
 void* dft_context_stream(dft_context* ctx);
