@@ -363,6 +363,15 @@ def main():
         total_ms, ms, results, launches = run(fast, args.warmup, args.steps)
     ms_per_step = total_ms / args.steps
     value = world * args.steps / (total_ms * 1e-3)
+    # e2e through the host C-ABI call, with both spin densities returned to host memory,
+    # right after the device-timed steps
+    e2e_ms = []
+    for _ in range(max(1, min(3, args.steps))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.scf_molecule(g, mol, 0, w["multiplicity"], w["functional"], fast, want_density=True)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_val = world / (statistics.median(e2e_ms) * 1e-3)
     # the plain FP64 method (the reference's algorithm) on the same GPU, for the comparison
     plain_steps = max(1, min(args.steps, w.get("plain_steps", 3)))
     plain_total, _, plain_res, _ = run(plain, 1, plain_steps)
@@ -374,16 +383,7 @@ def main():
     tight = _d.default_scf_options(stop_abs_de=1e-9, extra_bands=w["extra_bands"],
                                    poisson_tol=jacobi_tight_tol(w), poisson_max_sweeps=400000)
     tight_total, _, tight_res, _ = run(tight, 0, 1)
-    opts = fast
 
-    # e2e through the host C-ABI call, with both spin densities returned to host memory
-    e2e_ms = []
-    for _ in range(max(1, min(3, args.steps))):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        eng.scf_molecule(g, mol, 0, w["multiplicity"], w["functional"], opts, want_density=True)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_val = world / (statistics.median(e2e_ms) * 1e-3)
     N = g.getSize()
     h2d = len(w["Z"]) * (4 + 24)
     d2h = 2 * N * 8
