@@ -87,7 +87,7 @@ dft_status_t dft_context_create(int device, dft_context** out) {
         cudaDeviceProp prop;
         DFT_CUDA(cudaGetDeviceProperties(&prop, device));
         if (prop.major < 10)
-            dftb::fail(DFT_CUDA_ERROR, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+            dftb::fail(DFT_CUDA_ERROR, "device %d is sm_%d%d; the library is compiled for sm_100a", device, prop.major, prop.minor);
         auto* c = new dft_context();
         c->device = device;
         c->num_sms = prop.multiProcessorCount;
