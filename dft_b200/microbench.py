@@ -8,6 +8,7 @@
     python -m dft_b200.microbench gram   --n 64 --ka 64 --kb 64 --precision 1   # tcgen05 Gram
     python -m dft_b200.microbench poisson --n 128 --poisson multigrid [--train 32]
     python -m dft_b200.microbench train --n 96 --tc 1                 # network training step
+    python -m dft_b200.microbench rotate --n 64 --ka 128 --kb 64 --precision 1   # tcgen05 rotation
     python -m dft_b200.microbench scf --system h2o_128 --poisson multigrid --mixed 1 --stop-abs-de 1e-6
 
 Each mode prints one JSON line with the time and the achieved bandwidth for the
@@ -58,7 +59,7 @@ def cube(n, h):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram", "poisson", "train"])
+    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram", "poisson", "train", "rotate"])
     ap.add_argument("--tc", type=int, default=1, help="network convolutions on the tensor cores (1) or CUDA cores (0)")
     ap.add_argument("--ka", type=int, default=64)
     ap.add_argument("--kb", type=int, default=64)
@@ -180,6 +181,18 @@ def main():
         t = _events(torch, stream, run, a.reps)
         out.update(n=a.n, poisson=a.poisson, network=bool(net), ms=statistics.median(t), sweeps=res["s"],
                    cycles=res["c"])
+    elif a.mode == "rotate":
+        g = cube(a.n, a.h)
+        N = g.getSize()
+        k, m = a.ka, a.kb
+        rng = np.random.default_rng(0)
+        V = eng.upload(rng.standard_normal(N * k))
+        X = eng.array(N * m)
+        Y = rng.standard_normal((k, m))
+        t = _events(torch, stream, lambda: eng.rotate(g, V, N, k, Y, X, N, precision=a.precision), a.reps, flush)
+        ms = statistics.median(t)
+        out.update(n=a.n, k=k, m=m, precision=a.precision, ms=ms, tflops=2.0 * N * k * m / (ms * 1e-3) / 1e12,
+                   gbs=8.0 * N * (k + m) / (ms * 1e-3) / 1e9)
     elif a.mode == "train":
         g = cube(a.n, a.h)
         net = d.PoissonNet(eng, seed=7)
