@@ -46,7 +46,8 @@ class dft_scf_opts(C.Structure):
                 ("poisson_max_sweeps", C.c_long), ("extra_bands", C.c_int), ("eig", dft_eig_opts),
                 ("verbose", C.c_int), ("poisson_start", C.c_int), ("poisson_net", C.c_void_p), ("mixer", C.c_int),
                 ("pulay_depth", C.c_int), ("pulay_beta", C.c_double), ("adaptive_eig_tol", C.c_int),
-                ("smearing_kt", C.c_double)]
+                ("smearing_kt", C.c_double), ("kerker_q0", C.c_double),
+                ("initial_density", C.c_int)]
 
 
 # dft_poisson_start
@@ -116,6 +117,7 @@ _SIGS = {
     "dft_context_set_tuning": ([_P, C.c_char_p, C.c_long], C.c_int),
     "dft_context_stream": ([_P], C.c_void_p),
     "dft_context_launch_count": ([_P], C.c_longlong),
+    "dft_context_counter": ([_P, C.c_char_p], C.c_longlong),
     "dft_device_alloc": ([_P, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
     "dft_device_free": ([_P, _P], C.c_int),
     "dft_copy_h2d": ([_P, _P, _P, C.c_size_t], C.c_int),
@@ -134,6 +136,7 @@ _SIGS = {
                                 C.POINTER(dft_eig_opts), C.POINTER(C.c_int)], C.c_int),
     "dft_rotate_dev": ([_P, C.POINTER(dft_grid), _P, C.c_long, C.c_int, _D, C.c_int, _P, C.c_long, C.c_int],
                        C.c_int),
+    "dft_screened_poisson_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double], C.c_int),
     "dft_gram_dev": ([_P, C.POINTER(dft_grid), _P, C.c_long, C.c_int, _P, C.c_long, C.c_int, C.c_int, _D], C.c_int),
     "dft_scf_default_options": ([C.POINTER(dft_scf_opts)], None),
     "dft_scf_molecule": ([_P, C.POINTER(dft_grid), C.c_int, C.POINTER(C.c_int), _D, C.c_int, C.c_int, C.c_int,
@@ -351,6 +354,9 @@ class Engine:
     def launches(self) -> int:
         return load().dft_context_launch_count(self.ctx)
 
+    def counter(self, name: str) -> int:
+        return load().dft_context_counter(self.ctx, name.encode())
+
     def array(self, n) -> DeviceArray:
         return DeviceArray(self, n)
 
@@ -435,6 +441,11 @@ class Engine:
         out = np.zeros((ka, kb))
         _check(load().dft_gram_dev(self.ctx, C.byref(g), _ptr(A), lda, ka, _ptr(B), ldb, kb, int(precision), _dp(out)))
         return out
+
+    def screened_poisson(self, grid, src, x, q2):
+        """x ~ (-lap_h + q2)^{-1} src by one multigrid cycle (the Kerker mixer's screening solve)."""
+        g = grid.c()
+        _check(load().dft_screened_poisson_dev(self.ctx, C.byref(g), _ptr(src), _ptr(x), float(q2)))
 
     def rotate(self, grid, V, ldv, k, Y, X, ldx, precision=0):
         """X = V * Y for band blocks (Y: k x m host matrix)."""

@@ -36,6 +36,7 @@ SOURCES = {
     "neural.cu": [],
     "poisson_start.cu": [],
     "precond_mg.cu": [],
+    "atomic_start.cu": [],
     "eigh.cpp": [],
 }
 

@@ -41,6 +41,8 @@ dft_status_t guard(dft_context* ctx, F&& f) {
 namespace dftb {
 
 void* ws_get(dft_context* ctx, int slot, size_t bytes) {
+    static_assert(WS_NUM <= (int)(sizeof(ctx->ws) / sizeof(ctx->ws[0])), "workspace slots");
+    if (slot < 0 || slot >= WS_NUM) fail(DFT_INVALID_ARGUMENT, "workspace slot %d out of range", slot);
     Workspace& w = ctx->ws[slot];
     if (w.bytes >= bytes && w.ptr) return w.ptr;
     if (w.ptr) {
@@ -88,6 +90,9 @@ dft_status_t dft_context_create(int device, dft_context** out) {
         DFT_CUDA(cudaGetDeviceProperties(&prop, device));
         if (prop.major < 10)
             dftb::fail(DFT_CUDA_ERROR, "device %d is sm_%d%d; the library is compiled for sm_100a", device, prop.major, prop.minor);
+        // the allocation-free Hartree entry point's fixed array: load its module now, while
+        // allocating is allowed, rather than at that entry point's first call
+        dftb::noalloc_scratch(device);
         auto* c = new dft_context();
         c->device = device;
         c->num_sms = prop.multiProcessorCount;
@@ -132,6 +137,9 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
         } else if (k == "network_tensor_cores") {
             NEED(value == 0 || value == 1, "network_tensor_cores must be 0 or 1");
             ctx->net_tensor_cores = (int)value;
+        } else if (k == "hpsi_bands_per_thread") {
+            NEED(value == 0 || value == 1 || value == 2 || value == 4, "hpsi_bands_per_thread must be 0 (auto), 1, 2 or 4");
+            ctx->hpsi_bands_per_thread = (int)value;
         } else {
             dftb::fail(DFT_INVALID_ARGUMENT, "unknown tuning key '%s'", key);
         }
@@ -140,6 +148,13 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
 
 void* dft_context_stream(dft_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 long long dft_context_launch_count(dft_context* ctx) { return ctx ? ctx->launches : 0; }
+
+long long dft_context_counter(dft_context* ctx, const char* name) {
+    if (!ctx || !name) return -1;
+    if (!std::strcmp(name, "launches")) return ctx->launches;
+    if (!std::strcmp(name, "tensor_core_products")) return ctx->tc_launches;
+    return -1;
+}
 
 dft_status_t dft_device_alloc(dft_context* ctx, size_t bytes, void** out) {
     return guard(ctx, [&] {
@@ -308,6 +323,15 @@ dft_status_t dft_rotate_dev(dft_context* ctx, const dft_grid* g, const double* V
         std::vector<double> Yv(Y, Y + (size_t)k * m);
         if (precision) dftb::rotate_tc(ctx, G, V, ldv, k, Yv, m, X, ldx);
         else dftb::rotate(ctx, G, V, ldv, k, Yv, m, X, ldx, 1.0, 0.0);
+        dftb::sync(ctx);
+    });
+}
+
+dft_status_t dft_screened_poisson_dev(dft_context* ctx, const dft_grid* g, const double* src, double* x, double q2) {
+    return guard(ctx, [&] {
+        NEED(ctx && src && x, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::screened_poisson_vcycle(ctx, G, src, 1, q2, x, G.N);
         dftb::sync(ctx);
     });
 }

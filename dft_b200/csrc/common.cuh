@@ -95,12 +95,14 @@ struct dft_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     long long launches = 0;
+    long long tc_launches = 0;  // of which tensor-core (tcgen05) eigensolver products
     int num_sms = 148;
     // tuning knobs (dft_context_set_tuning)
     int jacobi_sweeps_per_launch = 0;  // 0 = auto, 1 = one sweep per launch, 2/4/8 = temporal blocking
     int net_tensor_cores = 1;          // network convolutions on tcgen05 (1) or FP32 CUDA cores (0)
+    int hpsi_bands_per_thread = 0;     // H psi bands per thread: 0 = auto, 1, 2 or 4
     // named scratch buffers (reductions, Jacobi ping-pong, XC intermediates, Davidson)
-    dftb::Workspace ws[24];
+    dftb::Workspace ws[32];
     double* host_pinned = nullptr;  // small pinned staging area for scalars
     size_t host_pinned_bytes = 0;
     void* gram_ticket = nullptr;    // block counter of the one-launch narrow Gram product
@@ -133,7 +135,8 @@ enum WsSlot {
     WS_PG2 = 21,
     WS_PG3 = 22,
     WS_PG4 = 23,
-    WS_NUM = 24,
+    WS_TMP3 = 24,    // superposition start tables (atomic_start.cu)
+    WS_NUM = 25,     // slots in use (dft_context::ws has room for 32)
 };
 
 void* ws_get(dft_context* ctx, int slot, size_t bytes);

@@ -450,7 +450,8 @@ void gram_fp64(dft_context* ctx, const Grid& g, const double* A, long long lda, 
 }
 
 int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, int nbands, double* psi,
-                   long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o) {
+                   long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o,
+                   const double* start, int nstart) {
     if (nocc <= 0) fail(DFT_INVALID_ARGUMENT, "El numero de orbitales debe ser mayor que cero.");
     if (nbands < nocc) fail(DFT_INVALID_ARGUMENT, "nbands must be >= the number of orbitals");
     if (nbands > g.N) fail(DFT_INVALID_ARGUMENT, "more bands than grid points");
@@ -472,8 +473,16 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
     const double kin = g.ix2 + g.iy2 + g.iz2;  // buildHamiltonianDiagonal :496-500 (1/dx^2 + 1/dy^2 + 1/dz^2)
     const int eb = std::max(1, std::min((int)((g.N + 255) / 256), ctx->num_sms * 2));
 
-    // ---- start block: given vectors or the reference's seeds --------------------------
-    if (init) {
+    // ---- start block: a given start basis, given vectors or the reference's seeds -------
+    int k0 = nb;
+    if (start && nstart > 0) {
+        // a start basis of any width (e.g. atomic orbitals): the first Rayleigh-Ritz step picks
+        // the lowest nb combinations
+        k0 = std::min(nstart, kmax - 1);
+        DFT_CUDA(cudaMemcpy2DAsync(Vb, vecb, start, vecb, sizeof(double) * (size_t)g.N, k0, cudaMemcpyDeviceToDevice,
+                                   ctx->stream));
+        if (k0 > std::max(nb, kr)) W = (double*)ws_get(ctx, WS_DAV5, vecb * k0);
+    } else if (init) {
         DFT_CUDA(cudaMemcpy2DAsync(Vb, vecb, psi, vecb, sizeof(double) * (size_t)g.N, nb, cudaMemcpyDeviceToDevice,
                                    ctx->stream));
     } else {
@@ -481,7 +490,7 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
     }
-    int k = orthonormalise(ctx, g, Vb, 0, Vb, nb, ld, W);
+    int k = orthonormalise(ctx, g, Vb, 0, Vb, k0, ld, W);
     int seed = nb;
     while (k < nb) {  // rank-deficient start: top up with further seeds
         const int need = nb - k;

@@ -462,6 +462,7 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
     gram_tc_reduce_kernel<<<rb, 256, 0, ctx->stream>>>((int)nch, (int)nel, partial, g.dV, res);
     DFT_LAUNCH_CHECK();
     count_launch(ctx, 2);
+    ctx->tc_launches += 1;
     double* h = pinned(ctx, nel + 1);
     DFT_CUDA(cudaMemcpyAsync(h, res, sizeof(double) * nel, cudaMemcpyDeviceToHost, ctx->stream));
     DFT_CUDA(cudaMemcpyAsync(h + nel, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -515,6 +516,7 @@ void rotate_tc(dft_context* ctx, const Grid& g, const double* V, long long ldv, 
     }
     DFT_LAUNCH_CHECK();
     count_launch(ctx);
+    ctx->tc_launches += 1;
     int* h = (int*)pinned(ctx, 1);
     DFT_CUDA(cudaMemcpyAsync(h, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     sync(ctx);  // also keeps Y alive until its copy has run

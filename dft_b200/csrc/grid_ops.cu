@@ -157,39 +157,63 @@ namespace {
 
 constexpr int HB_X = 32, HB_Y = 8;
 
-// One thread per (i,j) column of one band, marching k over a z-chunk.
+// One thread per (i,j) column of NB bands, marching k over a z-chunk: V is read once per point
+// for all NB bands and the NB bands' loads are independent, so more of them are in flight.
 // reference KohnShamHamiltonianMolecule.cpp:59-177: lap = k0*c (+ neighbours in the order
-// x-, x+, y-, y+, z-, z+), H psi = -0.5*lap + V*c; absent neighbours are skipped.
+// x-, x+, y-, y+, z-, z+), H psi = -0.5*lap + V*c; absent neighbours are skipped.  The
+// operation order per band is the reference's, so every band is bit-identical for any NB.
+template <int NB>
 __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* __restrict__ V,
                                                          const double* __restrict__ psi, double* __restrict__ out,
-                                                         long long ld, int zchunk, int nzc, double k0) {
+                                                         long long ld, int nbands, int zchunk, int nzc, double k0) {
     const int i = blockIdx.x * HB_X + threadIdx.x;
     const int j = blockIdx.y * HB_Y + threadIdx.y;
-    const int band = blockIdx.z / nzc;
-    const int kc = blockIdx.z - band * nzc;
+    const int group = blockIdx.z / nzc;
+    const int kc = blockIdx.z - group * nzc;
     if (i >= g.nx || j >= g.ny) return;
-    const double* __restrict__ p = psi + (long long)band * ld;
-    double* __restrict__ o = out + (long long)band * ld;
+    const int b0 = group * NB;
+    const int nb = min(NB, nbands - b0);
+    const double* __restrict__ p = psi + (long long)b0 * ld;
+    double* __restrict__ o = out + (long long)b0 * ld;
     const long long sxy = (long long)g.nx * g.ny;
     const int kb = kc * zchunk;
     const int ke = min(g.nz, kb + zchunk);
     long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
-    double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
-    double cur = __ldg(p + idx);
+    double below[NB], cur[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        below[b] = (b < nb && kb > 0) ? __ldg(p + b * ld + idx - sxy) : 0.0;
+        cur[b] = b < nb ? __ldg(p + b * ld + idx) : 0.0;
+    }
     const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
     for (int k = kb; k < ke; ++k, idx += sxy) {
         const bool zr = k + 1 < g.nz;
-        const double above = zr ? __ldg(p + idx + sxy) : 0.0;
-        double lap = __dmul_rn(k0, cur);
-        if (xl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - 1), g.ix2));
-        if (xr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + 1), g.ix2));
-        if (yl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - g.nx), g.iy2));
-        if (yr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + g.nx), g.iy2));
-        if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below, g.iz2));
-        if (zr) lap = __dadd_rn(lap, __dmul_rn(above, g.iz2));
-        o[idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(__ldg(V + idx), cur));
-        below = cur;
-        cur = above;
+        const double v = __ldg(V + idx);
+        double above[NB], xm[NB], xp[NB], ym[NB], yp[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const double* q = p + b * ld + idx;
+            const bool on = b < nb;
+            above[b] = (on && zr) ? __ldg(q + sxy) : 0.0;
+            xm[b] = (on && xl) ? __ldg(q - 1) : 0.0;
+            xp[b] = (on && xr) ? __ldg(q + 1) : 0.0;
+            ym[b] = (on && yl) ? __ldg(q - g.nx) : 0.0;
+            yp[b] = (on && yr) ? __ldg(q + g.nx) : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            if (b >= nb) break;
+            double lap = __dmul_rn(k0, cur[b]);
+            if (xl) lap = __dadd_rn(lap, __dmul_rn(xm[b], g.ix2));
+            if (xr) lap = __dadd_rn(lap, __dmul_rn(xp[b], g.ix2));
+            if (yl) lap = __dadd_rn(lap, __dmul_rn(ym[b], g.iy2));
+            if (yr) lap = __dadd_rn(lap, __dmul_rn(yp[b], g.iy2));
+            if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below[b], g.iz2));
+            if (zr) lap = __dadd_rn(lap, __dmul_rn(above[b], g.iz2));
+            o[b * ld + idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(v, cur[b]));
+            below[b] = cur[b];
+            cur[b] = above[b];
+        }
     }
 }
 
@@ -209,15 +233,25 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
     const double k0 = -2.0 * (g.ix2 + g.iy2 + g.iz2);
     dim3 block(HB_X, HB_Y);
     const int bx = (g.nx + HB_X - 1) / HB_X, by = (g.ny + HB_Y - 1) / HB_Y;
-    const int zc = pick_zchunk(g, (long long)bx * by, nbands, ctx->num_sms);
+    // bands per thread: the "hpsi_bands_per_thread" tuning key, else 2 for blocks of 2 or more
+    int nbt = ctx->hpsi_bands_per_thread > 0 ? ctx->hpsi_bands_per_thread : (nbands >= 2 ? 2 : 1);
+    nbt = std::min(nbt, std::max(1, nbands));
+    nbt = nbt >= 4 ? 4 : nbt >= 2 ? 2 : 1;
+    const int groups = (nbands + nbt - 1) / nbt;
+    const int zc = pick_zchunk(g, (long long)bx * by, groups, ctx->num_sms);
     const int nzc = (g.nz + zc - 1) / zc;
     // gridDim.z limit is 65535: split the band block if needed
-    const int max_bands = std::max(1, 65535 / nzc);
-    for (int b0 = 0; b0 < nbands; b0 += max_bands) {
-        const int nb = std::min(max_bands, nbands - b0);
-        dim3 grid(bx, by, nb * nzc);
-        hpsi_kernel<<<grid, block, 0, ctx->stream>>>(g, V, psi + (long long)b0 * ld, hpsi + (long long)b0 * ld, ld, zc,
-                                                     nzc, k0);
+    const int max_groups = std::max(1, 65535 / nzc);
+    for (int g0 = 0; g0 < groups; g0 += max_groups) {
+        const int ng = std::min(max_groups, groups - g0);
+        const int b0 = g0 * nbt;
+        const int nb = std::min(nbands - b0, ng * nbt);
+        dim3 grid(bx, by, ng * nzc);
+        const double* pi = psi + (long long)b0 * ld;
+        double* po = hpsi + (long long)b0 * ld;
+        if (nbt == 4) hpsi_kernel<4><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+        else if (nbt == 2) hpsi_kernel<2><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+        else hpsi_kernel<1><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
     }
@@ -936,9 +970,14 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
 // compute step, where a cudaMalloc/cudaFree would also synchronise the device.  For them
 // hartree_noalloc runs the same kernels on a fixed scratch array compiled into the library.
 //
-// Limit: grids of at most NOALLOC_MAX_POINTS points (128^3).  Every GPU that loads the
-// library holds the array (16 MiB + 128 B) until the process exits.  All calls share it:
-// calls that overlap on the GPU (several streams or contexts on one device) race on it.
+// Limit: grids of at most NOALLOC_MAX_POINTS points (128^3).  Every GPU on which a context
+// is created holds the array (16 MiB + 128 B) until the process exits: dft_context_create
+// looks up its address, which also makes CUDA load this file's module (and the array) when
+// modules load lazily, so the first allocation-free call does not load it in the middle of
+// the caller's compute step.  All calls share the array: calls that overlap on the GPU
+// (several streams or contexts on one device) race on it.  Each call runs one Jacobi sweep
+// per launch (jacobi_sweep_kernel), whatever jacobi_sweeps_per_launch says: the cluster and
+// persistent variants take further workspace.
 namespace {
 
 constexpr long long NOALLOC_MAX_POINTS = 128LL * 128 * 128;
@@ -947,6 +986,8 @@ constexpr int NOALLOC_CTRL_DOUBLES = 16;  // JacobiCtrl and the boundary charge 
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_MAX_POINTS + NOALLOC_CTRL_DOUBLES];
 
 static_assert(sizeof(JacobiCtrl) + sizeof(double) <= NOALLOC_CTRL_DOUBLES * sizeof(double), "control words");
+
+}  // namespace
 
 // Device address of g_noalloc_scratch, looked up once per device with that device current.
 double* noalloc_scratch(int device) {
@@ -964,8 +1005,6 @@ double* noalloc_scratch(int device) {
     return addr[device];
 }
 
-}  // namespace
-
 JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol,
                              long max_sweeps) {
     if (g.N > NOALLOC_MAX_POINTS)
@@ -978,11 +1017,8 @@ JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho,
     double* buf1 = scratch;
     JacobiCtrl* ctrl = (JacobiCtrl*)(scratch + NOALLOC_MAX_POINTS);
     double* qslot = scratch + NOALLOC_MAX_POINTS + NOALLOC_CTRL_DOUBLES - 1;
-    const bool exact_faces = (g.xmin + (double)(g.nx - 1) * g.dx == g.xmax) &&
-                             (g.ymin + (double)(g.ny - 1) * g.dy == g.ymax) &&
-                             (g.zmin + (double)(g.nz - 1) * g.dz == g.zmax);
     double Q = 0.0;
-    if (!exact_faces) {
+    if (!faces_exact(g)) {
         total_charge_seq_kernel<<<1, 32, 0, ctx->stream>>>(g.N, rho, g.dV, qslot);
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
@@ -1404,7 +1440,58 @@ __global__ void sub_kernel(long long n, const double* __restrict__ a, const doub
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
         out[p] = a[p] - b[p];
 }
+// out = sum_i c_i a_i (no clamp)
+__global__ void combine_kernel(long long n, LinComb L, double* __restrict__ out) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int i = 0; i < L.m; ++i) s += L.c[i] * L.a[i][p];
+        out[p] = s;
+    }
+}
+// out = max(0, a + beta (r - f x)); out may alias a
+__global__ void kerker_update_kernel(long long n, const double* a, const double* __restrict__ r,
+                                     const double* __restrict__ x, double f, double beta, double* out) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double v = a[p] + beta * (r[p] - f * x[p]);
+        out[p] = v > 0.0 ? v : 0.0;
+    }
+}
+__global__ void add2_plain_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
+                                  double* __restrict__ o) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        o[p] = a[p] + b[p];
+}
 }  // namespace
+
+void combine(dft_context* ctx, long long n, int m, const double* const* a, const double* c, double* out) {
+    if (m < 1 || m > 16) fail(DFT_INVALID_ARGUMENT, "combination of %d entries", m);
+    LinComb L{};
+    L.m = m;
+    for (int i = 0; i < m; ++i) {
+        L.a[i] = a[i];
+        L.c[i] = c[i];
+    }
+    combine_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, L, out);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
+void kerker_update(dft_context* ctx, const Grid& g, int ns, double* const* a, const double* const* r, double* rtot,
+                   double* x, double q2, double beta) {
+    if (ns == 2) {
+        add2_plain_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g.N, r[0], r[1], rtot);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+    }
+    // closed shell: the total residual is 2 r, so (q^2/2) V(2 r) = q^2 V(r)
+    screened_poisson_vcycle(ctx, g, ns == 2 ? rtot : r[0], 1, q2, x, g.N);
+    const double f = ns == 2 ? 0.5 * q2 : q2;
+    for (int sp = 0; sp < ns; ++sp) {
+        kerker_update_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g.N, a[sp], r[sp], x, f, beta, a[sp]);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+    }
+}
 
 void pulay_combine(dft_context* ctx, long long n, int m, const double* const* a, const double* const* r,
                    const double* c, double beta, double* out) {

@@ -4,6 +4,9 @@
 // host scalar, in which case it synchronises.
 #pragma once
 
+#include <array>
+#include <vector>
+
 #include "common.cuh"
 
 namespace dftb {
@@ -24,6 +27,8 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
 // true when every face's last node lands exactly on the bound (the reference's boundary is then zero)
 bool faces_exact(const Grid& g);
 // The same solve on the library's fixed scratch array: no device allocation (grid_ops.cu).
+// noalloc_scratch: the array's device address on `device` (must be current), looked up once.
+double* noalloc_scratch(int device);
 JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol,
                              long max_sweeps);
 
@@ -37,6 +42,14 @@ void mix(dft_context* ctx, long long n, double* d, const double* o, double m);
 // out = max(0, sum_i c_i (a_i + beta r_i)) over m <= 16 history entries (Pulay mixing)
 void pulay_combine(dft_context* ctx, long long n, int m, const double* const* a, const double* const* r,
                    const double* c, double beta, double* out);
+// out = sum_i c_i a_i over m <= 16 fields (no clamp)
+void combine(dft_context* ctx, long long n, int m, const double* const* a, const double* c, double* out);
+// Kerker-screened density step for ns spin fields (ns = 1: closed shell, the field is n_alpha):
+// x = (-lap_h + q2)^{-1} (r_0 + r_1) by one multigrid cycle (rtot: scratch for the sum), then
+// a_s = max(0, a_s + beta (r_s - (q2/2) x)), i.e. the total-charge residual is multiplied by
+// -lap/(-lap + q2) (the real-space Kerker factor G^2/(G^2 + q0^2)) and the spin residual is kept.
+void kerker_update(dft_context* ctx, const Grid& g, int ns, double* const* a, const double* const* r, double* rtot,
+                   double* x, double q2, double beta);
 // out = a - b
 void sub(dft_context* ctx, long long n, const double* a, const double* b, double* out);
 
@@ -84,6 +97,11 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
 void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb,
                             const double* theta_dev, double* T, long long ld);
 
+// One multigrid V(2,2) cycle from zero for (-lap_h + q2) x_a = src_a, x = 0 outside the box, for
+// nb fields of ld points (precond_mg.cu): x ~ (-lap_h + q2)^{-1} src, a fixed linear map.
+void screened_poisson_vcycle(dft_context* ctx, const Grid& g, const double* src, int nb, double q2, double* x,
+                             long long ld);
+
 struct EigOpts {
     double tol = 1e-7;
     int max_iterations = 2000;
@@ -93,8 +111,11 @@ struct EigOpts {
     int mixed_precision = 0;       // 1 = tensor-core (TF32 hi+lo) Gram products while residuals are large
     double mixed_switch = 1e-3;    // occupied residual below which the solver switches to FP64
 };
+// start/nstart: an optional start basis of nstart vectors (leading dimension ld) that replaces
+// psi's contents and the seeds; the first Rayleigh-Ritz step takes the lowest nbands from it.
 int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, int nbands, double* psi,
-                   long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o);
+                   long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o,
+                   const double* start = nullptr, int nstart = 0);
 
 // Molecular SCF (scf.cu).
 void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z, const double* xyz, int charge,
@@ -103,5 +124,22 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
 // Radial atoms, one persistent launch (radial.cu).
 void solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, long points, double rmax,
                  dft_atom_result* results);
+// The same batch for nz atoms with one functional, keeping the converged atoms on the device:
+// dens (nz x points) the total density n(r), orbs (nz x RADIAL_MAX_SHELLS x points) the radial
+// functions u_nl(r) = r R_nl(r) of the alpha shells, listed per atom as (n, l) in shells.
+constexpr int RADIAL_MAX_SHELLS = 8;
+void radial_atom_tables(dft_context* ctx, int nz, const int* Z, int kind, long points, double rmax, double* dens,
+                        double* orbs, std::vector<std::vector<std::array<int, 2>>>& shells);
+
+// Number of start vectors atomic_start writes: 2l + 1 per occupied (n, l) shell of every atom.
+int atomic_orbital_count(int nnuc, const int* Z);
+// Superposition start of the molecular SCF (atomic_start.cu): the radial atoms of every nucleus'
+// element (functional `kind`, 2000 points, r_max 30 bohr) are solved in one batch; their total
+// densities, summed at every node and scaled to ne_a + ne_b electrons, split in the ratio
+// ne_a : ne_b, give da and db.  When basis != nullptr it also receives one start vector per
+// occupied atomic orbital (u_nl(r)/r times 1, x/r, y/r or z/r), at most max_basis of them,
+// band-major with leading dimension ld; returns the number written.
+int atomic_start(dft_context* ctx, const Grid& g, int nnuc, const int* Z, const double* xyz, int kind, int ne_a,
+                 int ne_b, double* da, double* db, double* basis, long long ld, int max_basis);
 
 }  // namespace dftb

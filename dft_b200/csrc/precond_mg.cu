@@ -139,14 +139,19 @@ __global__ void __launch_bounds__(1024) pc_coarsest_kernel(Grid g, long long ld,
     for (int p = threadIdx.x; p < n; p += blockDim.x) x[p] = 0.0;
     __syncthreads();
     const double d = 2.0 * (g.ix2 + g.iy2 + g.iz2) + shift[a];
-    for (int s = 0; s < sweeps; ++s) {
-        const double* cur = (s & 1) ? y : x;
-        double* nxt = (s & 1) ? x : y;
+    for (int it = 0; it < sweeps; ++it) {
+        const double* cur = (it & 1) ? y : x;
+        double* nxt = (it & 1) ? x : y;
         for (int p = threadIdx.x; p < n; p += blockDim.x) nxt[p] = (nb_sum_open(g, cur, p) + s * src[p]) / d;
         __syncthreads();
     }
     const double* res = (sweeps & 1) ? y : x;
     for (int p = threadIdx.x; p < n; p += blockDim.x) e[p] = res[p];
+}
+
+// shift[a] = c for every field (the screened Poisson equation of the Kerker mixer)
+__global__ void pc_fill_kernel(int nb, double c, double* __restrict__ shift) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nb; a += gridDim.x * blockDim.x) shift[a] = c;
 }
 
 // c_a = 2 max(-theta[src[a]], 1 Ha): the shift of each correction band, from the Ritz values
@@ -159,7 +164,7 @@ __global__ void pc_shift_kernel(int nb, const double* __restrict__ theta, const 
 __global__ void pc_gather_kernel(long long n, long long ld, const double* __restrict__ R, const int* __restrict__ srcmap,
                                  double* __restrict__ out) {
     const int a = blockIdx.y;
-    const double* r = R + (long long)srcmap[a] * ld;
+    const double* r = R + (long long)(srcmap ? srcmap[a] : a) * ld;
     double* o = out + (long long)a * ld;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
         o[p] = r[p];
@@ -220,11 +225,11 @@ void pc_vcycle(dft_context* ctx, std::vector<PCLevel>& L, size_t i, double s, co
     DFT_LAUNCH_CHECK();
 }
 
-}  // namespace
-
-void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb,
-                            const double* theta_dev, double* T, long long ld) {
-    if (nb <= 0) return;
+// One V(2,2) cycle from zero, all nb fields together, for (den + shift_a) t - sum_nb w t_nb =
+// s * R_{src[a]} on g (src_dev == nullptr: field a itself), into T.  shift_dev must not live in
+// the WS_PG2 workspace.
+void vcycle_batch(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb, const double* shift,
+                  double s, double* T, long long ld) {
     std::vector<PCLevel> L;
     PCLevel f{};
     f.g = g;
@@ -283,16 +288,35 @@ void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, co
                                       (int)(sizeof(double) * 2 * PC_COARSEST_MAX)));
         attr = true;
     }
-    // shifts c_a = 2 sigma_a, computed on the device (no host round trip)
-    double* shift = (double*)ws_get(ctx, WS_PG3, sizeof(double) * (size_t)nb + 64);
-    pc_shift_kernel<<<(nb + 127) / 128, 128, 0, ctx->stream>>>(nb, theta_dev, src_dev, shift);
     pc_gather_kernel<<<pc_grid(ctx, g.N, nb), 256, 0, ctx->stream>>>(g.N, ld, R, src_dev, L[0].src);
     count_launch(ctx);
-    pc_vcycle(ctx, L, 0, 2.0, shift, nb);
+    pc_vcycle(ctx, L, 0, s, shift, nb);
     if (L[0].v != T)
         DFT_CUDA(cudaMemcpy2DAsync(T, sizeof(double) * ld, L[0].v, sizeof(double) * ld, sizeof(double) * g.N, nb,
                                    cudaMemcpyDeviceToDevice, ctx->stream));
     DFT_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb,
+                            const double* theta_dev, double* T, long long ld) {
+    if (nb <= 0) return;
+    // shifts c_a = 2 sigma_a, computed on the device (no host round trip)
+    double* shift = (double*)ws_get(ctx, WS_PG3, sizeof(double) * (size_t)nb + 64);
+    pc_shift_kernel<<<(nb + 127) / 128, 128, 0, ctx->stream>>>(nb, theta_dev, src_dev, shift);
+    count_launch(ctx);
+    vcycle_batch(ctx, g, R, src_dev, nb, shift, 2.0, T, ld);
+}
+
+void screened_poisson_vcycle(dft_context* ctx, const Grid& g, const double* src, int nb, double q2, double* x,
+                             long long ld) {
+    if (nb <= 0) return;
+    if (!(q2 > 0.0) || !std::isfinite(q2)) fail(DFT_INVALID_ARGUMENT, "screening q^2 must be > 0");
+    double* shift = (double*)ws_get(ctx, WS_PG3, sizeof(double) * (size_t)nb + 64);
+    pc_fill_kernel<<<(nb + 127) / 128, 128, 0, ctx->stream>>>(nb, q2, shift);
+    count_launch(ctx);
+    vcycle_batch(ctx, g, src, nullptr, nb, shift, 1.0, x, ld);
 }
 
 }  // namespace dftb

@@ -514,12 +514,16 @@ void configuration(int Z, std::vector<std::array<int, 4>>& rows) {
 
 }  // namespace
 
-void solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, long points, double rmax,
-                 dft_atom_result* results) {
+namespace {
+
+// Builds the run specs, launches the batch and leaves every run's arrays in the WS_RADIAL
+// workspace (returned; per_run doubles per run, layout A_* then MAXORB x O_*).
+double* run_batch(dft_context* ctx, int nruns, const int* Z, const int* kinds, long points, double rmax,
+                  dft_atom_result* results, std::vector<RunSpec>& specs, long long& per_run) {
     if (points < 2) fail(DFT_INVALID_ARGUMENT, "La malla radial debe contener al menos dos puntos.");
     if (points > 12000) fail(DFT_INVALID_ARGUMENT, "at most 12000 radial points per run");
     if (!(rmax > 0.0)) fail(DFT_INVALID_ARGUMENT, "RMAX debe ser mayor que cero.");
-    std::vector<RunSpec> specs(nruns);
+    specs.assign(nruns, RunSpec{});
     for (int rr = 0; rr < nruns; ++rr) {
         if (Z[rr] < 1 || Z[rr] > 30) fail(DFT_INVALID_ARGUMENT, "Configuracion atomica no disponible para Z = %d", Z[rr]);
         if (kinds[rr] != 0 && kinds[rr] != 1) fail(DFT_INVALID_ARGUMENT, "unknown functional kind %d", kinds[rr]);
@@ -545,7 +549,7 @@ void solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, lo
         }
         s.norb = q;
     }
-    const long long per_run = (long long)(A_COUNT + MAXORB * O_COUNT) * points;
+    per_run = (long long)(A_COUNT + MAXORB * O_COUNT) * points;
     double* ws = (double*)ws_get(ctx, WS_RADIAL, sizeof(double) * (size_t)per_run * nruns);
     const size_t spec_bytes = ((sizeof(RunSpec) * nruns + 255) / 256) * 256;  // keep the results 256-B aligned
     char* dbuf = (char*)ws_get(ctx, WS_TMP2, spec_bytes + sizeof(dft_atom_result) * nruns);
@@ -561,6 +565,54 @@ void solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, lo
     count_launch(ctx);
     DFT_CUDA(cudaMemcpyAsync(results, dres, sizeof(dft_atom_result) * nruns, cudaMemcpyDeviceToHost, ctx->stream));
     sync(ctx);
+    return ws;
+}
+
+}  // namespace
+
+void solve_atoms(dft_context* ctx, int nruns, const int* Z, const int* kinds, long points, double rmax,
+                 dft_atom_result* results) {
+    std::vector<RunSpec> specs;
+    long long per_run = 0;
+    run_batch(ctx, nruns, Z, kinds, points, rmax, results, specs, per_run);
+}
+
+int atomic_orbital_count(int nnuc, const int* Z) {
+    int n = 0;
+    std::vector<std::array<int, 4>> rows;
+    for (int a = 0; a < nnuc; ++a) {
+        if (Z[a] < 1 || Z[a] > 30) continue;
+        configuration(Z[a], rows);
+        for (auto& row : rows)
+            if (row[2] > 0 && row[1] <= 2) n += 2 * row[1] + 1;
+    }
+    return n;
+}
+
+void radial_atom_tables(dft_context* ctx, int nz, const int* Z, int kind, long points, double rmax, double* dens,
+                        double* orbs, std::vector<std::vector<std::array<int, 2>>>& shells) {
+    std::vector<int> kinds(nz, kind);
+    std::vector<dft_atom_result> res(nz);
+    std::vector<RunSpec> specs;
+    long long per_run = 0;
+    const double* ws = run_batch(ctx, nz, Z, kinds.data(), points, rmax, res.data(), specs, per_run);
+    shells.assign(nz, {});
+    for (int rr = 0; rr < nz; ++rr) {
+        if (res[rr].status != DFT_OK)
+            fail((dft_status_t)res[rr].status, "radial atom Z = %d failed (status %d)", Z[rr], res[rr].status);
+        const double* base = ws + (long long)rr * per_run;
+        DFT_CUDA(cudaMemcpyAsync(dens + (long long)rr * points, base + (long long)A_OD * points,
+                                 sizeof(double) * points, cudaMemcpyDeviceToDevice, ctx->stream));
+        const RunSpec& sp = specs[rr];
+        for (int q = 0; q < sp.norb; ++q) {
+            if (sp.spin[q] != 0) continue;  // the alpha shells: every occupied (n, l) of the atom
+            const int k = (int)shells[rr].size();
+            DFT_CUDA(cudaMemcpyAsync(orbs + ((long long)rr * RADIAL_MAX_SHELLS + k) * points,
+                                     base + (long long)(A_COUNT + q * O_COUNT + O_U) * points,
+                                     sizeof(double) * points, cudaMemcpyDeviceToDevice, ctx->stream));
+            shells[rr].push_back({sp.n[q], sp.l[q]});
+        }
+    }
 }
 
 }  // namespace dftb

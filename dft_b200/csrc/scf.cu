@@ -133,15 +133,33 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             enn += (double)Z[a] * (double)Z[c] / std::sqrt(d2);
         }
 
-    // ---- initial densities from orbitals in the bare V_ext (MolecularSCFHelpers.cpp:515-579) --
-    int it_a = solve_orbitals(ctx, g, vext.p, na, bands_a, psia.p, ld, false, eiga.data(), resa.data(), eo);
-    (void)it_a;
-    spin_density(ctx, N, psia.p, bands_a, ld, occa.data(), da.p);
-    if (closed) {
-        DFT_CUDA(cudaMemcpyAsync(db.p, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+    // ---- initial densities ------------------------------------------------------------
+    if (o.initial_density != 0 && o.initial_density != 1)
+        fail(DFT_INVALID_ARGUMENT, "unknown initial_density %d", o.initial_density);
+    // superposed radial atoms (option): densities now, atomic orbitals as the first eigensolve's
+    // start basis (both spins), freed after the first iteration
+    const bool atoms_start = o.initial_density == 1;
+    int nao = 0;
+    DevBuf aobuf;
+    if (atoms_start) {
+        const long long kcap = std::max<long long>(eo.max_subspace * (long long)std::max(bands_a, bands_b),
+                                                   std::max(bands_a, bands_b) + 16LL) - 1;
+        const int want = (int)std::min<long long>(atomic_orbital_count(nnuc, Z), kcap);
+        if (want > 0) {
+            DevBuf tmp((size_t)want * ld);
+            std::swap(aobuf.p, tmp.p);
+        }
+        nao = atomic_start(ctx, g, nnuc, Z, xyz, kind, na, nb, da.p, db.p, aobuf.p, ld, want);
     } else {
-        solve_orbitals(ctx, g, vext.p, nb, bands_b, psib.p, ld, false, eigb.data(), resb.data(), eo);
-        spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), db.p);
+        // orbitals in the bare V_ext (MolecularSCFHelpers.cpp:515-579)
+        solve_orbitals(ctx, g, vext.p, na, bands_a, psia.p, ld, false, eiga.data(), resa.data(), eo);
+        spin_density(ctx, N, psia.p, bands_a, ld, occa.data(), da.p);
+        if (closed) {
+            DFT_CUDA(cudaMemcpyAsync(db.p, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+        } else {
+            solve_orbitals(ctx, g, vext.p, nb, bands_b, psib.p, ld, false, eigb.data(), resb.data(), eo);
+            spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), db.p);
+        }
     }
 
     // ---- Fermi-Dirac occupations (option; the reference fills the lowest levels) --------
@@ -186,6 +204,11 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     const double pbeta = o.pulay_beta > 0.0 ? o.pulay_beta : 0.2;
     if (o.mixer != 0 && o.mixer != 1) fail(DFT_INVALID_ARGUMENT, "unknown mixer %d", o.mixer);
     DevBuf phist(o.mixer == 1 ? (size_t)2 * pdepth * ns * N : 0);
+    // Kerker screening of the total-charge residual (option; 0 = off, the reference's mixer)
+    const double kq0 = o.kerker_q0;
+    if (kq0 < 0.0 || !std::isfinite(kq0)) fail(DFT_INVALID_ARGUMENT, "kerker_q0 must be >= 0");
+    const double kq2 = kq0 * kq0;
+    DevBuf kbuf(kq0 > 0.0 ? (size_t)(ns + 2) * N : 0);
     std::vector<double> Bp((size_t)pdepth * pdepth, 0.0);
     int pcount = 0, phead = 0;
     auto pulay_mix = [&]() {
@@ -249,6 +272,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             std::fill(cf.begin(), cf.end(), 0.0);
             cf[slot] = 1.0;
         }
+        double* dst[2] = {da.p, db.p};
         for (int sp = 0; sp < ns; ++sp) {
             const double* a[16];
             const double* r[16];
@@ -256,7 +280,17 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
                 a[i] = phist.p + (size_t)i * 2 * ns * N + (size_t)sp * N;
                 r[i] = a[i] + (size_t)ns * N;
             }
-            pulay_combine(ctx, N, m, a, r, cf.data(), pbeta, sp == 0 ? da.p : db.p);
+            if (kq0 > 0.0) {
+                // n_in = sum c_i n_in,i + beta K(sum c_i r_i): the optimal residual screened
+                combine(ctx, N, m, a, cf.data(), dst[sp]);
+                combine(ctx, N, m, r, cf.data(), kbuf.p + (size_t)sp * N);
+            } else {
+                pulay_combine(ctx, N, m, a, r, cf.data(), pbeta, dst[sp]);
+            }
+        }
+        if (kq0 > 0.0) {
+            const double* rr[2] = {kbuf.p, kbuf.p + N};
+            kerker_update(ctx, g, ns, dst, rr, kbuf.p + (size_t)ns * N, kbuf.p + (size_t)(ns + 1) * N, kq2, pbeta);
         }
         if (closed) DFT_CUDA(cudaMemcpyAsync(db.p, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
     };
@@ -294,11 +328,20 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         t0 = Clock::now();
         EigOpts ek = eo;
         if (o.adaptive_eig_tol && std::isfinite(prevD)) ek.tol = std::max(eo.tol, std::min(1e-3, 0.1 * prevD));
-        rec.eig_iterations_alpha =
-            solve_orbitals(ctx, g, va.p, nconv_a, bands_a, psia.p, ld, true, eiga.data(), resa.data(), ek);
+        // the first iteration of the atomic start begins from the atomic orbitals (or, with
+        // none, from the reference's seeds); later ones from the previous orbitals
+        const bool first_atoms = atoms_start && it == 1;
+        const double* sb = first_atoms && nao > 0 ? aobuf.p : nullptr;
+        rec.eig_iterations_alpha = solve_orbitals(ctx, g, va.p, nconv_a, bands_a, psia.p, ld, !first_atoms,
+                                                  eiga.data(), resa.data(), ek, sb, nao);
         if (!closed)
-            rec.eig_iterations_beta =
-                solve_orbitals(ctx, g, vb.p, nconv_b, bands_b, psib.p, ld, true, eigb.data(), resb.data(), ek);
+            rec.eig_iterations_beta = solve_orbitals(ctx, g, vb.p, nconv_b, bands_b, psib.p, ld, !first_atoms,
+                                                     eigb.data(), resb.data(), ek, sb, nao);
+        if (first_atoms && aobuf.p) {
+            sync(ctx);
+            cudaFree(aobuf.p);
+            aobuf.p = nullptr;
+        }
         if (kt > 0.0) {
             nconv_a = fermi(eiga, na, occa);
             if (closed) {
@@ -366,6 +409,21 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
                     "[scf] it=%3d E=%.12f dE=%.3e dRho=%.3e KS=%.3e mix=%.3f sweeps=%ld/%ld eig_it=%d/%d  %.1f ms\n", it,
                     E[5], dE, effd, resid, imix, jin.sweeps, jout.sweeps, rec.eig_iterations_alpha,
                     rec.eig_iterations_beta, rec.ms_total);
+        if (o.verbose > 1) {
+            // per spin: the lowest levels, the levels around the highest occupied one, and the
+            // spin density change, to tell level crossings at the Fermi level from sloshing
+            auto levels = [&](const char* tag, const std::vector<double>& e, int nocc, double dr) {
+                const int m = (int)e.size();
+                fprintf(stderr, "[scf]   %s dRho=%.3e low:", tag, dr);
+                for (int i = 0; i < std::min(3, m); ++i) fprintf(stderr, " %.5f", e[i]);
+                fprintf(stderr, " | homo-3..:");
+                for (int i = std::max(0, nocc - 4); i < std::min(m, nocc + 4); ++i)
+                    fprintf(stderr, "%s%.5f", i == nocc ? " || " : " ", e[i]);
+                fprintf(stderr, "\n");
+            };
+            levels("a", eiga, na, density_difference(ctx, g, da.p, oa.p));
+            if (!closed) levels("b", eigb, nb, density_difference(ctx, g, db.p, ob.p));
+        }
         if (converged) break;
         if (o.stop_abs_de > 0.0 && dE < o.stop_abs_de) break;
         // adaptive mixing with the pre-update factor applied (:447-484)
@@ -375,6 +433,15 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         }
         if (o.mixer == 1) {
             pulay_mix();
+        } else if (kq0 > 0.0) {
+            // n_in += mixing * K(n_out - n_in)
+            sub(ctx, N, oa.p, da.p, kbuf.p);
+            if (!closed) sub(ctx, N, ob.p, db.p, kbuf.p + N);
+            double* dst[2] = {da.p, db.p};
+            const double* rr[2] = {kbuf.p, kbuf.p + N};
+            kerker_update(ctx, g, ns, dst, rr, kbuf.p + (size_t)ns * N, kbuf.p + (size_t)(ns + 1) * N, kq2, imix);
+            if (closed)
+                DFT_CUDA(cudaMemcpyAsync(db.p, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
         } else {
             mix(ctx, N, da.p, oa.p, imix);
             mix(ctx, N, db.p, ob.p, imix);

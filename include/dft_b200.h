@@ -66,12 +66,17 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               identical for every value).
  *   "network_tensor_cores":     1 (default) = the Poisson-start network's 16- and 32-channel
  *                               convolutions on tcgen05, 0 = FP32 CUDA cores (results agree to
- *                               BF16 rounding, not bit for bit). */
+ *                               BF16 rounding, not bit for bit).
+ *   "hpsi_bands_per_thread":    0 = auto (default), 1, 2 or 4 bands marched together by each
+ *                               thread of the H psi kernel (results identical for every value). */
 dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long value);
 /* The cudaStream_t the context launches on, as an opaque handle (for event timing). */
 void* dft_context_stream(dft_context* ctx);
 /* Number of kernels this context has launched so far (diagnostics, bench accounting). */
 long long dft_context_launch_count(dft_context* ctx);
+/* Named counters of this context (diagnostics): "launches" (as above), "tensor_core_products"
+ * (tcgen05 Gram products and subspace rotations of the eigensolver); -1 for an unknown name. */
+long long dft_context_counter(dft_context* ctx, const char* name);
 dft_status_t dft_device_alloc(dft_context* ctx, size_t bytes, void** out);
 dft_status_t dft_device_free(dft_context* ctx, void* ptr);
 dft_status_t dft_copy_h2d(dft_context* ctx, void* dst, const void* src, size_t bytes);
@@ -101,12 +106,15 @@ dft_status_t dft_hartree_dev(dft_context* ctx, const dft_grid* g, const double* 
  * application's compute step, where cudaMalloc/cudaFree would also stall the device.
  * This entry point calls no cudaMalloc, cudaFree or other allocating routine; its scratch
  * (the second Jacobi iterate and the control words) is a fixed array compiled into the
- * library, so every GPU that loads the library holds 16 MiB + 128 B until the process
- * exits.  Limit: nx*ny*nz <= 2,097,152 points (128^3); larger grids are rejected with
- * DFT_INVALID_ARGUMENT.  The first call on each device looks up the array's device
- * address (once, with that device current); make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (several streams or
- * contexts on one device at once) race on it.  No counterpart in the reference. */
+ * library, so every GPU on which a context is created holds 16 MiB + 128 B until the
+ * process exits.  dft_context_create looks up the array's device address, which also
+ * makes CUDA load it where modules load lazily, so this entry point neither loads nor
+ * allocates anything.  Limit: nx*ny*nz <= 2,097,152 points (128^3); larger grids are
+ * rejected with DFT_INVALID_ARGUMENT.  Every call runs one Jacobi sweep per launch,
+ * whatever the "jacobi_sweeps_per_launch" tuning key says, so small grids take more
+ * launches than with dft_hartree_dev.  All calls share the array: calls that overlap on
+ * the GPU (several streams or contexts on one device at once) race on it.  No counterpart
+ * in the reference. */
 dft_status_t dft_hartree_noalloc_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
                                      long max_sweeps, long* sweeps_out, double* last_diff_out);
 
@@ -163,6 +171,12 @@ typedef struct {
 dft_status_t dft_rotate_dev(dft_context* ctx, const dft_grid* g, const double* V, long ldv, int k, const double* Y,
                             int m, double* X, long ldx, int precision);
 
+/* x ~ (-lap_h + q2)^{-1} src by one multigrid V(2,2) cycle from zero (7-point Laplacian,
+ * x = 0 outside the box; src, x: device, N doubles; q2 > 0).  The screening solve of the
+ * Kerker mixer (dft_scf_opts.kerker_q0), exposed for testing; no counterpart in the
+ * reference, whose mixer is linear (MolecularSCFHelpers.cpp:27-44). */
+dft_status_t dft_screened_poisson_dev(dft_context* ctx, const dft_grid* g, const double* src, double* x, double q2);
+
 /* dV * A^T B for band blocks A (ka x N, leading dimension lda) and B (kb x N), result in
  * C_host (ka x kb, row-major).  precision 0 = FP64, 1 = tensor cores (TF32 hi+lo split).
  * The block eigensolver's Gram product, exposed for testing; no counterpart in the reference
@@ -218,6 +232,13 @@ typedef struct {
     int adaptive_eig_tol;    /* 1: eigensolver tolerance max(eig.tol, min(1e-3, 0.1 * previous dRho)) */
     double smearing_kt;      /* > 0: Fermi-Dirac occupations at this temperature (Ha) over the extra
                                 bands instead of the reference's integer aufbau (0) */
+    double kerker_q0;        /* > 0: Kerker screening of the total-charge residual in either mixer,
+                                -lap/(-lap + q0^2) by one multigrid cycle (bohr^-1; 0 = off) */
+    int initial_density;     /* 0: orbitals of the bare nuclear potential, as the reference
+                                (buildInitialMolecularDensities, MolecularSCFHelpers.cpp:515-579);
+                                1: superposed radial atoms of the same functional (batched radial
+                                SCF, SelfConsistentField.cpp:539-786), scaled to the electron count,
+                                and their occupied atomic orbitals as the first eigensolve's start */
 } dft_scf_opts;
 
 /* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)

@@ -186,6 +186,17 @@ class _Lib:
                                          multiplicity, kind, iterations, _d(s)))
         return float(s[0]), float(s[1])
 
+    def scf_to_de(self, n, bounds, Z, xyz, multiplicity, kind, de_stop=1e-6, max_iterations=250):
+        """The reference's SCF loop to |dE| < de_stop: (seconds, init seconds, iterations,
+        energy, last |dE|).  Reference library only (ref_scf_to_de)."""
+        nn, ba = self.grid_args(n, bounds)
+        Z = _arr(Z, np.int32)
+        xyz = _arr(xyz)
+        out = np.zeros(5)
+        self.check(self.fn("scf_to_de")(nn.ctypes.data_as(_lp), _d(ba), len(Z), Z.ctypes.data_as(_ip), _d(xyz),
+                                        multiplicity, kind, C.c_double(de_stop), max_iterations, _d(out)))
+        return float(out[0]), float(out[1]), int(out[2]), float(out[3]), float(out[4])
+
     # ---- radial -------------------------------------------------------------
     def solve_atom(self, Z, kind, points=2000, rmax=30.0):
         e5 = np.zeros(5)

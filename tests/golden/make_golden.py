@@ -162,8 +162,10 @@ def ops():
     dump("ops_ref.json", fx)
 
 
-def readme(path="/root/reference/README.md"):
-    """The reference's published radial results (README.md:171-241, carbon :413-441), read as text."""
+def readme(path=None):
+    """The reference's published radial results (README.md:171-241, carbon :413-441), read as text
+    from the checkout named by DFT_REFERENCE_DIR (default: the reference mount of the build host)."""
+    path = path or os.path.join(os.environ.get("DFT_REFERENCE_DIR", "/root/reference"), "README.md")
     text = open(path, encoding="utf-16").read().splitlines()
     rows = []
     for line in text[170:241]:

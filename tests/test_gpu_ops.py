@@ -31,11 +31,19 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
+@pytest.fixture(params=[0, 1, 2, 4], ids=lambda t: f"bpt{t}")
+def hpsi_bands_per_thread(request, engine):
+    """Every H psi launch shape: auto, 1, 2 or 4 bands marched by each thread."""
+    engine.set_tuning("hpsi_bands_per_thread", request.param)
+    yield request.param
+    engine.set_tuning("hpsi_bands_per_thread", 0)
+
+
 @pytest.mark.parametrize("n,b", GRIDS)
-def test_hpsi_bit_exact(engine, port, n, b):
+def test_hpsi_bit_exact(engine, port, n, b, hpsi_bands_per_thread):
     rng = np.random.default_rng(11)
     N = int(np.prod(n))
-    nb_, ld = 3, N + 37  # padded leading dimension
+    nb_, ld = 5, N + 37  # padded leading dimension; 5 bands leave a partial group of 2 or 4
     V = rng.standard_normal(N)
     psi = np.zeros((nb_, ld))
     psi[:, :N] = rng.standard_normal((nb_, N))
@@ -46,7 +54,7 @@ def test_hpsi_bit_exact(engine, port, n, b):
         assert np.array_equal(H[k, :N], port.apply_hamiltonian(n, b, V, psi[k, :N])), k
 
 
-def test_hpsi_large_numpy_restatement(engine):
+def test_hpsi_large_numpy_restatement(engine, hpsi_bands_per_thread):
     """128^3 x 4 bands: bit-identical to a vectorised numpy restatement of the same stencil order."""
     n, b = (128, 128, 128), (-12.7, 12.7) * 3
     g = G(n, b)
