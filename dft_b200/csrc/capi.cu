@@ -137,6 +137,12 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
         } else if (k == "network_tensor_cores") {
             NEED(value == 0 || value == 1, "network_tensor_cores must be 0 or 1");
             ctx->net_tensor_cores = (int)value;
+        } else if (k == "grid_barrier_poll_limit") {
+            NEED(value >= 0, "grid_barrier_poll_limit must be >= 0 (0 = default)");
+            ctx->grid_barrier_poll_limit = value;
+        } else if (k == "radial_pivot_exponent") {
+            NEED(value >= -300 && value <= 300, "radial_pivot_exponent must be in [-300, 300]");
+            ctx->radial_pivot_exp = (int)value;
         } else if (k == "hpsi_bands_per_thread") {
             NEED(value == 0 || value == 1 || value == 2 || value == 4, "hpsi_bands_per_thread must be 0 (auto), 1, 2 or 4");
             ctx->hpsi_bands_per_thread = (int)value;

@@ -101,6 +101,8 @@ struct dft_context {
     int jacobi_sweeps_per_launch = 0;  // 0 = auto, 1 = one sweep per launch, 2/4/8 = temporal blocking
     int net_tensor_cores = 1;          // network convolutions on tcgen05 (1) or FP32 CUDA cores (0)
     int hpsi_bands_per_thread = 0;     // H psi bands per thread: 0 = auto, 1, 2 or 4
+    long long grid_barrier_poll_limit = 0;  // persistent Jacobi barrier polls before giving up (0 = 2^24)
+    int radial_pivot_exp = -14;        // radial inverse iteration: |pivot| < 10^exp is singular
     // named scratch buffers (reductions, Jacobi ping-pong, XC intermediates, Davidson)
     dftb::Workspace ws[32];
     double* host_pinned = nullptr;  // small pinned staging area for scalars

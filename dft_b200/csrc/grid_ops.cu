@@ -542,8 +542,9 @@ __global__ void __launch_bounds__(TB_R* TB_R, 1)
 // blocks stay resident (cooperative launch) and meet at a grid barrier after every sweep;
 // every block reads the same global max|dV| after the barrier, so all stop at the same sweep.
 // Loads of the iterates bypass L1 (__ldcg): other SMs rewrite them every sweep.
-// The barrier wait is bounded: a block that waits longer than ~2^24 polls sets ctrl->error and
-// leaves, and so do the others at their next barrier.
+// The barrier wait is bounded: a block that polls poll_limit times (2^24 unless the
+// "grid_barrier_poll_limit" tuning key says otherwise) without seeing the barrier open sets
+// ctrl->error and leaves, and so do the others at their next barrier; the host reports it.
 struct JacobiPCtrl {
     unsigned long long slot[3];  // per-sweep max |dV| (sweep s uses slot s % 3)
     unsigned int count;          // grid barrier arrivals
@@ -554,7 +555,7 @@ struct JacobiPCtrl {
     double last_diff;
 };
 
-__device__ __forceinline__ bool grid_barrier(JacobiPCtrl* c, unsigned int nblocks) {
+__device__ __forceinline__ bool grid_barrier(JacobiPCtrl* c, unsigned int nblocks, long long poll_limit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -568,7 +569,7 @@ __device__ __forceinline__ bool grid_barrier(JacobiPCtrl* c, unsigned int nblock
         } else {
             long long polls = 0;
             while (atomicAdd(&c->gen, 0u) == gen) {
-                if (++polls > (1LL << 24) || atomicAdd(&c->error, 0) != 0) {
+                if (++polls >= poll_limit || atomicAdd(&c->error, 0) != 0) {
                     atomicExch(&c->error, 1);
                     ok = 0;
                     break;
@@ -585,7 +586,7 @@ __device__ __forceinline__ bool grid_barrier(JacobiPCtrl* c, unsigned int nblock
 
 __global__ void __launch_bounds__(256) jacobi_persistent_kernel(Grid g, const double* __restrict__ rho, double* buf0,
                                                                 double* buf1, JacobiPCtrl* ctrl, double den, double tol,
-                                                                long long cap) {
+                                                                long long cap, long long poll_limit) {
     __shared__ double sh[8];
     __shared__ double s_d;
     const double c4pi = 4.0 * xcf::PI;
@@ -620,7 +621,7 @@ __global__ void __launch_bounds__(256) jacobi_persistent_kernel(Grid g, const do
             for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sh[w]);
             atomicMax(&ctrl->slot[s % 3], (unsigned long long)__double_as_longlong(m));
         }
-        if (!grid_barrier(ctrl, nblocks)) return;
+        if (!grid_barrier(ctrl, nblocks, poll_limit)) return;
         if (threadIdx.x == 0) {
             s_d = __longlong_as_double((long long)atomicAdd(&ctrl->slot[s % 3], 0ull));
             if (blockIdx.x == 0) atomicExch(&ctrl->slot[(s + 2) % 3], 0ull);  // read by all before barrier s
@@ -810,7 +811,8 @@ static JacobiResult hartree_persistent(dft_context* ctx, const Grid& g, const do
     const double* r = rho;
     double* b0 = vh;
     double* b1 = buf1;
-    void* args[] = {&gg, &r, &b0, &b1, &ctrl, &den, &tol, &cap};
+    long long polls = ctx->grid_barrier_poll_limit > 0 ? ctx->grid_barrier_poll_limit : (1LL << 24);
+    void* args[] = {&gg, &r, &b0, &b1, &ctrl, &den, &tol, &cap, &polls};
     DFT_CUDA(cudaLaunchCooperativeKernel((const void*)jacobi_persistent_kernel, dim3(nblocks), dim3(256), args, 0,
                                          ctx->stream));
     count_launch(ctx);

@@ -36,6 +36,7 @@ constexpr double EPS = 1.0e-14;
 
 struct RunSpec {
     int Z, kind, norb;
+    double pivot_eps;  // |pivot| below this is singular (EPS unless tuned)
     int n[MAXORB], l[MAXORB], spin[MAXORB], el[MAXORB], idx[MAXORB];
 };
 
@@ -309,12 +310,12 @@ __global__ void __launch_bounds__(RT, 1)
             if (lane == 0) {
                 dw[0] = diag[0] - shift;
                 for (int i = 1; i < n && !bad; ++i) {
-                    if (fabs(dw[i - 1]) < EPS) bad = 1;
+                    if (fabs(dw[i - 1]) < sp.pivot_eps) bad = 1;
                     const double fac = off / dw[i - 1];
                     f[i] = fac;
                     dw[i] = (diag[i] - shift) - fac * off;
                 }
-                if (fabs(dw[n - 1]) < EPS) bad = 1;
+                if (fabs(dw[n - 1]) < sp.pivot_eps) bad = 1;
             }
             bad = __shfl_sync(0xffffffffu, bad, 0);
             if (bad) {
@@ -533,6 +534,7 @@ double* run_batch(dft_context* ctx, int nruns, const int* Z, const int* kinds, l
         std::memset(&s, 0, sizeof s);
         s.Z = Z[rr];
         s.kind = kinds[rr];
+        s.pivot_eps = ctx->radial_pivot_exp == -14 ? EPS : std::pow(10.0, (double)ctx->radial_pivot_exp);
         int q = 0;
         for (int spin = 0; spin < 2; ++spin) {
             int count_l[4] = {0, 0, 0, 0};

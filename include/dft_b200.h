@@ -68,7 +68,13 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               convolutions on tcgen05, 0 = FP32 CUDA cores (results agree to
  *                               BF16 rounding, not bit for bit).
  *   "hpsi_bands_per_thread":    0 = auto (default), 1, 2 or 4 bands marched together by each
- *                               thread of the H psi kernel (results identical for every value). */
+ *                               thread of the H psi kernel (results identical for every value).
+ *   "grid_barrier_poll_limit":  0 = 2^24 (default): polls a block of the persistent Jacobi
+ *                               launch makes at a grid barrier before it gives up; the solve then
+ *                               fails with DFT_CUDA_ERROR and the context stays usable.
+ *   "radial_pivot_exponent":    -14 (default): a pivot of the radial inverse iteration's Thomas
+ *                               factorisation below 10^value in magnitude is singular; the run's
+ *                               status becomes DFT_SINGULAR (reference NumericalMethods.cpp:105-122). */
 dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long value);
 /* The cudaStream_t the context launches on, as an opaque handle (for event timing). */
 void* dft_context_stream(dft_context* ctx);
