@@ -248,6 +248,50 @@ def measure_hpsi(eng, torch, stream, n=(192, 192, 192), bands=16, reps=5):
     return {"grid": list(n), "bands": bands, "ms": ms, "bytes": byts, "gbs": byts / (ms * 1e-3) / 1e9}
 
 
+def ablation(eng, torch, stream, flush, w, net, reps=1):
+    """Time-to-|dE|<1e-6 of one workload as the methods are switched on one at a time: multigrid
+    Poisson cycles (coarse-grid start) with the FP64 eigensolver and its multigrid
+    preconditioner, then + the learned start, + the mixed-precision (tcgen05) eigensolver, then
+    + Pulay/Kerker mixing, the adaptive eigensolver tolerance and the superposed-atoms start.
+    One untimed solve, then `reps` timed ones (L2 flushed before each); per configuration the
+    SCF iterations, energy and the number of tensor-core products."""
+    import dft_b200
+    g = dft_b200.CartesianGrid(*w["n"], *w["bounds"])
+    mol = molecule(w)
+    base = dict(stop_abs_de=1e-6, extra_bands=w["extra_bands"], poisson_start=dft_b200.POISSON_MULTIGRID,
+                eig_preconditioner=-2)
+    steps = [("multigrid", {}), ("+network", {"poisson_net": net.handle}),
+             ("+mixed_precision", {"eig_mixed_precision": 1}),
+             ("+pulay_kerker_atoms", {"mixer": 1, "kerker_q0": 0.8, "adaptive_eig_tol": 1, "initial_density": 1})]
+    out, kw = {}, dict(base)
+    for name, extra in steps:
+        kw.update(extra)
+        o = dft_b200.default_scf_options(**kw)
+        eng.scf_molecule(g, mol, 0, w["multiplicity"], w["functional"], o)
+        ms, r, tc = [], None, 0
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            t0 = eng.counter("tensor_core_products")
+            r = eng.scf_molecule(g, mol, 0, w["multiplicity"], w["functional"], o)
+            tc = eng.counter("tensor_core_products") - t0
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        out[name] = {"ms": statistics.median(ms), "scf_iterations": r.iterations, "energy": r.total,
+                     "eig_iterations": [h["eig_iterations_alpha"] for h in r.history],
+                     "poisson_sweeps": sum(h["poisson_sweeps_in"] + h["poisson_sweeps_out"] for h in r.history),
+                     "tensor_core_products": tc}
+    first = out[steps[0][0]]
+    for v in out.values():
+        v["speedup_vs_multigrid"] = first["ms"] / v["ms"]
+        v["energy_delta_vs_multigrid"] = v["energy"] - first["energy"]
+    return {"workload": w["name"], "desc": w["desc"], "configurations": out}
+
+
 def cpu_baseline(w, sample_iterations=1):
     """The reference's own CPU code on this host: initial densities + `sample_iterations`
     SCF iterations of the workload, scaled to one SCF to |dE| < 1e-6 by the reference's own

@@ -37,7 +37,7 @@ SOURCES = {
     "poisson_start.cu": [],
     "precond_mg.cu": [],
     "atomic_start.cu": [],
-    "eigh.cpp": [],
+    "eigh.cpp": ["-Xcompiler", "-O3"],
 }
 
 

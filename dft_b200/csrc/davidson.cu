@@ -399,6 +399,39 @@ void rotate(dft_context* ctx, const Grid& g, const double* in, long long ldi, in
 
 namespace {
 
+// Y = L^-T for the Cholesky factor S = L L^T of an n x n SPD matrix (row-major), so that
+// T Y has the identity as Gram matrix.  False when a pivot falls below rel * max diag(S).
+bool cholesky_inverse_t(int n, const std::vector<double>& S, double rel, std::vector<double>& Y) {
+    double smax = 0.0;
+    for (int i = 0; i < n; ++i) smax = std::max(smax, S[(size_t)i * n + i]);
+    if (!(smax > 0.0) || !std::isfinite(smax)) return false;
+    std::vector<double> L((size_t)n * n, 0.0);
+    for (int j = 0; j < n; ++j) {
+        double d = S[(size_t)j * n + j];
+        for (int k = 0; k < j; ++k) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
+        if (!(d > rel * smax)) return false;
+        const double ljj = std::sqrt(d);
+        L[(size_t)j * n + j] = ljj;
+        for (int i = j + 1; i < n; ++i) {
+            double v = S[(size_t)i * n + j];
+            for (int k = 0; k < j; ++k) v -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
+            L[(size_t)i * n + j] = v / ljj;
+        }
+    }
+    // M = L^-1 (lower triangular) by forward substitution, column by column; Y = M^T
+    Y.assign((size_t)n * n, 0.0);
+    for (int c = 0; c < n; ++c) {
+        for (int i = c; i < n; ++i) {
+            double v = i == c ? 1.0 : 0.0;
+            for (int k = c; k < i; ++k) v -= L[(size_t)i * n + k] * Y[(size_t)c * n + k];
+            Y[(size_t)c * n + i] = v / L[(size_t)i * n + i];  // Y[c][i] = M[i][c]
+        }
+    }
+    for (double v : Y)
+        if (!std::isfinite(v)) return false;
+    return true;
+}
+
 // Orthonormalise the nt columns of T against V[0:k] and among themselves (dV inner product).
 // Dependent directions are dropped; returns the number kept (compacted to the front of T).
 // tc: Gram products on the tensor cores (TF32 hi+lo, ~1e-6 relative) instead of FP64
@@ -423,6 +456,14 @@ int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, doub
         gram_any(tc, ctx, g, T, ld, nt, T, ld, nt, S);
         for (int i = 0; i < nt; ++i)
             for (int j = 0; j < i; ++j) S[(size_t)i * nt + j] = S[(size_t)j * nt + i] = 0.5 * (S[(size_t)i * nt + j] + S[(size_t)j * nt + i]);
+        // Cholesky QR: S = L L^T, T <- T L^-T, when every pivot stays well above round-off
+        // (O(nt^3/3) on the host); a nearly dependent block falls through to the SVQB below,
+        // which drops the dependent directions
+        if (cholesky_inverse_t(nt, S, tc ? 1e-7 : 1e-12, Yk)) {
+            rotate(ctx, g, T, ld, nt, Yk, nt, W, ld, 1.0, 0.0);
+            DFT_CUDA(cudaMemcpyAsync(T, W, sizeof(double) * (size_t)ld * nt, cudaMemcpyDeviceToDevice, ctx->stream));
+            continue;
+        }
         std::vector<double> Sc = S;
         if (!eigh(nt, Sc, w, Z)) fail(DFT_NUMERICAL, "orthonormalisation eigensolve failed");
         const double wmax = w[nt - 1];
@@ -550,11 +591,10 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
     bool done = false;
     for (it = 1; it <= o.max_iterations; ++it) {
         // ---- Rayleigh–Ritz --------------------------------------------------------------
+        // the lowest nb Ritz pairs only (Z: k x nb); a thick restart below asks for more
         std::vector<double> Gc = G;
-        if (!eigh(k, Gc, w, Z)) fail(DFT_NUMERICAL, "projected eigensolve failed");
-        Y.assign((size_t)k * nb, 0.0);
-        for (int i = 0; i < k; ++i)
-            for (int j = 0; j < nb; ++j) Y[(size_t)i * nb + j] = Z[(size_t)i * k + j];
+        if (!eigh_lowest(k, Gc, nb, w, Z)) fail(DFT_NUMERICAL, "projected eigensolve failed");
+        Y = Z;
         for (int j = 0; j < nb; ++j) theta[j] = w[j];
         rot(Vb, k, Y, nb, X);
         rot(AV, k, Y, nb, AX);
@@ -617,9 +657,13 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         const int na = (int)active.size();
         if (k + na > kmax) {  // thick restart to the lowest kr Ritz vectors
             const int keep = std::min(k, std::max(nb, std::min(kr, kmax - na)));
-            std::vector<double> Zk((size_t)k * keep);
-            for (int i = 0; i < k; ++i)
-                for (int j = 0; j < keep; ++j) Zk[(size_t)i * keep + j] = Z[(size_t)i * k + j];
+            std::vector<double> Zk;
+            if (keep > nb) {
+                std::vector<double> Gc = G;
+                if (!eigh_lowest(k, Gc, keep, w, Zk)) fail(DFT_NUMERICAL, "projected eigensolve failed");
+            } else {
+                Zk = Z;
+            }
             rot(Vb, k, Zk, keep, W);
             DFT_CUDA(cudaMemcpyAsync(Vb, W, vecb * keep, cudaMemcpyDeviceToDevice, ctx->stream));
             rot(AV, k, Zk, keep, W);
