@@ -292,6 +292,57 @@ def ablation(eng, torch, stream, flush, w, net, reps=1):
     return {"workload": w["name"], "desc": w["desc"], "configurations": out}
 
 
+def kernel_table(eng, torch, stream, flush, peak, n=192, h=0.2, reps=3):
+    """Event-timed operators at an n^3 grid (L2 flushed before each timing), with the
+    algorithmic bytes of each: Jacobi 24 B per interior point-sweep (one sweep per launch, and
+    8 temporally blocked sweeps per launch, whose figure is effective: it may exceed the
+    copy peak), XC (both spins, potential + energy) 32 B per point (read n_a, n_b, write
+    v_a, v_b), H psi 16 + 8/b B per band-point."""
+    import dft_b200
+    half = 0.5 * h * (n - 1)
+    g = dft_b200.CartesianGrid(n, n, n, -half, half, -half, half, -half, half)
+    N = g.getSize()
+    x = np.linspace(-half, half, n)
+    Zc, Yc, Xc = np.meshgrid(x, x, x, indexing="ij")
+    r2 = (Xc ** 2 + Yc ** 2 + Zc ** 2).ravel()
+    na = eng.upload(0.6 * np.exp(-0.3 * r2) + 1e-4)
+    nb = eng.upload(0.4 * np.exp(-0.25 * r2) + 1e-4)
+    rho = eng.upload(np.exp(-0.3 * r2))
+    va, vb, vh = eng.array(N), eng.array(N), eng.array(N)
+
+    def timed(fn):
+        fn()
+        ms = []
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    out = {"grid": [n, n, n]}
+    interior = (n - 2) ** 3
+    sweeps = 200
+    for spl, name in ((1, "jacobi_sweep_kernel"), (8, "jacobi_tb_kernel (8 sweeps per launch)")):
+        eng.set_tuning("jacobi_sweeps_per_launch", spl)
+        ms = timed(lambda: eng.hartree(g, rho, vh, 0.0, sweeps))
+        gbs = 24.0 * interior * sweeps / (ms * 1e-3) / 1e9
+        out[name] = {"ms_per_sweep": ms / sweeps, "gbs": gbs, "frac": gbs / peak}
+    eng.set_tuning("jacobi_sweeps_per_launch", 0)
+    for kind in ("PBE96", "PZ81"):
+        ms = timed(lambda: eng.xc(g, kind, na, nb, va, vb, energy=True))
+        gbs = 32.0 * N / (ms * 1e-3) / 1e9
+        out[f"xc_{kind}"] = {"ms": ms, "gbs": gbs, "frac": gbs / peak,
+                             "kernels": "xc_point_kernel + xc_div_kernel" if kind == "PBE96" else
+                             "xc_point_kernel + xc_lda_copy_kernel"}
+    return out
+
+
 def cpu_baseline(w, sample_iterations=1):
     """The reference's own CPU code on this host: initial densities + `sample_iterations`
     SCF iterations of the workload, scaled to one SCF to |dE| < 1e-6 by the reference's own
@@ -379,6 +430,8 @@ def main():
     ap.add_argument("--workload", default="h2_48", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ablation", action="store_true")
+    ap.add_argument("--ablation-workload", default="h2o_128", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -532,6 +585,13 @@ def main():
                  "grid": hp["grid"], "bands": hp["bands"], "ms": hp["ms"]},
         "clocks": clk.summary(),
     }
+    if world == 1:
+        out["kernels"] = kernel_table(eng, torch, stream, flush, peaks["hbm_gbs"])
+    if world == 1 and not args.no_ablation:
+        # the learned and mixed-precision methods switched on one at a time on the larger molecule
+        wa = WORKLOADS[args.ablation_workload]
+        net_a = net if wa["bounds"] == w["bounds"] and wa["n"] == w["n"] else train_network(eng, wa)[0]
+        out["ablation"] = ablation(eng, torch, stream, flush, wa, net_a)
     if world == 1 and not args.no_cpu_baseline:
         w["gpu_iterations"] = last.iterations
         out["cpu_baseline"] = cpu_baseline(w)

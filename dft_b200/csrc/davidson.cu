@@ -448,8 +448,40 @@ int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, doub
     std::vector<double> C, S, w, Z, Yk;
     // directions below the Gram products' noise floor are dropped
     const double floor_rel = tc ? 1e-8 : 1e-13;
+    const double chol_rel = tc ? 1e-7 : 1e-12;
     for (int pass = 0; pass < 2 && nt > 0; ++pass) {
-        if (k > 0) {
+        if (k > 0 && T == V + (long long)k * ld) {
+            // one product [V; T]^T T gives C = V^T T and T^T T; the projected block's Gram is then
+            // T^T T - C^T C, and one rotation applies T <- (T - V C) L^-T (V orthonormal)
+            std::vector<double> M;
+            gram_any(tc, ctx, g, V, ld, k + nt, T, ld, nt, M);  // (k + nt) x nt
+            S.assign((size_t)nt * nt, 0.0);
+            for (int i = 0; i < nt; ++i)
+                for (int j = 0; j <= i; ++j) {
+                    double v = 0.5 * (M[(size_t)(k + i) * nt + j] + M[(size_t)(k + j) * nt + i]);
+                    for (int r = 0; r < k; ++r) v -= M[(size_t)r * nt + i] * M[(size_t)r * nt + j];
+                    S[(size_t)i * nt + j] = S[(size_t)j * nt + i] = v;
+                }
+            if (cholesky_inverse_t(nt, S, chol_rel, Yk)) {
+                std::vector<double> Yc((size_t)(k + nt) * nt, 0.0);
+                for (int r = 0; r < k; ++r)
+                    for (int j = 0; j < nt; ++j) {
+                        double v = 0.0;
+                        for (int c = 0; c <= j; ++c) v -= M[(size_t)r * nt + c] * Yk[(size_t)c * nt + j];
+                        Yc[(size_t)r * nt + j] = v;
+                    }
+                for (int i = 0; i < nt; ++i)
+                    for (int j = 0; j < nt; ++j) Yc[(size_t)(k + i) * nt + j] = Yk[(size_t)i * nt + j];
+                rotate(ctx, g, V, ld, k + nt, Yc, nt, W, ld, 1.0, 0.0);
+                DFT_CUDA(cudaMemcpyAsync(T, W, sizeof(double) * (size_t)ld * nt, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+                continue;
+            }
+            // nearly dependent: project with the C already at hand, then the explicit path below
+            C.assign((size_t)k * nt, 0.0);
+            for (size_t q = 0; q < (size_t)k * nt; ++q) C[q] = M[q];
+            rotate(ctx, g, V, ld, k, C, nt, T, ld, -1.0, 1.0);
+        } else if (k > 0) {
             gram_any(tc, ctx, g, V, ld, k, T, ld, nt, C);  // k x nt
             rotate(ctx, g, V, ld, k, C, nt, T, ld, -1.0, 1.0);
         }
@@ -459,7 +491,7 @@ int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, doub
         // Cholesky QR: S = L L^T, T <- T L^-T, when every pivot stays well above round-off
         // (O(nt^3/3) on the host); a nearly dependent block falls through to the SVQB below,
         // which drops the dependent directions
-        if (cholesky_inverse_t(nt, S, tc ? 1e-7 : 1e-12, Yk)) {
+        if (cholesky_inverse_t(nt, S, chol_rel, Yk)) {
             rotate(ctx, g, T, ld, nt, Yk, nt, W, ld, 1.0, 0.0);
             DFT_CUDA(cudaMemcpyAsync(T, W, sizeof(double) * (size_t)ld * nt, cudaMemcpyDeviceToDevice, ctx->stream));
             continue;
