@@ -47,7 +47,7 @@ class dft_scf_opts(C.Structure):
                 ("verbose", C.c_int), ("poisson_start", C.c_int), ("poisson_net", C.c_void_p), ("mixer", C.c_int),
                 ("pulay_depth", C.c_int), ("pulay_beta", C.c_double), ("adaptive_eig_tol", C.c_int),
                 ("smearing_kt", C.c_double), ("kerker_q0", C.c_double),
-                ("initial_density", C.c_int)]
+                ("log_path", C.c_char_p), ("initial_density", C.c_int)]
 
 
 # dft_poisson_start
@@ -94,7 +94,11 @@ class dft_scf_result(C.Structure):
                 ("alpha_potential", C.POINTER(C.c_double)), ("beta_potential", C.POINTER(C.c_double)),
                 ("orbitals", C.POINTER(C.c_double)),
                 ("history", C.POINTER(dft_scf_iteration)), ("history_capacity", C.c_int),
-                ("history_len", C.c_int), ("seconds", C.c_double)]
+                ("history_len", C.c_int), ("seconds", C.c_double),
+                ("last_energy_criterion_iteration", C.c_int), ("last_density_criterion_iteration", C.c_int),
+                ("last_ks_criterion_iteration", C.c_int), ("min_energy_difference", C.c_double),
+                ("min_density_difference", C.c_double), ("min_ks_residual", C.c_double),
+                ("final_mixing", C.c_double)]
 
 
 class dft_atom_result(C.Structure):
@@ -601,6 +605,8 @@ def default_scf_options(**kw) -> dft_scf_opts:
     for k, v in kw.items():
         if k == "poisson_net" and hasattr(v, "handle"):
             v = v.handle
+        if k == "log_path" and isinstance(v, str):
+            v = v.encode()
         if k not in scf_fields and not (k.startswith("eig_") and k[4:] in eig_fields):
             raise TypeError(f"unknown SCF option {k!r}")
         if k not in scf_fields:
@@ -638,6 +644,7 @@ class SCFResult:
     seconds: float = 0.0
     n_alpha: int = 0
     n_beta: int = 0
+    convergence: dict = field(default_factory=dict)
 
     @property
     def total(self):
@@ -647,8 +654,38 @@ class SCFResult:
     def from_c(cls, r: dft_scf_result, eig, da, db, hist):
         e = EnergyComponents(r.kinetic, r.external, r.hartree, r.exchange_correlation, r.nuclear_repulsion, r.total)
         h = [{k: getattr(hist[i], k) for k, _ in dft_scf_iteration._fields_} for i in range(r.history_len)]
+        conv = {"lastEnergyCriterionIteration": r.last_energy_criterion_iteration,
+                "lastDensityCriterionIteration": r.last_density_criterion_iteration,
+                "lastKSCriterionIteration": r.last_ks_criterion_iteration,
+                "finalEnergyDifference": r.energy_difference, "finalDensityDifference": r.density_difference,
+                "finalKSResidual": r.max_ks_residual, "finalMixing": r.final_mixing,
+                "minimumEnergyDifference": r.min_energy_difference,
+                "minimumDensityDifference": r.min_density_difference, "minimumKSResidual": r.min_ks_residual}
         return cls(e, r.iterations, bool(r.converged), r.density_difference, r.energy_difference, r.max_ks_residual,
-                   list(eig[: r.n_alpha + r.n_beta]), da, db, h, r.seconds, r.n_alpha, r.n_beta)
+                   list(eig[: r.n_alpha + r.n_beta]), da, db, h, r.seconds, r.n_alpha, r.n_beta, conv)
+
+    def to_dict(self, charge: int = 0) -> dict:
+        """The reference's MolecularResult (DFTData.h:86-91) without the grid fields, plus the
+        convergence analysis (MolecularSCFHelpers.h:47-72) and the phase times summed over the
+        iterations (seconds, the MolecularSCFTiming fields this engine measures)."""
+        phases = {k: 1e-3 * sum(h[k] for h in self.history)
+                  for k in ("ms_hartree", "ms_xc", "ms_orbitals", "ms_density", "ms_energy", "ms_total")}
+        timing = {"hartree": phases["ms_hartree"], "exchangeCorrelation": phases["ms_xc"],
+                  "orbitals": phases["ms_orbitals"], "outputDensity": phases["ms_density"],
+                  "totalEnergy": phases["ms_energy"], "totalIterations": phases["ms_total"], "total": self.seconds}
+        return {"electrons": self.n_alpha + self.n_beta, "charge": charge,
+                "scf": {"energy": vars(self.energy), "iterations": self.iterations, "converged": self.converged,
+                        "densityDifference": self.densityDifference, "energyDifference": self.energyDifference,
+                        "maxKSResidual": self.maxKSResidual,
+                        "alphaEigenvalues": self.eigenvalues[: self.n_alpha],
+                        "betaEigenvalues": self.eigenvalues[self.n_alpha:]},
+                "convergenceAnalysis": self.convergence, "timing": timing, "history": self.history}
+
+    def write_json(self, path: str, charge: int = 0) -> None:
+        """The result file: one JSON document (to_dict)."""
+        import json
+        with open(path, "w") as f:
+            json.dump(self.to_dict(charge), f, indent=1)
 
 
 @dataclass

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <limits>
+#include <string>
 #include <vector>
 
 #include "neural.h"
@@ -304,6 +305,35 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     bool converged = false;
     int it = 0;
     res->history_len = 0;
+    // convergence analysis (MolecularSCFConvergenceAnalysis, reference MolecularSCFHelpers.h:47-72)
+    res->last_energy_criterion_iteration = res->last_density_criterion_iteration = res->last_ks_criterion_iteration = 0;
+    res->min_energy_difference = res->min_density_difference = res->min_ks_residual =
+        std::numeric_limits<double>::infinity();
+    res->final_mixing = 0.0;
+    // JSON-lines log (option): one object per iteration and a final result line
+    FILE* log = nullptr;
+    if (o.log_path) {
+        log = std::fopen(o.log_path, "w");
+        if (!log) fail(DFT_INVALID_ARGUMENT, "cannot open the SCF log file '%s'", o.log_path);
+    }
+    struct LogCloser {
+        FILE*& f;
+        ~LogCloser() {
+            if (f) std::fclose(f);
+        }
+    } log_closer{log};
+    auto jnum = [](double v) {  // JSON has no inf/nan
+        char b[40];
+        if (std::isfinite(v)) std::snprintf(b, sizeof b, "%.17g", v);
+        else std::snprintf(b, sizeof b, "null");
+        return std::string(b);
+    };
+    auto jlevels = [&](const std::vector<double>& e, int nocc) {
+        std::string r = "[";
+        for (int i = std::max(0, nocc - 3); i < std::min((int)e.size(), nocc + 3); ++i)
+            r += (r.size() > 1 ? "," : "") + jnum(e[i]);
+        return r + "]";
+    };
     std::vector<double> Ta(bands_a), Tb(bands_b);
     for (it = 1; it <= o.max_iterations; ++it) {
         const auto t_it = Clock::now();
@@ -404,6 +434,30 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         rec.mixing = o.mixer == 1 ? pbeta : imix;
         rec.ms_total = ms_since(t_it);
         if (res->history && res->history_len < res->history_capacity) res->history[res->history_len++] = rec;
+        if (dE < o.energy_tol) res->last_energy_criterion_iteration = it;
+        if (effd < o.density_tol) res->last_density_criterion_iteration = it;
+        if (resid < o.ks_tol) res->last_ks_criterion_iteration = it;
+        res->min_energy_difference = std::min(res->min_energy_difference, dE);
+        res->min_density_difference = std::min(res->min_density_difference, effd);
+        res->min_ks_residual = std::min(res->min_ks_residual, resid);
+        res->final_mixing = rec.mixing;
+        if (log) {
+            std::fprintf(log,
+                         "{\"iteration\":%d,\"energy\":%s,\"energy_difference\":%s,\"density_difference\":%s,"
+                         "\"ks_residual\":%s,\"mixing\":%s,\"kinetic\":%s,\"external\":%s,\"hartree\":%s,"
+                         "\"exchange_correlation\":%s,\"nuclear_repulsion\":%s,\"poisson_sweeps_in\":%ld,"
+                         "\"poisson_sweeps_out\":%ld,\"eig_iterations_alpha\":%d,\"eig_iterations_beta\":%d,"
+                         "\"levels_alpha\":%s,\"levels_beta\":%s,\"ms_hartree\":%s,\"ms_xc\":%s,"
+                         "\"ms_orbitals\":%s,\"ms_density\":%s,\"ms_energy\":%s,\"ms_total\":%s}\n",
+                         it, jnum(E[5]).c_str(), jnum(dE).c_str(), jnum(effd).c_str(), jnum(resid).c_str(),
+                         jnum(rec.mixing).c_str(), jnum(E[0]).c_str(), jnum(E[1]).c_str(), jnum(E[2]).c_str(),
+                         jnum(E[3]).c_str(), jnum(E[4]).c_str(), jin.sweeps, jout.sweeps, rec.eig_iterations_alpha,
+                         rec.eig_iterations_beta, jlevels(eiga, na).c_str(),
+                         jlevels(closed ? eiga : eigb, nb).c_str(), jnum(rec.ms_hartree).c_str(),
+                         jnum(rec.ms_xc).c_str(), jnum(rec.ms_orbitals).c_str(), jnum(rec.ms_density).c_str(),
+                         jnum(rec.ms_energy).c_str(), jnum(rec.ms_total).c_str());
+            std::fflush(log);
+        }
         if (o.verbose)
             fprintf(stderr,
                     "[scf] it=%3d E=%.12f dE=%.3e dRho=%.3e KS=%.3e mix=%.3f sweeps=%ld/%ld eig_it=%d/%d  %.1f ms\n", it,
@@ -483,6 +537,25 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     }
     sync(ctx);
     res->seconds = ms_since(t_start) * 1e-3;
+    if (log) {
+        std::fprintf(log,
+                     "{\"result\":{\"electrons\":%d,\"charge\":%d,\"multiplicity\":%d,\"converged\":%s,"
+                     "\"iterations\":%d,\"energy\":{\"kinetic\":%s,\"external\":%s,\"hartree\":%s,"
+                     "\"exchangeCorrelation\":%s,\"nuclearRepulsion\":%s,\"total\":%s},"
+                     "\"densityDifference\":%s,\"energyDifference\":%s,\"maxKSResidual\":%s,"
+                     "\"convergenceAnalysis\":{\"lastEnergyCriterionIteration\":%d,"
+                     "\"lastDensityCriterionIteration\":%d,\"lastKSCriterionIteration\":%d,"
+                     "\"minimumEnergyDifference\":%s,\"minimumDensityDifference\":%s,\"minimumKSResidual\":%s,"
+                     "\"finalMixing\":%s},\"alphaLevels\":%s,\"betaLevels\":%s,\"seconds\":%s}}\n",
+                     ne, charge, multiplicity, converged ? "true" : "false", res->iterations, jnum(E[0]).c_str(),
+                     jnum(E[1]).c_str(), jnum(E[2]).c_str(), jnum(E[3]).c_str(), jnum(E[4]).c_str(),
+                     jnum(E[5]).c_str(), jnum(effd).c_str(), jnum(dE).c_str(), jnum(resid).c_str(),
+                     res->last_energy_criterion_iteration, res->last_density_criterion_iteration,
+                     res->last_ks_criterion_iteration, jnum(res->min_energy_difference).c_str(),
+                     jnum(res->min_density_difference).c_str(), jnum(res->min_ks_residual).c_str(),
+                     jnum(res->final_mixing).c_str(), jlevels(eiga, na).c_str(),
+                     jlevels(closed ? eiga : eigb, nb).c_str(), jnum(res->seconds).c_str());
+    }
 }
 
 }  // namespace dftb

@@ -240,6 +240,11 @@ typedef struct {
                                 bands instead of the reference's integer aufbau (0) */
     double kerker_q0;        /* > 0: Kerker screening of the total-charge residual in either mixer,
                                 -lap/(-lap + q0^2) by one multigrid cycle (bohr^-1; 0 = off) */
+    const char* log_path;    /* non-NULL: one JSON object per SCF iteration (the dft_scf_iteration
+                                fields, energy components, the levels around the Fermi level per
+                                spin) and a final {"result": ...} line, written to this file; the
+                                reference prints the same quantities as tables
+                                (MolecularSCFHelpers.cpp:251-513) */
     int initial_density;     /* 0: orbitals of the bare nuclear potential, as the reference
                                 (buildInitialMolecularDensities, MolecularSCFHelpers.cpp:515-579);
                                 1: superposed radial atoms of the same functional (batched radial
@@ -272,6 +277,12 @@ typedef struct {
     dft_scf_iteration* history;     /* caller buffer of history_capacity records, or NULL */
     int history_capacity, history_len;
     double seconds;                 /* wall time of the solve */
+    /* MolecularSCFConvergenceAnalysis (reference MolecularSCFHelpers.h:47-72): the last
+     * iteration meeting each of the three stop criteria (0 = none) and the smallest value each
+     * measure reached; the final values are energy_difference, density_difference and
+     * max_ks_residual above */
+    int last_energy_criterion_iteration, last_density_criterion_iteration, last_ks_criterion_iteration;
+    double min_energy_difference, min_density_difference, min_ks_residual, final_mixing;
 } dft_scf_result;
 
 void dft_scf_default_options(dft_scf_opts* opts);

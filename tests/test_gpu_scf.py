@@ -100,3 +100,35 @@ def test_radial_bad_inputs(engine):
         engine.solve_atoms([31], ["PZ81"])
     with pytest.raises(dft_b200.DFTError):
         engine.solve_atoms([1], ["PZ81"], points=1)
+
+
+def test_scf_log_and_result_file(engine, tmp_path):
+    """The JSON-lines log (one object per iteration, then the result) and the result file
+    agree with the returned result and its history; the convergence analysis matches the
+    reference's definitions (MolecularSCFHelpers.h:47-72)."""
+    import json
+
+    g = dft_b200.CartesianGrid(14, 14, 14, -4.0, 4.0, -4.0, 4.0, -4.0, 4.0)
+    m = dft_b200.Molecule()
+    m.addNucleus(1, -0.7, 0.013, 0.02)
+    m.addNucleus(1, 0.7, 0.013, 0.02)
+    log = tmp_path / "scf.jsonl"
+    r = engine.scf_molecule(g, m, 0, 1, "PZ81", dft_b200.default_scf_options(log_path=str(log)))
+    lines = [json.loads(x) for x in log.read_text().splitlines()]
+    assert len(lines) == r.iterations + 1
+    assert [x["iteration"] for x in lines[:-1]] == list(range(1, r.iterations + 1))
+    res = lines[-1]["result"]
+    assert res["energy"]["total"] == r.total and res["iterations"] == r.iterations
+    assert res["converged"] == r.converged
+    hist = r.history
+    assert r.convergence["minimumEnergyDifference"] == min(h["energy_difference"] for h in hist)
+    assert r.convergence["minimumDensityDifference"] == min(h["density_difference"] for h in hist)
+    if r.converged:
+        assert r.convergence["lastEnergyCriterionIteration"] == r.iterations
+    for x, h in zip(lines[:-1], hist):
+        assert x["energy"] == h["energy"] and x["poisson_sweeps_in"] == h["poisson_sweeps_in"]
+    out = tmp_path / "result.json"
+    r.write_json(str(out))
+    doc = json.loads(out.read_text())
+    assert doc["scf"]["energy"]["total"] == r.total and doc["electrons"] == 2
+    assert doc["convergenceAnalysis"]["lastKSCriterionIteration"] == r.convergence["lastKSCriterionIteration"]
