@@ -37,7 +37,7 @@ class dft_grid(C.Structure):
 
 class dft_eig_opts(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iterations", C.c_int), ("max_subspace", C.c_int), ("verbose", C.c_int),
-                ("preconditioner", C.c_int), ("mixed_precision", C.c_int)]
+                ("preconditioner", C.c_int), ("mixed_precision", C.c_int), ("preconditioner_net", C.c_void_p)]
 
 
 class dft_scf_opts(C.Structure):
@@ -162,6 +162,8 @@ _SIGS = {
                                    C.c_double, C.c_int, C.c_int, _P, C.POINTER(C.c_int)], C.c_int),
     "dft_pnet_train_poisson": ([_P, _P, C.POINTER(dft_pnet_train_opts), C.POINTER(dft_pnet_train_report)],
                                C.c_int),
+    "dft_pnet_train_preconditioner": ([_P, _P, C.POINTER(dft_grid), _P, C.c_int, C.c_int,
+                                       C.POINTER(dft_pnet_train_opts), C.POINTER(dft_pnet_train_report)], C.c_int),
 }
 
 _lib = None
@@ -459,10 +461,11 @@ class Engine:
                                      int(precision)))
 
     def solve_orbitals(self, grid, V, nocc, nbands, psi, ld, init=False, tol=1e-7, max_iterations=2000,
-                       max_subspace=3, verbose=False, preconditioner=4, mixed_precision=0):
+                       max_subspace=3, verbose=False, preconditioner=4, mixed_precision=0, preconditioner_net=None):
         g = grid.c()
         eig = np.zeros(nbands)
-        o = dft_eig_opts(tol, max_iterations, max_subspace, int(verbose), int(preconditioner), int(mixed_precision))
+        o = dft_eig_opts(tol, max_iterations, max_subspace, int(verbose), int(preconditioner), int(mixed_precision),
+                         preconditioner_net.handle if preconditioner_net is not None else None)
         it = C.c_int()
         _check(load().dft_solve_orbitals_dev(self.ctx, C.byref(g), _ptr(V), nocc, nbands, _ptr(psi), ld, int(init),
                                              _dp(eig), C.byref(o), C.byref(it)))
@@ -579,6 +582,28 @@ class PoissonNet:
         r.epoch_loss = C.cast(hist, C.POINTER(C.c_double))
         r.epoch_loss_capacity = epochs
         _check(load().dft_pnet_train_poisson(self.engine.ctx, self.handle, C.byref(o), C.byref(r)))
+        out = {k: getattr(r, k) for k, _ in dft_pnet_train_report._fields_ if k not in ("epoch_loss",
+                                                                                      "epoch_loss_capacity")}
+        out["epoch_loss"] = list(hist)
+        return out
+
+    def train_preconditioner(self, grid, V, nocc, nbands, samples=96, validation=16, epochs=12, batch=4, lr=2e-3,
+                             lr_min=5e-5, seed=2026, cycles=12, verbose=False) -> dict:
+        """Trains this network as the learned Davidson preconditioner (preconditioner -3) on the
+        residual bands of a plain block eigensolve in the device potential V on `grid`; targets
+        from `cycles` refined multigrid cycles.  Returns the training report."""
+        o = dft_pnet_train_opts()
+        o.samples, o.validation, o.epochs, o.batch = samples, validation, epochs, batch
+        o.lr, o.lr_min, o.seed = lr, lr_min, seed
+        o.target_tol, o.target_max_sweeps = 1e-7, cycles
+        o.verbose = int(verbose)
+        r = dft_pnet_train_report()
+        hist = (C.c_double * epochs)()
+        r.epoch_loss = C.cast(hist, C.POINTER(C.c_double))
+        r.epoch_loss_capacity = epochs
+        g = grid.c()
+        _check(load().dft_pnet_train_preconditioner(self.engine.ctx, self.handle, C.byref(g), _ptr(V), int(nocc),
+                                                    int(nbands), C.byref(o), C.byref(r)))
         out = {k: getattr(r, k) for k, _ in dft_pnet_train_report._fields_ if k not in ("epoch_loss",
                                                                                       "epoch_loss_capacity")}
         out["epoch_loss"] = list(hist)

@@ -311,6 +311,7 @@ dft_status_t dft_solve_orbitals_dev(dft_context* ctx, const dft_grid* g, const d
             if (opts->max_iterations > 0) o.max_iterations = opts->max_iterations;
             if (opts->max_subspace >= 2) o.max_subspace = opts->max_subspace;
             o.precond_steps = opts->preconditioner;
+            o.precond_net = opts->preconditioner_net;
             o.mixed_precision = opts->mixed_precision;
             o.verbose = opts->verbose;
         }
@@ -473,5 +474,15 @@ dft_status_t dft_pnet_train_poisson(dft_context* ctx, dft_pnet* net, const dft_p
     return guard(ctx, [&] {
         NEED(ctx && net && opts && report, "NULL argument");
         dftb::pnet_train_poisson(ctx, net, opts, report);
+    });
+}
+
+dft_status_t dft_pnet_train_preconditioner(dft_context* ctx, dft_pnet* net, const dft_grid* g, const double* V,
+                                           int nocc, int nbands, const dft_pnet_train_opts* opts,
+                                           dft_pnet_train_report* report) {
+    return guard(ctx, [&] {
+        NEED(ctx && net && g && V && opts && report, "NULL argument");
+        NEED(nocc > 0 && nbands >= nocc, "need 0 < nocc <= nbands");
+        dftb::pnet_train_precond(ctx, net, dftb::make_grid(g), V, nocc, nbands, opts, report);
     });
 }

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "eigh.h"
+#include "neural.h"
 #include "ops.h"
 
 namespace dftb {
@@ -529,6 +530,8 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
     if (nbands < nocc) fail(DFT_INVALID_ARGUMENT, "nbands must be >= the number of orbitals");
     if (nbands > g.N) fail(DFT_INVALID_ARGUMENT, "more bands than grid points");
     if (ld < g.N) fail(DFT_INVALID_ARGUMENT, "ld must be >= nx*ny*nz");
+    if (o.precond_steps == -3 && !o.precond_net) fail(DFT_INVALID_ARGUMENT, "preconditioner -3 needs a network");
+    if (o.precond_steps < -3) fail(DFT_INVALID_ARGUMENT, "unknown preconditioner %d", o.precond_steps);
     const int nb = nbands;
     // basis cap: max_subspace x nbands, and at least nbands + 16 (the reference's subspace of 16);
     // a restart keeps the lowest kr Ritz vectors (thick restart)
@@ -704,6 +707,7 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
             G.assign((size_t)k * k, 0.0);
             for (int i = 0; i < k; ++i) G[(size_t)i * k + i] = w[i];
         }
+        if (o.harvest) o.harvest(o.harvest_user, R, ld, active.data(), na, theta.data());
         double* T = Vb + (long long)k * ld;
         DFT_CUDA(cudaMemcpyAsync(dsrc, active.data(), sizeof(int) * na, cudaMemcpyHostToDevice, ctx->stream));
         // auto (-2): one multigrid cycle on large grids, where a few smoothing steps no longer
@@ -716,6 +720,8 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         } else if (pc < 0) {
             // one multigrid cycle for (T + sigma_b) t = r_b, sigma_b = max(-theta_b, 1 Ha)
             precondition_multigrid(ctx, g, R, dsrc, na, dtheta, T, ld);
+            // -3: plus the learned correction toward the equation's solution
+            if (pc == -3) pnet_precondition(ctx, o.precond_net, g, R, ld, active.data(), na, T);
         } else {
             // (T + sigma_b) t = r_b with sigma_b = max(-theta_b, 1 Ha): the far-field (V ~ 0) form of
             // (H - theta_b) for bound states; t0 = r/d, then damped-Jacobi steps (w = 2/3)

@@ -867,6 +867,43 @@ __global__ void build_input_kernel(long long n, const double* __restrict__ rho, 
     }
 }
 
+// ---- learned Davidson preconditioner: t = t0 + s * net([c r / s, t0 / s]), s = max|t0| ------
+__global__ void absmax_kernel(long long n, const double* __restrict__ x, unsigned long long* __restrict__ out) {
+    double m = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(x[p]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+__global__ void pc_input_kernel(long long n, const double* __restrict__ r, const double* __restrict__ t0,
+                                const unsigned long long* __restrict__ sbits, double c, bf16* __restrict__ x) {
+    const double s = __longlong_as_double((long long)*sbits);
+    const double is = s > 0.0 ? 1.0 / s : 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        reinterpret_cast<uint32_t*>(x)[p] = pack_bf2((float)(c * r[p] * is), (float)(t0[p] * is));
+}
+// interior points: t += s y
+__global__ void pc_apply_kernel(Grid g, const float* __restrict__ y, const unsigned long long* __restrict__ sbits,
+                                double* __restrict__ t) {
+    const double s = __longlong_as_double((long long)*sbits);
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((long long)g.nx * g.ny));
+        const bool face = i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz;
+        if (!face) t[p] += s * (double)y[p];
+    }
+}
+// training target (t* - t0) / s on the interior, 0 on faces
+__global__ void pc_target_kernel(Grid g, const double* __restrict__ ts, const double* __restrict__ t0,
+                                 const unsigned long long* __restrict__ sbits, float* __restrict__ t) {
+    const double s = __longlong_as_double((long long)*sbits);
+    const double is = s > 0.0 ? 1.0 / s : 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((long long)g.nx * g.ny));
+        const bool face = i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz;
+        t[p] = face ? 0.f : (float)((ts[p] - t0[p]) * is);
+    }
+}
+
 // training target: (v - vup) / s on the interior, 0 on faces
 __global__ void build_target_kernel(Grid g, const double* __restrict__ v, const double* __restrict__ vup,
                                     const double* __restrict__ s, float* __restrict__ t) {
@@ -940,6 +977,7 @@ struct dft_pnet {
     dftb::DBuf<double> red;
     dftb::DBuf<int> tc_err;  // set by a tensor-core convolution block whose wait timed out
     dftb::DBuf<__nv_bfloat16> dzb;  // output gradient rounded to BF16 for the tensor-core data gradient
+    dftb::DBuf<unsigned long long> sbits;  // per-band scale of the preconditioner's input/output
 };
 
 namespace dftb {
@@ -1480,6 +1518,173 @@ void pnet_train_poisson(dft_context* ctx, dft_pnet* n, const dft_pnet_train_opts
     sync(ctx);
     rep->val_loss = h[0] / o->validation;
     rep->val_loss_coarse = h[1] / o->validation;
+}
+
+
+// ---- learned Davidson preconditioner ------------------------------------------------------
+// The preconditioning equation of the block eigensolver is (T + sigma) t = r (T = -1/2 lap_h,
+// zero outside the box).  One batched multigrid cycle gives t0; the network, fed the scaled
+// residual and t0, predicts the rest of the way to the equation's solution on the interior:
+// t = t0 + s net([2 h^2 r / s, t0 / s]), s = max |t0| (the equation is linear, so the scaled
+// problem looks the same for every band).
+
+void pnet_precondition(dft_context* ctx, dft_pnet* n, const Grid& g, const double* R, long long ld, const int* active,
+                       int na, double* T) {
+    if (na <= 0) return;
+    const Vol v0{g.nx, g.ny, g.nz};
+    ensure_buffers(n, v0, false);
+    unsigned long long* sb = n->sbits.get(1);
+    const double c = 2.0 * (g.dx * g.dx + g.dy * g.dy + g.dz * g.dz) / 3.0;
+    const int nb = blocks_for(ctx, g.N);
+    for (int a = 0; a < na; ++a) {
+        const double* r = R + (long long)active[a] * ld;
+        double* t = T + (long long)a * ld;
+        DFT_CUDA(cudaMemsetAsync(sb, 0, sizeof(unsigned long long), ctx->stream));
+        absmax_kernel<<<nb, 256, 0, ctx->stream>>>(g.N, t, sb);
+        pc_input_kernel<<<nb, 256, 0, ctx->stream>>>(g.N, r, t, sb, c, n->x.p);
+        forward(ctx, n, v0, n->x.p);
+        pc_apply_kernel<<<nb, 256, 0, ctx->stream>>>(g, n->y.p, sb, t);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx, 3);
+    }
+    check_tc(ctx, n);
+}
+
+namespace {
+// residual bands harvested from the plain eigensolver's iterations
+struct Harvest {
+    dft_context* ctx;
+    long long N;
+    int want, got = 0;
+    double* R;                  // want x N
+    std::vector<double> sigma;  // max(-theta, 1)
+};
+void harvest_residuals(void* user, const double* R, long long ld, const int* active, int na, const double* theta) {
+    auto* h = (Harvest*)user;
+    for (int a = 0; a < na && h->got < h->want; ++a, ++h->got) {
+        DFT_CUDA(cudaMemcpyAsync(h->R + (long long)h->got * h->N, R + (long long)active[a] * ld,
+                                 sizeof(double) * (size_t)h->N, cudaMemcpyDeviceToDevice, h->ctx->stream));
+        h->sigma.push_back(std::max(-theta[active[a]], 1.0));
+    }
+}
+}  // namespace
+
+void pnet_train_precond(dft_context* ctx, dft_pnet* n, const Grid& g, const double* V, int nocc, int nbands,
+                        const dft_pnet_train_opts* o, dft_pnet_train_report* rep) {
+    using Clock = std::chrono::steady_clock;
+    if (!o || !rep) fail(DFT_INVALID_ARGUMENT, "NULL options or report");
+    if (o->samples < 3 || o->validation < 1 || o->validation >= o->samples || o->epochs < 1 || o->batch < 1 ||
+        !(o->lr > 0) || o->lr_min < 0 || o->target_max_sweeps < 2)
+        fail(DFT_INVALID_ARGUMENT, "invalid training options");
+    if (g.nx < 8 || g.ny < 8 || g.nz < 8) fail(DFT_INVALID_ARGUMENT, "training grid too small");
+    const auto t0 = Clock::now();
+    const long long N = g.N;
+    // ---- data: the plain solver's residual bands in V (multigrid preconditioner), then per band
+    // one cycle (the network's input) and target_max_sweeps cycles of refinement (its target)
+    DBuf<double> Rs, X0, Xs, res, e, sig, psi;
+    Harvest hv{ctx, N, o->samples};
+    hv.R = Rs.get((size_t)o->samples * N);
+    EigOpts eo;
+    eo.tol = o->target_tol > 0 ? o->target_tol : 1e-7;
+    eo.max_iterations = 400;
+    eo.precond_steps = -1;
+    eo.harvest = harvest_residuals;
+    eo.harvest_user = &hv;
+    std::vector<double> eig(nbands), rn(nbands);
+    double* pp = psi.get((size_t)nbands * N);
+    try {
+        solve_orbitals(ctx, g, V, nocc, nbands, pp, N, false, eig.data(), rn.data(), eo);
+    } catch (const Error& err) {
+        if (err.status != DFT_NOT_CONVERGED) throw;  // enough residuals may have been harvested anyway
+    }
+    const int ns = hv.got;
+    if (ns < o->validation + 2) fail(DFT_INVALID_ARGUMENT, "the eigensolver produced only %d residual bands", ns);
+    double* sd = sig.get((size_t)ns);
+    DFT_CUDA(cudaMemcpyAsync(sd, hv.sigma.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, ctx->stream));
+    double* x0 = X0.get((size_t)ns * N);
+    double* xs = Xs.get((size_t)ns * N);
+    double* rr = res.get((size_t)ns * N);
+    double* ee = e.get((size_t)ns * N);
+    helmholtz_refine(ctx, g, hv.R, ns, sd, x0, N, 1, rr, ee);
+    helmholtz_refine(ctx, g, hv.R, ns, sd, xs, N, (int)o->target_max_sweeps, rr, ee);
+    const Vol v0{g.nx, g.ny, g.nz};
+    ensure_buffers(n, v0, true);
+    struct Sample {
+        DBuf<bf16> x;
+        DBuf<float> t;
+    };
+    std::vector<std::unique_ptr<Sample>> data;
+    unsigned long long* sb = n->sbits.get(1);
+    const double c = 2.0 * (g.dx * g.dx + g.dy * g.dy + g.dz * g.dz) / 3.0;
+    const int nbk = blocks_for(ctx, N);
+    for (int q = 0; q < ns; ++q) {
+        auto smp = std::make_unique<Sample>();
+        DFT_CUDA(cudaMemsetAsync(sb, 0, sizeof(unsigned long long), ctx->stream));
+        absmax_kernel<<<nbk, 256, 0, ctx->stream>>>(N, x0 + (long long)q * N, sb);
+        pc_input_kernel<<<nbk, 256, 0, ctx->stream>>>(N, hv.R + (long long)q * N, x0 + (long long)q * N, sb, c,
+                                                       smp->x.get((size_t)N * 2));
+        pc_target_kernel<<<nbk, 256, 0, ctx->stream>>>(g, xs + (long long)q * N, x0 + (long long)q * N, sb,
+                                                        smp->t.get((size_t)N));
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx, 3);
+        data.push_back(std::move(smp));
+    }
+    sync(ctx);
+    rep->seconds_data = std::chrono::duration<double>(Clock::now() - t0).count();
+    rep->mean_target_sweeps = (double)o->target_max_sweeps;
+    // ---- training: mean squared error of the correction over interior points
+    const int nval = std::min(o->validation, ns - 2);
+    const int ntrain = ns - nval;
+    const int spe = (ntrain + o->batch - 1) / o->batch;
+    const long total = (long)spe * o->epochs;
+    std::mt19937_64 rng(o->seed ^ 0x2545F4914F6CDD1DULL);
+    std::vector<int> order(ntrain);
+    std::iota(order.begin(), order.end(), 0);
+    double* h = pinned(ctx, 2);
+    const LossSpec L = loss_spec(g, 0, 1.0);
+    const auto t1 = Clock::now();
+    long step = 0;
+    for (int ep = 0; ep < o->epochs; ++ep) {
+        std::shuffle(order.begin(), order.end(), rng);
+        DFT_CUDA(cudaMemsetAsync(n->red.p, 0, 8, ctx->stream));
+        for (int b0 = 0; b0 < ntrain; b0 += o->batch) {
+            const int nb = std::min(o->batch, ntrain - b0);
+            DFT_CUDA(cudaMemsetAsync(n->g.p, 0, n->np * 4, ctx->stream));
+            for (int b = 0; b < nb; ++b) {
+                const Sample& smp = *data[order[b0 + b]];
+                forward(ctx, n, v0, smp.x.p);
+                backward(ctx, n, v0, smp.x.p, smp.t.p, L);
+            }
+            const double cosf_ = 0.5 * (1.0 + std::cos(3.14159265358979323846 * (double)step / (double)total));
+            adam_step(ctx, n, (float)(o->lr_min + (o->lr - o->lr_min) * cosf_), 1.f / (float)nb);
+            ++step;
+        }
+        DFT_CUDA(cudaMemcpyAsync(h, n->red.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        sync(ctx);
+        const double el = h[0] / ntrain;
+        check_tc(ctx, n);
+        if (ep == 0) rep->train_loss_first_epoch = el;
+        rep->train_loss_last_epoch = el;
+        if (rep->epoch_loss && ep < rep->epoch_loss_capacity) rep->epoch_loss[ep] = el;
+        if (o->verbose) fprintf(stderr, "[pnet precond] epoch %d loss %.6e\n", ep + 1, el);
+    }
+    sync(ctx);
+    rep->seconds_train = std::chrono::duration<double>(Clock::now() - t1).count();
+    rep->steps = (int)step;
+    rep->ms_per_step = step ? 1e3 * rep->seconds_train / step : 0.0;
+    // ---- validation: network vs one multigrid cycle alone (zero correction)
+    double* red2 = n->red.p;
+    DFT_CUDA(cudaMemsetAsync(red2, 0, 16, ctx->stream));
+    for (int q = ntrain; q < ns; ++q) {
+        const Sample& smp = *data[q];
+        forward(ctx, n, v0, smp.x.p);
+        loss_dy(ctx, n, v0, L, n->y.p, smp.t.p, nullptr, red2);
+        loss_dy(ctx, n, v0, L, nullptr, smp.t.p, nullptr, red2 + 1);
+    }
+    DFT_CUDA(cudaMemcpyAsync(h, red2, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    rep->val_loss = h[0] / nval;
+    rep->val_loss_coarse = h[1] / nval;
 }
 
 }  // namespace dftb

@@ -70,4 +70,13 @@ int synthetic_density(dft_context* ctx, const Grid& g, unsigned long long seed, 
 void pnet_train_poisson(dft_context* ctx, dft_pnet* net, const dft_pnet_train_opts* opts,
                         dft_pnet_train_report* report);
 
+// Learned Davidson preconditioner: T_a (the multigrid cycle's t0 for band active[a] of R) gets
+// the network's correction toward the solution of (T + sigma) t = r on the interior.
+void pnet_precondition(dft_context* ctx, dft_pnet* net, const Grid& g, const double* R, long long ld,
+                       const int* active, int na, double* T);
+// Trains it on residual bands that the plain eigensolver (multigrid preconditioner) produces in
+// the potential V (device), targets from opts->target_max_sweeps refined multigrid cycles.
+void pnet_train_precond(dft_context* ctx, dft_pnet* net, const Grid& g, const double* V, int nocc, int nbands,
+                        const dft_pnet_train_opts* opts, dft_pnet_train_report* report);
+
 }  // namespace dftb

@@ -102,12 +102,22 @@ void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, co
 void screened_poisson_vcycle(dft_context* ctx, const Grid& g, const double* src, int nb, double q2, double* x,
                              long long ld);
 
+// X_a ~ (T + sigma_a)^-1 R_a for nb fields by `cycles` multigrid cycles with iterative refinement
+// (the first from zero), sigma on the device; res and e: scratch of nb x ld doubles each.
+void helmholtz_refine(dft_context* ctx, const Grid& g, const double* R, int nb, const double* sigma_dev, double* X,
+                      long long ld, int cycles, double* res, double* e);
+
 struct EigOpts {
     double tol = 1e-7;
     int max_iterations = 2000;
     int max_subspace = 3;
     int verbose = 0;
-    int precond_steps = 4;  // 0 = the reference's diagonal preconditioner
+    int precond_steps = 4;  // 0 = the reference's diagonal preconditioner; -3 = learned (precond_net)
+    dft_pnet* precond_net = nullptr;
+    // training-data hook: called every iteration with the residual block and its active bands
+    void (*harvest)(void* user, const double* R, long long ld, const int* active, int na, const double* theta) =
+        nullptr;
+    void* harvest_user = nullptr;
     int mixed_precision = 0;       // 1 = tensor-core (TF32 hi+lo) Gram products while residuals are large
     double mixed_switch = 1e-3;    // occupied residual below which the solver switches to FP64
 };

@@ -309,6 +309,35 @@ void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, co
     vcycle_batch(ctx, g, R, src_dev, nb, shift, 2.0, T, ld);
 }
 
+namespace {
+__global__ void pc_sigma_shift_kernel(int nb, const double* __restrict__ sigma, double* __restrict__ shift) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nb; a += gridDim.x * blockDim.x) shift[a] = 2.0 * sigma[a];
+}
+__global__ void pc_add_kernel(long long n, long long ld, const double* __restrict__ e, double* __restrict__ x) {
+    const int a = blockIdx.y;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        x[(long long)a * ld + p] += e[(long long)a * ld + p];
+}
+}  // namespace
+
+void helmholtz_refine(dft_context* ctx, const Grid& g, const double* R, int nb, const double* sigma_dev, double* X,
+                      long long ld, int cycles, double* res, double* e) {
+    if (nb <= 0) return;
+    double* shift = (double*)ws_get(ctx, WS_PG3, sizeof(double) * (size_t)nb + 64);
+    pc_sigma_shift_kernel<<<(nb + 127) / 128, 128, 0, ctx->stream>>>(nb, sigma_dev, shift);
+    count_launch(ctx);
+    vcycle_batch(ctx, g, R, nullptr, nb, shift, 2.0, X, ld);
+    for (int c = 1; c < cycles; ++c) {
+        // res = 2 R - ((den + 2 sigma) X - sum), the equation's residual in the cycle's scaling
+        pc_residual_kernel<<<pc_grid(ctx, g.N, nb), 256, 0, ctx->stream>>>(g, ld, R, 2.0, shift, X, res);
+        count_launch(ctx);
+        vcycle_batch(ctx, g, res, nullptr, nb, shift, 1.0, e, ld);
+        pc_add_kernel<<<pc_grid(ctx, g.N, nb), 256, 0, ctx->stream>>>(g.N, ld, e, X);
+        count_launch(ctx);
+        DFT_LAUNCH_CHECK();
+    }
+}
+
 void screened_poisson_vcycle(dft_context* ctx, const Grid& g, const double* src, int nb, double q2, double* x,
                              long long ld) {
     if (nb <= 0) return;

@@ -75,6 +75,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     eo.max_iterations = o.eig.max_iterations > 0 ? o.eig.max_iterations : 2000;
     eo.max_subspace = o.eig.max_subspace >= 2 ? o.eig.max_subspace : 3;
     eo.precond_steps = o.eig.preconditioner;
+    eo.precond_net = o.eig.preconditioner_net;
     eo.mixed_precision = o.eig.mixed_precision;
     eo.verbose = o.eig.verbose;
 

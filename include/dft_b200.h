@@ -165,9 +165,12 @@ typedef struct {
     int preconditioner;  /* 0: the reference's diagonal (theta - diag)^-1 (EigenvalueSolverMolecule.cpp:521-555);
                             k > 0: k damped-Jacobi smoothing steps on (T + sigma) t = r (default 4);
                             -1: one multigrid V(2,2) cycle on (T + sigma) t = r, all bands batched;
-                            -2: -1 on grids of 80^3 points or more, 4 below */
+                            -2: -1 on grids of 80^3 points or more, 4 below;
+                            -3: -1 plus the learned correction of preconditioner_net, trained by
+                                dft_pnet_train_preconditioner */
     int mixed_precision; /* 1: Gram products on the tensor cores (TF32 hi+lo split, FP32 accumulation)
                             until the occupied residuals fall below 1e-3, then FP64 to the end */
+    dft_pnet* preconditioner_net; /* the network of preconditioner -3 (not owned), else NULL */
 } dft_eig_opts;
 
 /* X (m x N, leading dimension ldx, device) = V (k x N, ldv, device) * Y (k x m, host,
@@ -398,6 +401,20 @@ typedef struct {
 /* Trains the network on the device with its own forward, backward and Adam kernels. */
 dft_status_t dft_pnet_train_poisson(dft_context* ctx, dft_pnet* net, const dft_pnet_train_opts* opts,
                                     dft_pnet_train_report* report);
+
+/* Learned Davidson preconditioner (replaces the diagonal correction of davidsonCorrection,
+ * reference EigenvalueSolverMolecule.cpp:521-555, as dft_eig_opts.preconditioner = -3).  The
+ * correction equation (T + sigma) t = r (T = -1/2 lap_h, sigma = max(-theta, 1 Ha)) gets one
+ * multigrid cycle, t0, and the network (the same 3-level BF16 U-Net, inputs 2 h^2 r / s and
+ * t0 / s with s = max |t0|) adds the remaining correction toward the equation's solution on the
+ * interior.  Training pairs come from the plain solver: the residual bands of a block
+ * eigensolve (nocc occupied of nbands) in the device potential V on grid g, their targets from
+ * opts->target_max_sweeps refined multigrid cycles; opts->samples residual bands are taken
+ * (the first opts->validation of them are held out).  report->val_loss is the network's
+ * error, report->val_loss_coarse that of the single cycle. */
+dft_status_t dft_pnet_train_preconditioner(dft_context* ctx, dft_pnet* net, const dft_grid* g, const double* V,
+                                           int nocc, int nbands, const dft_pnet_train_opts* opts,
+                                           dft_pnet_train_report* report);
 
 #ifdef __cplusplus
 }
