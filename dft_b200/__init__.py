@@ -47,7 +47,13 @@ class dft_scf_opts(C.Structure):
                 ("verbose", C.c_int), ("poisson_start", C.c_int), ("poisson_net", C.c_void_p), ("mixer", C.c_int),
                 ("pulay_depth", C.c_int), ("pulay_beta", C.c_double), ("adaptive_eig_tol", C.c_int),
                 ("smearing_kt", C.c_double), ("kerker_q0", C.c_double),
-                ("log_path", C.c_char_p), ("initial_density", C.c_int)]
+                ("log_path", C.c_char_p), ("autotune", C.c_int), ("initial_density", C.c_int)]
+
+
+class dft_autotune_report(C.Structure):
+    _fields_ = [("hpsi_bands_per_thread", C.c_int), ("hpsi_ms", C.c_double * 3),
+                ("jacobi_sweeps_per_launch", C.c_int), ("jacobi_us_per_sweep", C.c_double * 6),
+                ("cached", C.c_int)]
 
 
 # dft_poisson_start
@@ -120,6 +126,7 @@ _SIGS = {
     "dft_context_synchronize": ([_P], C.c_int),
     "dft_context_set_tuning": ([_P, C.c_char_p, C.c_long], C.c_int),
     "dft_context_stream": ([_P], C.c_void_p),
+    "dft_autotune": ([_P, C.POINTER(dft_grid), C.c_int, C.POINTER(dft_autotune_report)], C.c_int),
     "dft_context_launch_count": ([_P], C.c_longlong),
     "dft_context_counter": ([_P, C.c_char_p], C.c_longlong),
     "dft_device_alloc": ([_P, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
@@ -359,6 +366,15 @@ class Engine:
     @property
     def launches(self) -> int:
         return load().dft_context_launch_count(self.ctx)
+
+    def autotune(self, grid, nbands: int) -> dict:
+        """Times the bit-identical launch variants on this grid and keeps the fastest."""
+        g = grid.c()
+        r = dft_autotune_report()
+        _check(load().dft_autotune(self.ctx, C.byref(g), int(nbands), C.byref(r)))
+        return {"hpsi_bands_per_thread": r.hpsi_bands_per_thread, "hpsi_ms": list(r.hpsi_ms),
+                "jacobi_sweeps_per_launch": r.jacobi_sweeps_per_launch,
+                "jacobi_us_per_sweep": list(r.jacobi_us_per_sweep), "cached": bool(r.cached)}
 
     def counter(self, name: str) -> int:
         return load().dft_context_counter(self.ctx, name.encode())

@@ -37,6 +37,7 @@ SOURCES = {
     "poisson_start.cu": [],
     "precond_mg.cu": [],
     "atomic_start.cu": [],
+    "autotune.cu": [],
     "eigh.cpp": ["-Xcompiler", "-O3"],
 }
 

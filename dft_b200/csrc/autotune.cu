@@ -1,0 +1,124 @@
+// Launch-shape autotuner.  Several kernels here come in variants that give bit-identical
+// results and differ only in speed, which depends on the grid and the band count: the H psi
+// kernel marches 1, 2 or 4 bands per thread, and the Jacobi Poisson solve runs one sweep per
+// launch, 2/4/8 temporally blocked sweeps per launch, the whole solve in one persistent
+// cooperative launch, or the whole solve in the shared memory of a 16-block cluster.  The
+// autotuner times every variant on the caller's grid (CUDA events on the context's stream,
+// after one warm-up call each) and remembers the fastest per grid in the context; kernels on
+// that grid use it wherever the corresponding tuning knob is 0 (auto).  A repeated call for a
+// grid already tuned costs nothing.
+#include <algorithm>
+#include <vector>
+
+#include "ops.h"
+
+namespace dftb {
+
+namespace {
+
+struct Events {
+    cudaEvent_t a = nullptr, b = nullptr;
+    Events() {
+        DFT_CUDA(cudaEventCreate(&a));
+        DFT_CUDA(cudaEventCreate(&b));
+    }
+    ~Events() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+// milliseconds of fn() on the context's stream: one warm-up call, then the fastest of reps
+template <typename F>
+double time_ms(dft_context* ctx, Events& ev, int reps, F&& fn) {
+    fn();
+    sync(ctx);
+    double best = 1e300;
+    for (int r = 0; r < reps; ++r) {
+        DFT_CUDA(cudaEventRecord(ev.a, ctx->stream));
+        fn();
+        DFT_CUDA(cudaEventRecord(ev.b, ctx->stream));
+        DFT_CUDA(cudaEventSynchronize(ev.b));
+        float ms = 0.f;
+        DFT_CUDA(cudaEventElapsedTime(&ms, ev.a, ev.b));
+        best = std::min(best, (double)ms);
+    }
+    return best;
+}
+
+}  // namespace
+
+void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* rep) {
+    if (nbands < 1) fail(DFT_INVALID_ARGUMENT, "nbands must be >= 1");
+    dft_autotune_report r{};
+    const std::array<long long, 3> key{g.nx, g.ny, g.nz};
+    auto hit = ctx->tuned.find(key);
+    if (hit != ctx->tuned.end()) {
+        r.hpsi_bands_per_thread = hit->second[0];
+        r.jacobi_sweeps_per_launch = hit->second[1];
+        r.cached = 1;
+        if (rep) *rep = r;
+        return;
+    }
+    // the knobs are set per variant while timing and put back afterwards
+    const int keep_bpt = ctx->hpsi_bands_per_thread, keep_spl = ctx->jacobi_sweeps_per_launch;
+    struct Restore {
+        dft_context* c;
+        int b, s;
+        ~Restore() {
+            c->hpsi_bands_per_thread = b;
+            c->jacobi_sweeps_per_launch = s;
+        }
+    } restore{ctx, keep_bpt, keep_spl};
+    Events ev;
+    const long long N = g.N;
+    // timing buffers: at most 16 bands (the per-band cost is what differs), zero fields (the
+    // arithmetic of these kernels does not depend on the values)
+    const int tb = std::min(nbands, 16);
+    double* buf = nullptr;
+    DFT_CUDA(cudaMalloc(&buf, sizeof(double) * (size_t)N * (2 * tb + 3)));
+    struct Free {
+        double* p;
+        ~Free() {
+            if (p) cudaFree(p);
+        }
+    } free_buf{buf};
+    DFT_CUDA(cudaMemsetAsync(buf, 0, sizeof(double) * (size_t)N * (2 * tb + 3), ctx->stream));
+    double *V = buf, *psi = buf + N, *hpsi = psi + (size_t)tb * N, *rho = hpsi + (size_t)tb * N, *vh = rho + N;
+    // ---- H psi: bands per thread
+    const int bpt[3] = {1, 2, 4};
+    int best_bpt = 1;
+    double best = 1e300;
+    for (int i = 0; i < 3; ++i) {
+        if (bpt[i] > tb && i > 0) {
+            r.hpsi_ms[i] = -1.0;
+            continue;
+        }
+        ctx->hpsi_bands_per_thread = bpt[i];
+        r.hpsi_ms[i] = time_ms(ctx, ev, 3, [&] { apply_hamiltonian(ctx, g, V, psi, hpsi, tb, N); });
+        if (r.hpsi_ms[i] < best) best = r.hpsi_ms[i], best_bpt = bpt[i];
+    }
+    r.hpsi_bands_per_thread = best_bpt;
+    // ---- Jacobi: sweeps per launch; tol = 0 never stops, so each call runs exactly `sweeps`
+    const int spl[6] = {-2, -1, 1, 2, 4, 8};
+    const long sweeps = 64;
+    int best_spl = 1;
+    best = 1e300;
+    for (int i = 0; i < 6; ++i) {
+        ctx->jacobi_sweeps_per_launch = spl[i];
+        double ms = -1.0;
+        try {
+            ms = time_ms(ctx, ev, 2, [&] { hartree(ctx, g, rho, vh, 0.0, sweeps); });
+        } catch (const Error& e) {
+            if (e.status != DFT_INVALID_ARGUMENT) throw;  // the cluster variant does not fit this grid
+        }
+        r.jacobi_us_per_sweep[i] = ms < 0 ? -1.0 : 1e3 * ms / sweeps;
+        if (ms >= 0 && ms < best) best = ms, best_spl = spl[i];
+    }
+    r.jacobi_sweeps_per_launch = best_spl;
+    sync(ctx);
+    ctx->tuned[key] = {best_bpt, best_spl};
+    if (rep) *rep = r;
+}
+
+}  // namespace dftb

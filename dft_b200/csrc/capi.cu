@@ -152,6 +152,13 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
     });
 }
 
+dft_status_t dft_autotune(dft_context* ctx, const dft_grid* g, int nbands, dft_autotune_report* report) {
+    return guard(ctx, [&] {
+        NEED(ctx && g, "NULL argument");
+        dftb::autotune(ctx, dftb::make_grid(g), nbands, report);
+    });
+}
+
 void* dft_context_stream(dft_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 long long dft_context_launch_count(dft_context* ctx) { return ctx ? ctx->launches : 0; }
 

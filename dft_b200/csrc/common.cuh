@@ -4,7 +4,9 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdarg>
+#include <map>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -102,6 +104,9 @@ struct dft_context {
     int net_tensor_cores = 1;          // network convolutions on tcgen05 (1) or FP32 CUDA cores (0)
     int hpsi_bands_per_thread = 0;     // H psi bands per thread: 0 = auto, 1, 2 or 4
     long long grid_barrier_poll_limit = 0;  // persistent Jacobi barrier polls before giving up (0 = 2^24)
+    // autotuner choices per grid (nx, ny, nz) -> {H psi bands per thread, Jacobi sweeps per launch},
+    // used where the corresponding knob is 0 (auto)
+    std::map<std::array<long long, 3>, std::array<int, 2>> tuned;
     int radial_pivot_exp = -14;        // radial inverse iteration: |pivot| < 10^exp is singular
     // named scratch buffers (reductions, Jacobi ping-pong, XC intermediates, Davidson)
     dftb::Workspace ws[32];

@@ -234,7 +234,11 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
     dim3 block(HB_X, HB_Y);
     const int bx = (g.nx + HB_X - 1) / HB_X, by = (g.ny + HB_Y - 1) / HB_Y;
     // bands per thread: the "hpsi_bands_per_thread" tuning key, else 2 for blocks of 2 or more
-    int nbt = ctx->hpsi_bands_per_thread > 0 ? ctx->hpsi_bands_per_thread : (nbands >= 2 ? 2 : 1);
+    int nbt = ctx->hpsi_bands_per_thread;
+    if (nbt <= 0) {
+        auto t = ctx->tuned.find({(long long)g.nx, (long long)g.ny, (long long)g.nz});
+        nbt = t != ctx->tuned.end() ? t->second[0] : (nbands >= 2 ? 2 : 1);
+    }
     nbt = std::min(nbt, std::max(1, nbands));
     nbt = nbt >= 4 ? 4 : nbt >= 2 ? 2 : 1;
     const int groups = (nbands + nbt - 1) / nbt;
@@ -925,6 +929,10 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
     // launch shape: one persistent launch on small grids (launch-latency bound), one sweep per
     // launch otherwise; 2/4/8 select the temporally blocked kernel
     int tmax = ctx->jacobi_sweeps_per_launch;
+    if (tmax == 0) {
+        auto t = ctx->tuned.find({(long long)g.nx, (long long)g.ny, (long long)g.nz});
+        if (t != ctx->tuned.end()) tmax = t->second[1];
+    }
     if (tmax == 0 || tmax == -2) {
         JacobiResult r;
         if (hartree_cluster(ctx, g, rho, vh, tol, max_sweeps, &r)) return r;

@@ -127,6 +127,9 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
                    long long ld, bool init, double* eig_host, double* resid_host, const EigOpts& o,
                    const double* start = nullptr, int nstart = 0);
 
+// Launch-shape autotuner (autotune.cu): sets the context's H psi and Jacobi knobs for (g, nbands).
+void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* rep);
+
 // Molecular SCF (scf.cu).
 void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z, const double* xyz, int charge,
                   int multiplicity, int kind, const dft_scf_opts* opts, dft_scf_result* res);

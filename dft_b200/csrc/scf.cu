@@ -123,6 +123,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     for (int i = 0; i < na; ++i) occa[i] = 1.0;  // buildSpinOccupations: one electron per orbital
     for (int i = 0; i < nb; ++i) occb[i] = 1.0;
 
+    if (o.autotune) autotune(ctx, g, std::max(bands_a, bands_b), nullptr);
     nuclear_potential(ctx, g, nnuc, Z, xyz, vext.p);
     // NuclearRepulsion::calculate (NuclearRepulsion.cpp:6-54)
     double enn = 0.0;

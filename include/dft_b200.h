@@ -76,6 +76,23 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               factorisation below 10^value in magnitude is singular; the run's
  *                               status becomes DFT_SINGULAR (reference NumericalMethods.cpp:105-122). */
 dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long value);
+
+/* Autotuner (no reference counterpart): times every bit-identical launch variant of the H psi
+ * kernel (1, 2, 4 bands per thread, on min(nbands, 16) bands) and of the Jacobi Poisson solve
+ * (sweeps per launch -2, -1, 1, 2, 4, 8; 64 sweeps) on grid g with CUDA events on the context's
+ * stream and remembers the fastest of each for grid g in the context: kernels on g use it
+ * wherever the "hpsi_bands_per_thread" or "jacobi_sweeps_per_launch" knob is 0 (auto), and a
+ * second call for g times nothing.  report may be NULL; a time of -1 marks a variant that does
+ * not apply (e.g. a grid too large for the cluster-resident Jacobi).  Allocates
+ * (2 min(nbands,16) + 3) x N doubles while it runs. */
+typedef struct {
+    int hpsi_bands_per_thread;     /* chosen */
+    double hpsi_ms[3];             /* 1, 2, 4 bands per thread */
+    int jacobi_sweeps_per_launch;  /* chosen */
+    double jacobi_us_per_sweep[6]; /* -2, -1, 1, 2, 4, 8 */
+    int cached;                    /* 1: the choice was remembered, nothing was timed */
+} dft_autotune_report;
+dft_status_t dft_autotune(dft_context* ctx, const dft_grid* g, int nbands, dft_autotune_report* report);
 /* The cudaStream_t the context launches on, as an opaque handle (for event timing). */
 void* dft_context_stream(dft_context* ctx);
 /* Number of kernels this context has launched so far (diagnostics, bench accounting). */
@@ -248,6 +265,8 @@ typedef struct {
                                 spin) and a final {"result": ...} line, written to this file; the
                                 reference prints the same quantities as tables
                                 (MolecularSCFHelpers.cpp:251-513) */
+    int autotune;            /* 1: run dft_autotune for the grid and band count first (launch shapes
+                                only; results are bit-identical) */
     int initial_density;     /* 0: orbitals of the bare nuclear potential, as the reference
                                 (buildInitialMolecularDensities, MolecularSCFHelpers.cpp:515-579);
                                 1: superposed radial atoms of the same functional (batched radial

@@ -21,6 +21,7 @@ STRUCTS = {
     "dft_poisson_start_info": d.dft_poisson_start_info,
     "dft_pnet_train_opts": d.dft_pnet_train_opts,
     "dft_pnet_train_report": d.dft_pnet_train_report,
+    "dft_autotune_report": d.dft_autotune_report,
 }
 
 
