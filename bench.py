@@ -38,9 +38,12 @@ from dft_b200 import systems  # noqa: E402
 
 # The H2 48^3 system is the one the reference itself can run to convergence on a CPU
 # (about 4 minutes to |dE| < 1e-6); H2O 128^3 (PBE96, 12 bands) is the larger molecule.
-WORKLOADS = {"h2_48": systems.h2_48(), "h2o_128": systems.h2o_128()}
+WORKLOADS = {"h2_48": systems.h2_48(), "h2o_128": systems.h2o_128(), "cluster20": systems.cluster()}
 for _w in WORKLOADS.values():
     _w["desc"] += ", Jacobi tol 1e-8 (cap 10000, cold start), stop |dE|<1e-6"
+# the 20-atom cluster: Kerker-screened Pulay mixing and the superposed-atoms start (the plain
+# FP64 method takes over an hour there; pass --no-plain)
+WORKLOADS["cluster20"]["fast_options"] = {"kerker_q0": 0.8, "initial_density": 1}
 
 
 def load_peaks():
@@ -113,7 +116,7 @@ def molecule(w):
     return m
 
 
-def scf_options(w, fast=False, net=None):
+def scf_options(w, fast=False, net=None, extra=None):
     """plain: the reference's method in FP64 (cold-start Jacobi, FP64 eigensolver).
     fast: multigrid cycles from the previous potential (the learned start for each density
     slot's first solve) before the same Jacobi stop rule, the mixed-precision eigensolver
@@ -123,9 +126,11 @@ def scf_options(w, fast=False, net=None):
     import dft_b200
     if not fast:
         return dft_b200.default_scf_options(stop_abs_de=1e-6, extra_bands=w["extra_bands"])
-    o = dft_b200.default_scf_options(stop_abs_de=1e-6, extra_bands=w["extra_bands"],
-                                     poisson_start=dft_b200.POISSON_MULTIGRID, eig_mixed_precision=1,
-                                     eig_preconditioner=-2, mixer=1, adaptive_eig_tol=1)
+    kw = dict(stop_abs_de=1e-6, extra_bands=w["extra_bands"], poisson_start=dft_b200.POISSON_MULTIGRID,
+              eig_mixed_precision=1, eig_preconditioner=-2, mixer=1, adaptive_eig_tol=1)
+    kw.update(w.get("fast_options", {}))
+    kw.update(extra or {})
+    o = dft_b200.default_scf_options(**kw)
     if net is not None:
         o.poisson_net = net.handle
     return o
@@ -431,6 +436,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ablation", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 and FP64-oracle SCF runs")
+    ap.add_argument("--fast-options", default="{}", help="JSON: extra options of the fast configuration")
     ap.add_argument("--ablation-workload", default="h2o_128", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
@@ -455,7 +462,7 @@ def main():
     g = dft_b200.CartesianGrid(*w["n"], *w["bounds"])
     mol = molecule(w)
     net, train_info = train_network(eng, w)
-    fast = scf_options(w, fast=True, net=net)
+    fast = scf_options(w, fast=True, net=net, extra=json.loads(args.fast_options))
     plain = scf_options(w)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -507,18 +514,37 @@ def main():
         eng.scf_molecule(g, mol, 0, w["multiplicity"], w["functional"], fast, want_density=True)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_val = world / (statistics.median(e2e_ms) * 1e-3)
-    # the plain FP64 method (the reference's algorithm) on the same GPU, for the comparison
-    plain_steps = max(1, min(args.steps, w.get("plain_steps", 3)))
-    plain_total, _, plain_res, _ = run(plain, 1, plain_steps)
-    plain_ms = plain_total / plain_steps
+    # the plain FP64 method (the reference's algorithm) on the same GPU, for the comparison, and
     # the plain method with a Poisson stop that bounds the potential's error (the reference's
     # max|dV| < 1e-8 stops ~1e-8/(1 - rho) away from the Jacobi fixed point): the FP64 oracle
-    # run for the energy error of the fast configuration
-    import dft_b200 as _d
-    tight = _d.default_scf_options(stop_abs_de=1e-9, extra_bands=w["extra_bands"],
-                                   poisson_start=_d.POISSON_MULTIGRID, poisson_tol=jacobi_tight_tol(w),
-                                   poisson_max_sweeps=400000)
-    tight_total, _, tight_res, _ = run(tight, 0, 1)
+    # run for the energy and eigenvalue errors of the fast configuration
+    cmp = {}
+    if not args.no_plain:
+        import dft_b200 as _d
+        plain_steps = max(1, min(args.steps, w.get("plain_steps", 3)))
+        plain_total, _, plain_res, _ = run(plain, 1, plain_steps)
+        plain_ms = plain_total / plain_steps
+        tight = _d.default_scf_options(stop_abs_de=1e-9, extra_bands=w["extra_bands"],
+                                       poisson_start=_d.POISSON_MULTIGRID, poisson_tol=jacobi_tight_tol(w),
+                                       poisson_max_sweeps=400000)
+        tight_total, _, tight_res, _ = run(tight, 0, 1)
+        pr, tr, fr = plain_res[-1], tight_res[-1], results[-1]
+        cmp = {"plain_fp64": {"ms_per_step": plain_ms, "steps": plain_steps, "energy": pr.total,
+                              "scf_iterations": pr.iterations,
+                              "poisson_sweeps": sum(h["poisson_sweeps_in"] + h["poisson_sweeps_out"]
+                                                    for h in pr.history),
+                              "phase_ms": {k: round(sum(h[k] for h in pr.history), 2)
+                                           for k in ("ms_hartree", "ms_xc", "ms_orbitals", "ms_density",
+                                                     "ms_energy")}},
+               "speedup_vs_plain_fp64": plain_ms / (total_ms / args.steps),
+               "energy_delta_vs_plain_fp64": fr.total - pr.total,
+               "plain_fp64_tight_poisson": {"ms": tight_total, "energy": tr.total, "poisson_tol": jacobi_tight_tol(w),
+                                            "scf_iterations": tr.iterations},
+               "energy_error_vs_tight": fr.total - tr.total,
+               "eigenvalue_error_vs_tight": float(np.max(np.abs(np.array(fr.eigenvalues) - np.array(tr.eigenvalues)))),
+               "plain_energy_error_vs_tight": pr.total - tr.total,
+               "plain_eigenvalue_error_vs_tight": float(np.max(np.abs(np.array(pr.eigenvalues) -
+                                                                      np.array(tr.eigenvalues))))}
 
     N = g.getSize()
     h2d = len(w["Z"]) * (4 + 24)
@@ -551,24 +577,7 @@ def main():
                              "tolerance following the density change",
                    "poisson_sweeps": sum(h["poisson_sweeps_in"] + h["poisson_sweeps_out"] for h in last.history),
                    "network": train_info,
-                   "plain_fp64": {"ms_per_step": plain_ms, "steps": plain_steps, "energy": plain_res[-1].total,
-                                  "scf_iterations": plain_res[-1].iterations,
-                                  "poisson_sweeps": sum(h["poisson_sweeps_in"] + h["poisson_sweeps_out"]
-                                                        for h in plain_res[-1].history),
-                                  "phase_ms": {k: round(sum(h[k] for h in plain_res[-1].history), 2)
-                                               for k in ("ms_hartree", "ms_xc", "ms_orbitals", "ms_density",
-                                                         "ms_energy")}},
-                   "speedup_vs_plain_fp64": plain_ms / ms_per_step,
-                   "energy_delta_vs_plain_fp64": last.total - plain_res[-1].total,
-                   "plain_fp64_tight_poisson": {"ms": tight_total, "energy": tight_res[-1].total,
-                                                "poisson_tol": jacobi_tight_tol(w),
-                                                "scf_iterations": tight_res[-1].iterations},
-                   "energy_error_vs_tight": last.total - tight_res[-1].total,
-                   "eigenvalue_error_vs_tight": float(np.max(np.abs(np.array(last.eigenvalues) -
-                                                                    np.array(tight_res[-1].eigenvalues)))),
-                   "plain_eigenvalue_error_vs_tight": float(np.max(np.abs(np.array(plain_res[-1].eigenvalues) -
-                                                                          np.array(tight_res[-1].eigenvalues)))),
-                   "plain_energy_error_vs_tight": plain_res[-1].total - tight_res[-1].total},
+                   **cmp},
         "gpu_launches": launches,
         "e2e": {"value": e2e_val, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": "gram_small_kernel (FP64 Gram of the eigensolver, one launch)",

@@ -33,36 +33,91 @@ __device__ __forceinline__ double nb_sum_open(const Grid& g, const double* v, lo
     return s;
 }
 
+// Fine-level kernels march z over a column (i, j) per thread, like the H psi kernel: the z
+// neighbours come from registers and no point index is divided.  blockIdx.z = band * nzc + chunk.
+constexpr int PX = 32, PY = 8;
+
 // out = v + omega ((sum + s src) / (den + c) - v); v == nullptr means v = 0
-__global__ void pc_smooth_kernel(Grid g, long long ld, const double* __restrict__ src, double s,
-                                 const double* __restrict__ shift, const double* __restrict__ v,
-                                 double* __restrict__ out, double omega) {
-    const int a = blockIdx.y;
+__global__ void __launch_bounds__(PX* PY) pc_smooth_kernel(Grid g, long long ld, const double* __restrict__ src,
+                                                          double s, const double* __restrict__ shift,
+                                                          const double* __restrict__ v, double* __restrict__ out,
+                                                          double omega, int zc, int nzc) {
+    const int i = blockIdx.x * PX + threadIdx.x, j = blockIdx.y * PY + threadIdx.y;
+    const int a = blockIdx.z / nzc, kc = blockIdx.z - a * nzc;
+    if (i >= g.nx || j >= g.ny) return;
     const double d = 2.0 * (g.ix2 + g.iy2 + g.iz2) + shift[a];
     const double* sa = src + (long long)a * ld;
-    const double* va = v ? v + (long long)a * ld : nullptr;
     double* oa = out + (long long)a * ld;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
-        if (!va) {
-            oa[p] = omega * s * sa[p] / d;
-        } else {
-            const double vj = (nb_sum_open(g, va, p) + s * sa[p]) / d;
-            oa[p] = va[p] + omega * (vj - va[p]);
-        }
+    const long long sxy = (long long)g.nx * g.ny;
+    const int kb = kc * zc, ke = min(g.nz, kb + zc);
+    long long p = (long long)kb * sxy + (long long)j * g.nx + i;
+    if (!v) {
+        for (int k = kb; k < ke; ++k, p += sxy) oa[p] = omega * s * sa[p] / d;
+        return;
+    }
+    const double* va = v + (long long)a * ld;
+    const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+    double below = kb > 0 ? va[p - sxy] : 0.0, cur = va[p];
+    for (int k = kb; k < ke; ++k, p += sxy) {
+        const double above = k + 1 < g.nz ? va[p + sxy] : 0.0;
+        double sum = g.iz2 * (below + above);
+        if (xl) sum += g.ix2 * va[p - 1];
+        if (xr) sum += g.ix2 * va[p + 1];
+        if (yl) sum += g.iy2 * va[p - g.nx];
+        if (yr) sum += g.iy2 * va[p + g.nx];
+        const double vj = (sum + s * sa[p]) / d;
+        oa[p] = cur + omega * (vj - cur);
+        below = cur;
+        cur = above;
     }
 }
 
 // r = s src - ((den + c) v - sum)
-__global__ void pc_residual_kernel(Grid g, long long ld, const double* __restrict__ src, double s,
-                                   const double* __restrict__ shift, const double* __restrict__ v,
-                                   double* __restrict__ r) {
-    const int a = blockIdx.y;
+__global__ void __launch_bounds__(PX* PY) pc_residual_kernel(Grid g, long long ld, const double* __restrict__ src,
+                                                            double s, const double* __restrict__ shift,
+                                                            const double* __restrict__ v, double* __restrict__ r,
+                                                            int zc, int nzc) {
+    const int i = blockIdx.x * PX + threadIdx.x, j = blockIdx.y * PY + threadIdx.y;
+    const int a = blockIdx.z / nzc, kc = blockIdx.z - a * nzc;
+    if (i >= g.nx || j >= g.ny) return;
     const double d = 2.0 * (g.ix2 + g.iy2 + g.iz2) + shift[a];
     const double* sa = src + (long long)a * ld;
     const double* va = v + (long long)a * ld;
     double* ra = r + (long long)a * ld;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x)
-        ra[p] = s * sa[p] - (d * va[p] - nb_sum_open(g, va, p));
+    const long long sxy = (long long)g.nx * g.ny;
+    const int kb = kc * zc, ke = min(g.nz, kb + zc);
+    long long p = (long long)kb * sxy + (long long)j * g.nx + i;
+    const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+    double below = kb > 0 ? va[p - sxy] : 0.0, cur = va[p];
+    for (int k = kb; k < ke; ++k, p += sxy) {
+        const double above = k + 1 < g.nz ? va[p + sxy] : 0.0;
+        double sum = g.iz2 * (below + above);
+        if (xl) sum += g.ix2 * va[p - 1];
+        if (xr) sum += g.ix2 * va[p + 1];
+        if (yl) sum += g.iy2 * va[p - g.nx];
+        if (yr) sum += g.iy2 * va[p + g.nx];
+        ra[p] = s * sa[p] - (d * cur - sum);
+        below = cur;
+        cur = above;
+    }
+}
+
+// launch shape of the column kernels for nb fields: z chunks long enough to amortise the march,
+// enough blocks to fill the machine; gridDim.z = nb * nzc must stay below 65536
+struct ColShape {
+    dim3 grid, block;
+    int zc, nzc;
+};
+ColShape col_shape(dft_context* ctx, const Grid& g, int nb) {
+    const int bx = (g.nx + PX - 1) / PX, by = (g.ny + PY - 1) / PY;
+    int zc = 32;
+    while (zc > 4 && (long long)bx * by * nb * ((g.nz + zc - 1) / zc) < 4LL * ctx->num_sms) zc >>= 1;
+    int nzc = (g.nz + zc - 1) / zc;
+    while ((long long)nb * nzc > 65535) {
+        zc *= 2;
+        nzc = (g.nz + zc - 1) / zc;
+    }
+    return {dim3(bx, by, nb * nzc), dim3(PX, PY), zc, nzc};
 }
 
 // Restriction along one axis (transposed trilinear weights times h/H), per band.
@@ -190,9 +245,10 @@ inline dim3 pc_grid(dft_context* ctx, long long n, int nb) {
 }
 
 void pc_smooth(dft_context* ctx, PCLevel& l, double s, const double* shift, int nb, int n, bool from_zero) {
+    const ColShape c = col_shape(ctx, l.g, nb);
     for (int k = 0; k < n; ++k) {
         const double* v = (from_zero && k == 0) ? nullptr : l.v;
-        pc_smooth_kernel<<<pc_grid(ctx, l.g.N, nb), 256, 0, ctx->stream>>>(l.g, l.ld, l.src, s, shift, v, l.tmp, 0.8);
+        pc_smooth_kernel<<<c.grid, c.block, 0, ctx->stream>>>(l.g, l.ld, l.src, s, shift, v, l.tmp, 0.8, c.zc, c.nzc);
         std::swap(l.v, l.tmp);
     }
     count_launch(ctx, n);
@@ -207,7 +263,10 @@ void pc_vcycle(dft_context* ctx, std::vector<PCLevel>& L, size_t i, double s, co
         return;
     }
     pc_smooth(ctx, l, s, shift, nb, 2, true);
-    pc_residual_kernel<<<pc_grid(ctx, l.g.N, nb), 256, 0, ctx->stream>>>(l.g, l.ld, l.src, s, shift, l.v, l.res);
+    {
+        const ColShape c = col_shape(ctx, l.g, nb);
+        pc_residual_kernel<<<c.grid, c.block, 0, ctx->stream>>>(l.g, l.ld, l.src, s, shift, l.v, l.res, c.zc, c.nzc);
+    }
     PCLevel& c = L[i + 1];
     const Grid& f = l.g;
     pc_restrict_axis_kernel<<<pc_grid(ctx, (long long)f.nz * f.ny * c.g.nx, nb), 256, 0, ctx->stream>>>(
@@ -329,7 +388,8 @@ void helmholtz_refine(dft_context* ctx, const Grid& g, const double* R, int nb, 
     vcycle_batch(ctx, g, R, nullptr, nb, shift, 2.0, X, ld);
     for (int c = 1; c < cycles; ++c) {
         // res = 2 R - ((den + 2 sigma) X - sum), the equation's residual in the cycle's scaling
-        pc_residual_kernel<<<pc_grid(ctx, g.N, nb), 256, 0, ctx->stream>>>(g, ld, R, 2.0, shift, X, res);
+        const ColShape cs = col_shape(ctx, g, nb);
+        pc_residual_kernel<<<cs.grid, cs.block, 0, ctx->stream>>>(g, ld, R, 2.0, shift, X, res, cs.zc, cs.nzc);
         count_launch(ctx);
         vcycle_batch(ctx, g, res, nullptr, nb, shift, 1.0, e, ld);
         pc_add_kernel<<<pc_grid(ctx, g.N, nb), 256, 0, ctx->stream>>>(g.N, ld, e, X);

@@ -609,6 +609,8 @@ void radial_atom_tables(dft_context* ctx, int nz, const int* Z, int kind, long p
         for (int q = 0; q < sp.norb; ++q) {
             if (sp.spin[q] != 0) continue;  // the alpha shells: every occupied (n, l) of the atom
             const int k = (int)shells[rr].size();
+            if (k >= RADIAL_MAX_SHELLS) fail(DFT_INVALID_ARGUMENT, "atom Z = %d has more than %d shells", Z[rr],
+                                             RADIAL_MAX_SHELLS);
             DFT_CUDA(cudaMemcpyAsync(orbs + ((long long)rr * RADIAL_MAX_SHELLS + k) * points,
                                      base + (long long)(A_COUNT + q * O_COUNT + O_U) * points,
                                      sizeof(double) * points, cudaMemcpyDeviceToDevice, ctx->stream));
