@@ -251,6 +251,185 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NC));
 }
 
+// Ring variant of the Gram tile (tuning key "tensor_core_ring"): the FP64 slices are staged
+// into a 2-deep shared-memory ring with cp.async (16-byte chunks, zero-filled past the ends),
+// so two slices are in flight per block without holding them in registers; each slice is
+// then split from shared memory into the TF32 hi/lo planes of one operand buffer (the same
+// core-matrix layout and MMAs as gram_tc_kernel).  Needs even leading dimensions and
+// 16-byte-aligned A and B; NC <= 128.
+constexpr int TR_STAGES = 2;
+constexpr int TR_RS = 36;  // doubles per staged row: 32 points + 4 of padding (fewer bank conflicts)
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+template <int NC>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    gram_tc_ring_kernel(const double* __restrict__ A, long long lda, int ka, const double* __restrict__ B,
+                        long long ldb, int kb, int nt, long long n, long long chunk, double* __restrict__ partial,
+                        int* __restrict__ error) {
+    extern __shared__ __align__(1024) uint32_t sm[];
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t bar;
+    constexpr int NW = TC_THREADS / 32;
+    constexpr int RA = TC_M / NW, RB = NC / NW;
+    constexpr int ROWS = TC_M + NC;
+    constexpr int a_words = TC_M * TC_KT, b_words = NC * TC_KT;
+    uint32_t* ahi = sm;  // one operand buffer: A hi, A lo, B hi, B lo
+    uint32_t* alo = ahi + a_words;
+    uint32_t* bhi = alo + a_words;
+    uint32_t* blo = bhi + b_words;
+    double* raw = reinterpret_cast<double*>(blo + b_words);  // TR_STAGES x ROWS x TR_RS
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TC_M, n0 = blockIdx.y * nt;
+    const int mrows = min(TC_M, ka - m0), nrows = min(nt, kb - n0);
+    const long long p0 = (long long)blockIdx.z * chunk, p1 = min(n, p0 + chunk);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(NC));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = idesc_tf32(NC);
+    // stage the slice starting at point ps into ring slot st: ROWS x 16 chunks of 2 doubles
+    auto stage = [&](long long ps, int st) {
+        double* dst0 = raw + (size_t)st * ROWS * TR_RS;
+        for (int c = tid; c < ROWS * 16; c += TC_THREADS) {
+            const int row = c >> 4, q = c & 15;
+            const long long pt = ps + 2 * q;
+            const double* base;
+            bool valid;
+            if (row < TC_M) {
+                valid = row < mrows;
+                base = A + (long long)(m0 + (valid ? row : 0)) * lda;
+            } else {
+                valid = row - TC_M < nrows;
+                base = B + (long long)(n0 + (valid ? row - TC_M : 0)) * ldb;
+            }
+            const long long left = p1 - pt;  // doubles left in this block's range
+            const uint32_t bytes = (!valid || left <= 0) ? 0u : (left >= 2 ? 16u : 8u);
+            cp_async16(smem_u32(dst0 + (size_t)row * TR_RS + 2 * q), bytes ? base + pt : base, bytes);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const int nsteps = (int)((p1 - p0 + TC_KT - 1) / TC_KT);
+    for (int s0 = 0; s0 < TR_STAGES; ++s0) {
+        if (s0 < nsteps) stage(p0 + (long long)s0 * TC_KT, s0);
+        else asm volatile("cp.async.commit_group;" ::: "memory");  // keep the group count uniform
+    }
+    bool ok = true;
+    uint32_t phase = 0;
+    bool pending = false;
+    const int lr = lane >> 2, lk = lane & 3;
+    for (int step = 0; step < nsteps; ++step) {
+        const int st = step % TR_STAGES;
+        // slice `step` has landed (at most TR_STAGES - 1 younger groups still in flight)
+        asm volatile("cp.async.wait_group %0;" ::"n"(TR_STAGES - 1) : "memory");
+        // the MMAs of the previous slice must be done before the operand buffer is rewritten;
+        // after a timed-out wait they count as still in flight (waited for again below)
+        if (pending) {
+            if (mbar_wait(&bar, phase)) {
+                phase ^= 1;
+                pending = false;
+            } else {
+                ok = false;
+            }
+        }
+        if (!__syncthreads_and(ok)) break;
+        const double* src = raw + (size_t)st * ROWS * TR_RS;
+#pragma unroll
+        for (int i = 0; i < RA; ++i) {
+            const int cm = warp + i * NW, r = (cm >> 3) * 8 + lr, pt = (cm & 7) * 4 + lk;
+            const double x = src[(size_t)r * TR_RS + pt];
+            const uint32_t h = to_tf32((float)x);
+            const uint32_t l = to_tf32((float)(x - (double)__uint_as_float(h)));
+            const int o = (((cm & 7) * (TC_M / 8) + (cm >> 3)) << 5) + lane;
+            ahi[o] = h;
+            alo[o] = l;
+        }
+#pragma unroll
+        for (int i = 0; i < RB; ++i) {
+            const int cm = warp + i * NW, r = (cm >> 3) * 8 + lr, pt = (cm & 7) * 4 + lk;
+            const double x = src[(size_t)(TC_M + r) * TR_RS + pt];
+            const uint32_t h = to_tf32((float)x);
+            const uint32_t l = to_tf32((float)(x - (double)__uint_as_float(h)));
+            const int o = (((cm & 7) * (NC / 8) + (cm >> 3)) << 5) + lane;
+            bhi[o] = h;
+            blo[o] = l;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            constexpr uint32_t lbo_a = (TC_M / 8) * 128, lbo_b = (uint32_t)(NC / 8) * 128, sbo = 128;
+            const uint32_t sa_hi = smem_u32(ahi), sa_lo = smem_u32(alo), sb_hi = smem_u32(bhi), sb_lo = smem_u32(blo);
+#pragma unroll
+            for (int kk = 0; kk < TC_KT / 8; ++kk) {
+                const uint32_t oa = kk * 2 * lbo_a, ob = kk * 2 * lbo_b;
+                const uint64_t dah = smem_desc(sa_hi + oa, lbo_a, sbo), dal = smem_desc(sa_lo + oa, lbo_a, sbo);
+                const uint64_t dbh = smem_desc(sb_hi + ob, lbo_b, sbo), dbl = smem_desc(sb_lo + ob, lbo_b, sbo);
+                const uint32_t first = (step == 0 && kk == 0) ? 0u : 1u;
+                mma_tf32(tmem, dah, dbh, idesc, first);
+                mma_tf32(tmem, dah, dbl, idesc, 1u);
+                mma_tf32(tmem, dal, dbh, idesc, 1u);
+            }
+            mma_commit(&bar);
+        }
+        pending = true;
+        // the ring slot just converted is free: stage the slice TR_STAGES ahead into it (every
+        // thread has passed the barrier above, so no one still reads it)
+        if (step + TR_STAGES < nsteps) stage(p0 + (long long)(step + TR_STAGES) * TC_KT, st);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    // drain (bounded): the last MMAs, or a second wait for the ones that timed out above
+    if (pending && !mbar_wait(&bar, phase)) ok = false;
+    ok = __syncthreads_and(ok);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (tid == 0) atomicExch(error, 1);
+    } else if (nsteps > 0) {
+        double* out = partial + (long long)blockIdx.z * ka * kb;
+        const int q4 = warp & 3, half = warp >> 2;
+        const int row = q4 * 32 + lane;
+        constexpr int CH = NC / (NW / 4);
+        for (int c0 = half * CH; c0 < half * CH + CH; c0 += 8) {
+            uint32_t v[8];
+            const uint32_t addr = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7])
+                         : "r"(addr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < mrows)
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (c0 + q < nrows) out[(long long)(m0 + row) * kb + (n0 + c0 + q)] = (double)__uint_as_float(v[q]);
+        }
+    } else {
+        double* out = partial + (long long)blockIdx.z * ka * kb;
+        for (int e = tid; e < mrows * nrows; e += TC_THREADS)
+            out[(long long)(m0 + e / nrows) * kb + (n0 + e % nrows)] = 0.0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NC));
+}
+
+template <int NC>
+constexpr size_t ring_smem() {
+    return sizeof(uint32_t) * (2 * TC_M * TC_KT + 2 * NC * TC_KT) +
+           sizeof(double) * (size_t)TR_STAGES * (TC_M + NC) * TR_RS;
+}
+
 __global__ void gram_tc_reduce_kernel(int nchunks, int nel, const double* __restrict__ partial, double scale,
                                       double* __restrict__ out) {
     const int lane = threadIdx.x & 31;
@@ -439,7 +618,29 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
     }
     DFT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
     const dim3 grid(mtiles, ntiles, (unsigned)nch);
-    switch (ncols) {
+    const bool ring = ctx->tc_ring && ncols <= 128 && lda % 2 == 0 && ldb % 2 == 0 &&
+                      ((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0;
+    if (ring) {
+        static bool rattr = false;
+        if (!rattr) {
+            DFT_CUDA(cudaFuncSetAttribute(gram_tc_ring_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)ring_smem<32>()));
+            DFT_CUDA(cudaFuncSetAttribute(gram_tc_ring_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)ring_smem<64>()));
+            DFT_CUDA(cudaFuncSetAttribute(gram_tc_ring_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)ring_smem<128>()));
+            rattr = true;
+        }
+        if (ncols == 32)
+            gram_tc_ring_kernel<32><<<grid, TC_THREADS, ring_smem<32>(), ctx->stream>>>(A, lda, ka, B, ldb, kb, nt, g.N,
+                                                                                       chunk, partial, err);
+        else if (ncols == 64)
+            gram_tc_ring_kernel<64><<<grid, TC_THREADS, ring_smem<64>(), ctx->stream>>>(A, lda, ka, B, ldb, kb, nt, g.N,
+                                                                                       chunk, partial, err);
+        else
+            gram_tc_ring_kernel<128><<<grid, TC_THREADS, ring_smem<128>(), ctx->stream>>>(A, lda, ka, B, ldb, kb, nt,
+                                                                                         g.N, chunk, partial, err);
+    } else switch (ncols) {
         case 32:
             gram_tc_kernel<32><<<grid, TC_THREADS, smem, ctx->stream>>>(A, lda, ka, B, ldb, kb, nt, g.N, chunk,
                                                                         partial, err);

@@ -69,6 +69,10 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               BF16 rounding, not bit for bit).
  *   "hpsi_bands_per_thread":    0 = auto (default), 1, 2 or 4 bands marched together by each
  *                               thread of the H psi kernel (results identical for every value).
+ *   "tensor_core_ring":         0 (default) = the tensor-core Gram product stages its FP64 slices
+ *                               through registers; 1 = through a 2-deep cp.async shared-memory
+ *                               ring (even leading dimensions, 16-byte-aligned blocks, <= 128
+ *                               columns per tile; otherwise the register path).  Same results.
  *   "grid_barrier_poll_limit":  0 = 2^24 (default): polls a block of the persistent Jacobi
  *                               launch makes at a grid barrier before it gives up; the solve then
  *                               fails with DFT_CUDA_ERROR and the context stays usable.

@@ -13,9 +13,19 @@ from oracle.bindings import PZ81  # noqa: F401
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=[0, 1], ids=["regs", "ring"])
+def tc_ring(request, engine):
+    """Both staging variants of the tensor-core Gram product (register prefetch, cp.async ring);
+    shapes the ring does not take (odd leading dimension, > 128 columns) fall back."""
+    engine.set_tuning("tensor_core_ring", request.param)
+    yield request.param
+    engine.set_tuning("tensor_core_ring", 0)
+
+
 @pytest.mark.parametrize("ka,kb,n", [(12, 12, (40, 40, 40)), (50, 70, (64, 48, 33)), (130, 300, (32, 32, 40)),
-                                     (200, 69, (48, 48, 48)), (1, 3, (5, 7, 9))])
-def test_gram_tensor_cores_vs_fp64(engine, ka, kb, n):
+                                     (200, 69, (48, 48, 48)), (1, 3, (5, 7, 9)), (129, 127, (33, 29, 41)),
+                                     (207, 69, (96, 96, 96))])
+def test_gram_tensor_cores_vs_fp64(engine, ka, kb, n, tc_ring):
     g = dft_b200.CartesianGrid(*n, -3.0, 3.0, -2.0, 2.5, -1.5, 1.7)
     N = g.getSize()
     rng = np.random.default_rng(ka * 1000 + kb)
@@ -31,7 +41,7 @@ def test_gram_tensor_cores_vs_fp64(engine, ka, kb, n):
     assert np.max(np.abs(ctc - c64)) < 1e-5 * np.max(np.abs(c64))
 
 
-def test_mixed_precision_eigensolver(engine, port):
+def test_mixed_precision_eigensolver(engine, port, tc_ring):
     n, b = (32, 30, 28), (-5.0, 5.0, -4.6, 4.6, -4.2, 4.2)
     g = dft_b200.CartesianGrid(*n, *b)
     N = g.getSize()
@@ -61,3 +71,27 @@ def test_rotation_tensor_cores_vs_fp64(engine, k, m, n):
     a, b = X64.to_host((m, N)), Xtc.to_host((m, N))
     assert np.max(np.abs(a - ref)) < 1e-11 * np.max(np.abs(ref))
     assert np.max(np.abs(b - a)) < 2e-6 * np.max(np.abs(a))
+
+
+def test_gram_ring_padded_rows_odd_points(engine):
+    """Odd point count with an even leading dimension: the ring's last 16-byte chunk carries one
+    point and a NaN in the padding, which must not be read."""
+    n = (33, 29, 41)
+    g = dft_b200.CartesianGrid(*n, -3.0, 3.0, -2.0, 2.5, -1.5, 1.7)
+    N = g.getSize()
+    assert N % 2 == 1
+    ld = N + 1
+    rng = np.random.default_rng(7)
+    A = np.full((20, ld), np.nan)
+    B = np.full((24, ld), np.nan)
+    A[:, :N] = rng.standard_normal((20, N))
+    B[:, :N] = rng.standard_normal((24, N))
+    dA, dB = engine.upload(A), engine.upload(B)
+    c64 = engine.gram(g, dA, ld, 20, dB, ld, 24, precision=0)
+    try:
+        engine.set_tuning("tensor_core_ring", 1)
+        ctc = engine.gram(g, dA, ld, 20, dB, ld, 24, precision=1)
+    finally:
+        engine.set_tuning("tensor_core_ring", 0)
+    assert np.all(np.isfinite(ctc))
+    assert np.max(np.abs(ctc - c64)) < 1e-5 * np.max(np.abs(c64))
