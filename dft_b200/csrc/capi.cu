@@ -113,6 +113,7 @@ dft_status_t dft_context_destroy(dft_context* ctx) {
             if (w.ptr) cudaFree(w.ptr);
         if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
         if (ctx->gram_ticket) cudaFree(ctx->gram_ticket);
+        for (auto& kv : ctx->mg_graphs) cudaGraphExecDestroy(kv.second.exec);
         cudaStreamDestroy(ctx->stream);
     });
     delete ctx;
@@ -143,6 +144,9 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
         } else if (k == "radial_pivot_exponent") {
             NEED(value >= -300 && value <= 300, "radial_pivot_exponent must be in [-300, 300]");
             ctx->radial_pivot_exp = (int)value;
+        } else if (k == "multigrid_graphs") {
+            NEED(value == 0 || value == 1, "multigrid_graphs must be 0 or 1");
+            ctx->multigrid_graphs = (int)value;
         } else if (k == "tensor_core_ring") {
             NEED(value == 0 || value == 1, "tensor_core_ring must be 0 or 1");
             ctx->tc_ring = (int)value;

@@ -93,6 +93,13 @@ struct Workspace {
 
 }  // namespace dftb
 
+// captured multigrid cycles (poisson_start.cu), keyed by grid and buffer addresses
+using MGGraphKey = std::array<long long, 6>;
+struct MGGraph {
+    cudaGraphExec_t exec;
+    long long launches;  // kernels per replay
+};
+
 struct dft_context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -108,6 +115,8 @@ struct dft_context {
     // autotuner choices per grid (nx, ny, nz) -> {H psi bands per thread, Jacobi sweeps per launch},
     // used where the corresponding knob is 0 (auto)
     std::map<std::array<long long, 3>, std::array<int, 2>> tuned;
+    int multigrid_graphs = 1;                 // replay captured multigrid cycles (1) or launch directly (0)
+    std::map<MGGraphKey, MGGraph> mg_graphs;  // the captured cycles
     int radial_pivot_exp = -14;        // radial inverse iteration: |pivot| < 10^exp is singular
     // named scratch buffers (reductions, Jacobi ping-pong, XC intermediates, Davidson)
     dftb::Workspace ws[32];

@@ -460,12 +460,10 @@ int multigrid(dft_context* ctx, const Grid& g, const double* rho, double* v, dou
     L[0].src = const_cast<double*>(rho);
     L[0].v = v;
     unsigned long long* rmax = (unsigned long long*)(slab + 8);
-    double* h = pinned(ctx, 1);
     const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
     const double fourpi = 4.0 * 3.14159265358979323846;
-    int c = 0;
-    double r = 0.0;
-    for (c = 1; c <= max_cycles; ++c) {
+    // one cycle: the V-cycle, then the residual's max norm into rmax
+    auto cycle = [&] {
         vcycle(ctx, L, 0, fourpi);
         if (L[0].v != v) {  // an odd number of smoothing swaps left the iterate in the temporary
             DFT_CUDA(cudaMemcpyAsync(v, L[0].v, sizeof(double) * (size_t)g.N, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -476,6 +474,56 @@ int multigrid(dft_context* ctx, const Grid& g, const double* rho, double* v, dou
         mg_residual_kernel<<<mg_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, rho, fourpi, v, L[0].res, rmax);
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
+    };
+    // The cycle's launch sequence is the same every time for this grid and these buffers: it
+    // is captured once as a CUDA graph and replayed (one launch instead of ~10 per level).
+    // A capture that fails for any reason leaves the direct launches in place.
+    cudaGraphExec_t exec = nullptr;
+    long long per_replay = 0;
+    if (ctx->multigrid_graphs) {
+        const MGGraphKey key{g.nx, g.ny, g.nz, (long long)(uintptr_t)slab, (long long)(uintptr_t)rho,
+                             (long long)(uintptr_t)v};
+        auto it = ctx->mg_graphs.find(key);
+        if (it != ctx->mg_graphs.end()) {
+            exec = it->second.exec;
+            per_replay = it->second.launches;
+        } else {
+            const long long l0 = ctx->launches;
+            cudaGraph_t graph = nullptr;
+            bool captured = false;
+            if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                try {
+                    cycle();
+                } catch (const Error&) {
+                }
+                captured = cudaStreamEndCapture(ctx->stream, &graph) == cudaSuccess && graph != nullptr;
+            }
+            cudaGetLastError();  // a failed capture leaves no sticky error; clear the last one
+            per_replay = ctx->launches - l0;
+            ctx->launches = l0;
+            if (captured && L[0].v == v && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+                if (ctx->mg_graphs.size() >= 16) {  // keep a handful: the buffers of the current solves
+                    cudaGraphExecDestroy(ctx->mg_graphs.begin()->second.exec);
+                    ctx->mg_graphs.erase(ctx->mg_graphs.begin());
+                }
+                ctx->mg_graphs[key] = {exec, per_replay};
+            } else {
+                exec = nullptr;
+                cudaGetLastError();
+            }
+            if (graph) cudaGraphDestroy(graph);
+        }
+    }
+    double* h = pinned(ctx, 1);
+    int c = 0;
+    double r = 0.0;
+    for (c = 1; c <= max_cycles; ++c) {
+        if (exec) {
+            DFT_CUDA(cudaGraphLaunch(exec, ctx->stream));
+            count_launch(ctx, per_replay);
+        } else {
+            cycle();
+        }
         DFT_CUDA(cudaMemcpyAsync(h, rmax, 8, cudaMemcpyDeviceToHost, ctx->stream));
         sync(ctx);
         r = h[0] / den;  // the size of the next Jacobi update

@@ -82,6 +82,8 @@ def main():
     ap.add_argument("--iterations", type=int, default=1)
     ap.add_argument("--functional", default="PBE96")
     ap.add_argument("--spl", type=int, default=0, help="Jacobi sweeps per launch (0 = auto)")
+    ap.add_argument("--bpt", type=int, default=0, help="H psi bands per thread (0 = auto)")
+    ap.add_argument("--ring", type=int, default=0, help="tensor-core Gram through the cp.async ring (1)")
     ap.add_argument("--system", default="h2_48", help="scf mode: h2_48, h2o_128, cluster20")
     ap.add_argument("--stop-abs-de", type=float, default=0.0)
     ap.add_argument("--verbose", type=int, default=0)
@@ -91,6 +93,8 @@ def main():
     eng = d.Engine(0)
     eng.set_tuning("jacobi_sweeps_per_launch", a.spl)
     eng.set_tuning("network_tensor_cores", a.tc)
+    eng.set_tuning("hpsi_bands_per_thread", a.bpt)
+    eng.set_tuning("tensor_core_ring", a.ring)
     stream = torch.cuda.ExternalStream(eng.stream)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     out = {"mode": a.mode}

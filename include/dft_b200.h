@@ -69,6 +69,9 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               BF16 rounding, not bit for bit).
  *   "hpsi_bands_per_thread":    0 = auto (default), 1, 2 or 4 bands marched together by each
  *                               thread of the H psi kernel (results identical for every value).
+ *   "multigrid_graphs":         1 (default) = each Poisson multigrid cycle is captured once per
+ *                               grid and buffers as a CUDA graph and replayed; 0 = launched kernel
+ *                               by kernel (same results).
  *   "tensor_core_ring":         0 (default) = the tensor-core Gram product stages its FP64 slices
  *                               through registers; 1 = through a 2-deep cp.async shared-memory
  *                               ring (even leading dimensions, 16-byte-aligned blocks, <= 128

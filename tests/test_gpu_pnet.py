@@ -203,3 +203,25 @@ def test_fermi_smearing_limits(engine):
     print(e)
     assert abs(e[1e-4][0] - e[0.0][0]) < 1e-6
     assert np.isfinite(e[2e-2][0]) and e[2e-2][1] < 100
+
+
+def test_multigrid_graph_replay_identical(engine):
+    """Replaying the captured multigrid cycle gives the same potential, bit for bit, as
+    launching its kernels one by one."""
+    n = (40, 36, 44)
+    g = dft_b200.CartesianGrid(*n, -5.85, 5.85, -5.25, 5.25, -6.45, 6.45)
+    N = g.getSize()
+    rho = engine.array(N)
+    engine.synthetic_density(g, 11, rho)
+    out = {}
+    try:
+        for graphs in (0, 1, 1):  # the second graph run replays the cached capture
+            engine.set_tuning("multigrid_graphs", graphs)
+            v = engine.array(N)
+            info = engine.poisson_start(g, None, rho, v, multigrid_cycles=6)
+            out.setdefault(graphs, []).append((v.to_host(), info["cycles"]))
+    finally:
+        engine.set_tuning("multigrid_graphs", 1)
+    ref, cyc = out[0][0]
+    for v, c in out[1]:
+        assert c == cyc and np.array_equal(v, ref)
