@@ -264,16 +264,24 @@ __global__ void __launch_bounds__(256) gram_small_kernel(const double* __restric
     for (int r = 0; r < RPW; ++r)
 #pragma unroll
         for (int j = 0; j < KB; ++j) acc[r][j] = 0.0;
-    for (long long p = (long long)blockIdx.x * 32 + lane; p < n; p += (long long)gridDim.x * 32) {
-        double b[KB];
+    // two points per step (both loads issued before the FMAs) for more loads in flight
+    const long long stride = (long long)gridDim.x * 32;
+    for (long long p = (long long)blockIdx.x * 32 + lane; p < n; p += 2 * stride) {
+        const long long p2 = p + stride;
+        const bool has2 = p2 < n;
+        double b[KB], b2[KB];
 #pragma unroll
-        for (int j = 0; j < KB; ++j) b[j] = j < kb ? __ldg(B + (long long)j * ldb + p) : 0.0;
+        for (int j = 0; j < KB; ++j) {
+            b[j] = j < kb ? __ldg(B + (long long)j * ldb + p) : 0.0;
+            b2[j] = (j < kb && has2) ? __ldg(B + (long long)j * ldb + p2) : 0.0;
+        }
 #pragma unroll
         for (int r = 0; r < RPW; ++r) {
             const int i = warp + 8 * r;
             const double a = i < ka ? __ldg(A + (long long)i * lda + p) : 0.0;
+            const double a2 = (i < ka && has2) ? __ldg(A + (long long)i * lda + p2) : 0.0;
 #pragma unroll
-            for (int j = 0; j < KB; ++j) acc[r][j] = fma(a, b[j], acc[r][j]);
+            for (int j = 0; j < KB; ++j) acc[r][j] = fma(a2, b2[j], fma(a, b[j], acc[r][j]));
         }
     }
     const int nel = ka * kb;
@@ -313,7 +321,7 @@ void gram(dft_context* ctx, const Grid& g, const double* A, long long lda, int k
     if (ka <= 64 && kb <= 16 && rpw * kbt <= 64) {
         // narrow product: one launch, the last block reduces
         const size_t nel = (size_t)ka * kb;
-        const int nblk = (int)std::max<long long>(1, std::min<long long>(2LL * ctx->num_sms, (g.N + 1023) / 1024));
+        const int nblk = (int)std::max<long long>(1, std::min<long long>(4LL * ctx->num_sms, (g.N + 255) / 256));
         double* partial = (double*)ws_get(ctx, WS_SMALL, sizeof(double) * (nel * nblk + nel) + 64);
         double* res = partial + nel * nblk;
         if (!ctx->gram_ticket) {
