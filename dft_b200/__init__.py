@@ -47,7 +47,8 @@ class dft_scf_opts(C.Structure):
                 ("verbose", C.c_int), ("poisson_start", C.c_int), ("poisson_net", C.c_void_p), ("mixer", C.c_int),
                 ("pulay_depth", C.c_int), ("pulay_beta", C.c_double), ("adaptive_eig_tol", C.c_int),
                 ("smearing_kt", C.c_double), ("kerker_q0", C.c_double),
-                ("log_path", C.c_char_p), ("autotune", C.c_int), ("initial_density", C.c_int)]
+                ("stop_abs_deig", C.c_double), ("log_path", C.c_char_p), ("autotune", C.c_int),
+                ("initial_density", C.c_int)]
 
 
 class dft_autotune_report(C.Structure):
@@ -87,7 +88,8 @@ class dft_scf_iteration(C.Structure):
                 ("poisson_sweeps_in", C.c_long), ("poisson_sweeps_out", C.c_long),
                 ("eig_iterations_alpha", C.c_int), ("eig_iterations_beta", C.c_int),
                 ("ms_hartree", C.c_double), ("ms_xc", C.c_double), ("ms_orbitals", C.c_double),
-                ("ms_density", C.c_double), ("ms_energy", C.c_double), ("ms_total", C.c_double)]
+                ("ms_density", C.c_double), ("ms_energy", C.c_double), ("ms_total", C.c_double),
+                ("eigenvalue_difference", C.c_double)]
 
 
 class dft_scf_result(C.Structure):
@@ -147,7 +149,7 @@ _SIGS = {
                                 C.POINTER(dft_eig_opts), C.POINTER(C.c_int)], C.c_int),
     "dft_rotate_dev": ([_P, C.POINTER(dft_grid), _P, C.c_long, C.c_int, _D, C.c_int, _P, C.c_long, C.c_int],
                        C.c_int),
-    "dft_screened_poisson_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double], C.c_int),
+    "dft_screened_poisson_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double, C.c_int], C.c_int),
     "dft_gram_dev": ([_P, C.POINTER(dft_grid), _P, C.c_long, C.c_int, _P, C.c_long, C.c_int, C.c_int, _D], C.c_int),
     "dft_scf_default_options": ([C.POINTER(dft_scf_opts)], None),
     "dft_scf_molecule": ([_P, C.POINTER(dft_grid), C.c_int, C.POINTER(C.c_int), _D, C.c_int, C.c_int, C.c_int,
@@ -464,10 +466,10 @@ class Engine:
         _check(load().dft_gram_dev(self.ctx, C.byref(g), _ptr(A), lda, ka, _ptr(B), ldb, kb, int(precision), _dp(out)))
         return out
 
-    def screened_poisson(self, grid, src, x, q2):
-        """x ~ (-lap_h + q2)^{-1} src by one multigrid cycle (the Kerker mixer's screening solve)."""
+    def screened_poisson(self, grid, src, x, q2, cycles=1):
+        """x ~ (-lap_h + q2)^{-1} src by `cycles` multigrid cycles (the Kerker mixer's screening solve)."""
         g = grid.c()
-        _check(load().dft_screened_poisson_dev(self.ctx, C.byref(g), _ptr(src), _ptr(x), float(q2)))
+        _check(load().dft_screened_poisson_dev(self.ctx, C.byref(g), _ptr(src), _ptr(x), float(q2), int(cycles)))
 
     def rotate(self, grid, V, ldv, k, Y, X, ldx, precision=0):
         """X = V * Y for band blocks (Y: k x m host matrix)."""

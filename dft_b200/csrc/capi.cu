@@ -348,11 +348,12 @@ dft_status_t dft_rotate_dev(dft_context* ctx, const dft_grid* g, const double* V
     });
 }
 
-dft_status_t dft_screened_poisson_dev(dft_context* ctx, const dft_grid* g, const double* src, double* x, double q2) {
+dft_status_t dft_screened_poisson_dev(dft_context* ctx, const dft_grid* g, const double* src, double* x, double q2,
+                                      int cycles) {
     return guard(ctx, [&] {
         NEED(ctx && src && x, "NULL argument");
         const dftb::Grid G = dftb::make_grid(g);
-        dftb::screened_poisson_vcycle(ctx, G, src, 1, q2, x, G.N);
+        dftb::screened_poisson_vcycle(ctx, G, src, 1, q2, x, G.N, cycles);
         dftb::sync(ctx);
     });
 }

@@ -1494,7 +1494,7 @@ void kerker_update(dft_context* ctx, const Grid& g, int ns, double* const* a, co
         count_launch(ctx);
     }
     // closed shell: the total residual is 2 r, so (q^2/2) V(2 r) = q^2 V(r)
-    screened_poisson_vcycle(ctx, g, ns == 2 ? rtot : r[0], 1, q2, x, g.N);
+    screened_poisson_vcycle(ctx, g, ns == 2 ? rtot : r[0], 1, q2, x, g.N, 2);
     const double f = ns == 2 ? 0.5 * q2 : q2;
     for (int sp = 0; sp < ns; ++sp) {
         kerker_update_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g.N, a[sp], r[sp], x, f, beta, a[sp]);

@@ -45,7 +45,7 @@ void pulay_combine(dft_context* ctx, long long n, int m, const double* const* a,
 // out = sum_i c_i a_i over m <= 16 fields (no clamp)
 void combine(dft_context* ctx, long long n, int m, const double* const* a, const double* c, double* out);
 // Kerker-screened density step for ns spin fields (ns = 1: closed shell, the field is n_alpha):
-// x = (-lap_h + q2)^{-1} (r_0 + r_1) by one multigrid cycle (rtot: scratch for the sum), then
+// x = (-lap_h + q2)^{-1} (r_0 + r_1) by two multigrid cycles (rtot: scratch for the sum), then
 // a_s = max(0, a_s + beta (r_s - (q2/2) x)), i.e. the total-charge residual is multiplied by
 // -lap/(-lap + q2) (the real-space Kerker factor G^2/(G^2 + q0^2)) and the spin residual is kept.
 void kerker_update(dft_context* ctx, const Grid& g, int ns, double* const* a, const double* const* r, double* rtot,
@@ -97,10 +97,11 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
 void precondition_multigrid(dft_context* ctx, const Grid& g, const double* R, const int* src_dev, int nb,
                             const double* theta_dev, double* T, long long ld);
 
-// One multigrid V(2,2) cycle from zero for (-lap_h + q2) x_a = src_a, x = 0 outside the box, for
-// nb fields of ld points (precond_mg.cu): x ~ (-lap_h + q2)^{-1} src, a fixed linear map.
+// `cycles` multigrid V(2,2) cycles (the first from zero, then iterative refinement) for
+// (-lap_h + q2) x_a = src_a, x = 0 outside the box, for nb fields of ld points (precond_mg.cu):
+// x ~ (-lap_h + q2)^{-1} src, a fixed linear map.
 void screened_poisson_vcycle(dft_context* ctx, const Grid& g, const double* src, int nb, double q2, double* x,
-                             long long ld);
+                             long long ld, int cycles = 1);
 
 // X_a ~ (T + sigma_a)^-1 R_a for nb fields by `cycles` multigrid cycles with iterative refinement
 // (the first from zero), sigma on the device; res and e: scratch of nb x ld doubles each.

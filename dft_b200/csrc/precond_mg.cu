@@ -399,13 +399,27 @@ void helmholtz_refine(dft_context* ctx, const Grid& g, const double* R, int nb, 
 }
 
 void screened_poisson_vcycle(dft_context* ctx, const Grid& g, const double* src, int nb, double q2, double* x,
-                             long long ld) {
+                             long long ld, int cycles) {
     if (nb <= 0) return;
     if (!(q2 > 0.0) || !std::isfinite(q2)) fail(DFT_INVALID_ARGUMENT, "screening q^2 must be > 0");
+    if (cycles < 1) fail(DFT_INVALID_ARGUMENT, "cycles must be >= 1");
     double* shift = (double*)ws_get(ctx, WS_PG3, sizeof(double) * (size_t)nb + 64);
     pc_fill_kernel<<<(nb + 127) / 128, 128, 0, ctx->stream>>>(nb, q2, shift);
     count_launch(ctx);
     vcycle_batch(ctx, g, src, nullptr, nb, shift, 1.0, x, ld);
+    if (cycles == 1) return;
+    // iterative refinement: res = src - (-lap + q2) x, e = V-cycle(res), x += e
+    double* scratch = (double*)ws_get(ctx, WS_PG4, sizeof(double) * 2 * (size_t)nb * ld);
+    double *res = scratch, *e = scratch + (size_t)nb * ld;
+    for (int c = 1; c < cycles; ++c) {
+        const ColShape cs = col_shape(ctx, g, nb);
+        pc_residual_kernel<<<cs.grid, cs.block, 0, ctx->stream>>>(g, ld, src, 1.0, shift, x, res, cs.zc, cs.nzc);
+        count_launch(ctx);
+        vcycle_batch(ctx, g, res, nullptr, nb, shift, 1.0, e, ld);
+        pc_add_kernel<<<pc_grid(ctx, g.N, nb), 256, 0, ctx->stream>>>(g.N, ld, e, x);
+        count_launch(ctx);
+        DFT_LAUNCH_CHECK();
+    }
 }
 
 }  // namespace dftb

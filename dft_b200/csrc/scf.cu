@@ -35,6 +35,50 @@ struct DevBuf {
     DevBuf& operator=(const DevBuf&) = delete;
 };
 
+// per-block sums of psi^2 over points within w bohr of a face, and over all points
+__global__ void wall_weight_kernel(Grid g, const double* __restrict__ psi, double w, double* __restrict__ partial) {
+    __shared__ double sh[2][8];
+    double a = 0.0, t = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((long long)g.nx * g.ny));
+        const double x = g.xmin + i * g.dx, y = g.ymin + j * g.dy, z = g.zmin + k * g.dz;
+        const double d = fmin(fmin(fmin(x - g.xmin, g.xmax - x), fmin(y - g.ymin, g.ymax - y)),
+                              fmin(z - g.zmin, g.zmax - z));
+        const double v = psi[p] * psi[p];
+        t += v;
+        if (d < w) a += v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sh[0][threadIdx.x >> 5] = a;
+        sh[1][threadIdx.x >> 5] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sa = 0.0, st = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) sa += sh[0][q], st += sh[1][q];
+        partial[2 * blockIdx.x] = sa;
+        partial[2 * blockIdx.x + 1] = st;
+    }
+}
+
+// fraction of |psi|^2 within w bohr of a face (diagnostics)
+double wall_fraction(dft_context* ctx, const Grid& g, const double* psi, double w) {
+    const int nb = std::max(1, std::min((int)((g.N + 255) / 256), ctx->num_sms * 4));
+    double* partial = (double*)ws_get(ctx, WS_SCF3, sizeof(double) * 2 * (size_t)nb);
+    wall_weight_kernel<<<nb, 256, 0, ctx->stream>>>(g, psi, w, partial);
+    DFT_LAUNCH_CHECK();
+    std::vector<double> h(2 * (size_t)nb);
+    DFT_CUDA(cudaMemcpyAsync(h.data(), partial, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    double a = 0.0, t = 0.0;
+    for (int q = 0; q < nb; ++q) a += h[2 * q], t += h[2 * q + 1];
+    return t > 0.0 ? a / t : 0.0;
+}
+
 }  // namespace
 
 void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z, const double* xyz, int charge,
@@ -306,6 +350,8 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     double effd = 0.0, resid = 0.0, dE = std::numeric_limits<double>::infinity();
     bool converged = false;
     int it = 0;
+    std::vector<double> prev_eig;
+    double deig = std::numeric_limits<double>::infinity();
     res->history_len = 0;
     // convergence analysis (MolecularSCFConvergenceAnalysis, reference MolecularSCFHelpers.h:47-72)
     res->last_energy_criterion_iteration = res->last_density_criterion_iteration = res->last_ks_criterion_iteration = 0;
@@ -428,6 +474,19 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             for (int i = 0; i < nb; ++i) resid = std::max(resid, resb[i]);
         rec.ms_energy = ms_since(t0);
         dE = std::isfinite(prevE) ? std::fabs(E[5] - prevE) : std::numeric_limits<double>::infinity();
+        // occupied eigenvalues (alpha, then beta) and their change since the previous iteration
+        {
+            std::vector<double> cur(eiga.begin(), eiga.begin() + na);
+            const std::vector<double>& eb = closed ? eiga : eigb;
+            cur.insert(cur.end(), eb.begin(), eb.begin() + nb);
+            deig = std::numeric_limits<double>::infinity();
+            if (prev_eig.size() == cur.size()) {
+                deig = 0.0;
+                for (size_t q = 0; q < cur.size(); ++q) deig = std::max(deig, std::fabs(cur[q] - prev_eig[q]));
+            }
+            prev_eig.swap(cur);
+        }
+        rec.eigenvalue_difference = deig;
         converged = dE < o.energy_tol && effd < o.density_tol && resid < o.ks_tol;
         rec.energy = E[5];
         rec.energy_difference = dE;
@@ -449,12 +508,12 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
                          "\"ks_residual\":%s,\"mixing\":%s,\"kinetic\":%s,\"external\":%s,\"hartree\":%s,"
                          "\"exchange_correlation\":%s,\"nuclear_repulsion\":%s,\"poisson_sweeps_in\":%ld,"
                          "\"poisson_sweeps_out\":%ld,\"eig_iterations_alpha\":%d,\"eig_iterations_beta\":%d,"
-                         "\"levels_alpha\":%s,\"levels_beta\":%s,\"ms_hartree\":%s,\"ms_xc\":%s,"
+                         "\"eigenvalue_difference\":%s,\"levels_alpha\":%s,\"levels_beta\":%s,\"ms_hartree\":%s,\"ms_xc\":%s,"
                          "\"ms_orbitals\":%s,\"ms_density\":%s,\"ms_energy\":%s,\"ms_total\":%s}\n",
                          it, jnum(E[5]).c_str(), jnum(dE).c_str(), jnum(effd).c_str(), jnum(resid).c_str(),
                          jnum(rec.mixing).c_str(), jnum(E[0]).c_str(), jnum(E[1]).c_str(), jnum(E[2]).c_str(),
                          jnum(E[3]).c_str(), jnum(E[4]).c_str(), jin.sweeps, jout.sweeps, rec.eig_iterations_alpha,
-                         rec.eig_iterations_beta, jlevels(eiga, na).c_str(),
+                         rec.eig_iterations_beta, jnum(deig).c_str(), jlevels(eiga, na).c_str(),
                          jlevels(closed ? eiga : eigb, nb).c_str(), jnum(rec.ms_hartree).c_str(),
                          jnum(rec.ms_xc).c_str(), jnum(rec.ms_orbitals).c_str(), jnum(rec.ms_density).c_str(),
                          jnum(rec.ms_energy).c_str(), jnum(rec.ms_total).c_str());
@@ -479,9 +538,16 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             };
             levels("a", eiga, na, density_difference(ctx, g, da.p, oa.p));
             if (!closed) levels("b", eigb, nb, density_difference(ctx, g, db.p, ob.p));
+            if (o.verbose > 2) {
+                // where the levels around the Fermi level live: fraction within 4 bohr of a face
+                fprintf(stderr, "[scf]   wall fraction (4 bohr) alpha homo-3..:");
+                for (int i = std::max(0, na - 4); i < std::min(bands_a, na + 4); ++i)
+                    fprintf(stderr, "%s%.3f", i == na ? " || " : " ", wall_fraction(ctx, g, psia.p + (long long)i * ld, 4.0));
+                fprintf(stderr, "\n");
+            }
         }
         if (converged) break;
-        if (o.stop_abs_de > 0.0 && dE < o.stop_abs_de) break;
+        if (o.stop_abs_de > 0.0 && dE < o.stop_abs_de && (o.stop_abs_deig <= 0.0 || deig < o.stop_abs_deig)) break;
         // adaptive mixing with the pre-update factor applied (:447-484)
         if (std::isfinite(prevD)) {
             if (effd > prevD * 1.05) mixing = std::max(0.10, mixing * 0.75);

@@ -204,11 +204,13 @@ typedef struct {
 dft_status_t dft_rotate_dev(dft_context* ctx, const dft_grid* g, const double* V, long ldv, int k, const double* Y,
                             int m, double* X, long ldx, int precision);
 
-/* x ~ (-lap_h + q2)^{-1} src by one multigrid V(2,2) cycle from zero (7-point Laplacian,
- * x = 0 outside the box; src, x: device, N doubles; q2 > 0).  The screening solve of the
- * Kerker mixer (dft_scf_opts.kerker_q0), exposed for testing; no counterpart in the
- * reference, whose mixer is linear (MolecularSCFHelpers.cpp:27-44). */
-dft_status_t dft_screened_poisson_dev(dft_context* ctx, const dft_grid* g, const double* src, double* x, double q2);
+/* x ~ (-lap_h + q2)^{-1} src by `cycles` multigrid V(2,2) cycles, the first from zero and the
+ * rest refining (7-point Laplacian, x = 0 outside the box; src, x: device, N doubles; q2 > 0).
+ * The screening solve of the Kerker mixer (dft_scf_opts.kerker_q0, which uses 2 cycles),
+ * exposed for testing; no counterpart in the reference, whose mixer is linear
+ * (MolecularSCFHelpers.cpp:27-44). */
+dft_status_t dft_screened_poisson_dev(dft_context* ctx, const dft_grid* g, const double* src, double* x, double q2,
+                                      int cycles);
 
 /* dV * A^T B for band blocks A (ka x N, leading dimension lda) and B (kb x N), result in
  * C_host (ka x kb, row-major).  precision 0 = FP64, 1 = tensor cores (TF32 hi+lo split).
@@ -267,6 +269,9 @@ typedef struct {
                                 bands instead of the reference's integer aufbau (0) */
     double kerker_q0;        /* > 0: Kerker screening of the total-charge residual in either mixer,
                                 -lap/(-lap + q0^2) by one multigrid cycle (bohr^-1; 0 = off) */
+    double stop_abs_deig;    /* > 0: the stop_abs_de stop also needs every occupied eigenvalue to have
+                                changed by less than this since the previous iteration (the energy is
+                                second order in the density error, eigenvalues first order) */
     const char* log_path;    /* non-NULL: one JSON object per SCF iteration (the dft_scf_iteration
                                 fields, energy components, the levels around the Fermi level per
                                 spin) and a final {"result": ...} line, written to this file; the
@@ -289,6 +294,7 @@ typedef struct {
     long poisson_sweeps_in, poisson_sweeps_out;
     int eig_iterations_alpha, eig_iterations_beta;
     double ms_hartree, ms_xc, ms_orbitals, ms_density, ms_energy, ms_total;
+    double eigenvalue_difference;  /* max |change| of the occupied eigenvalues since the previous iteration */
 } dft_scf_iteration;
 
 typedef struct {
