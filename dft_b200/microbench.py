@@ -59,7 +59,10 @@ def cube(n, h):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram", "poisson", "train", "rotate"])
+    ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram", "poisson", "train", "rotate",
+                                     "c4"])
+    ap.add_argument("--samples", type=int, default=512, help="c4: training densities")
+    ap.add_argument("--held-out", type=int, default=6, help="c4: held-out densities per grid")
     ap.add_argument("--tc", type=int, default=1, help="network convolutions on the tensor cores (1) or CUDA cores (0)")
     ap.add_argument("--ka", type=int, default=64)
     ap.add_argument("--kb", type=int, default=64)
@@ -185,6 +188,44 @@ def main():
         t = _events(torch, stream, run, a.reps)
         out.update(n=a.n, poisson=a.poisson, network=bool(net), ms=statistics.median(t), sweeps=res["s"],
                    cycles=res["c"])
+    elif a.mode == "c4":
+        # the learned Poisson start at the scale of the learned-start workload: seeded synthetic
+        # densities (1-8 Gaussians, widths 0.3-2 bohr, 2-40 electrons) on 96^3 and 128^3 grids at
+        # h = 0.2, targets the Jacobi fixed point to 1e-10; then, on held-out densities, the
+        # Jacobi sweeps (reference stop rule: max|dV| < 1e-8, cap 10000) and the final max error
+        # against the fixed point from each start
+        import time
+        grids = [cube(96, a.h), cube(128, a.h)]
+        net = d.PoissonNet(eng, seed=7)
+        t0 = time.perf_counter()
+        rep = net.train(grids, samples=a.samples, validation=max(8, a.samples // 16), epochs=10, batch=4, lr=3e-3,
+                        lr_min=1e-4, seed=2029, smooth_sweeps=0, mse_weight=1.0)
+        train_s = time.perf_counter() - t0
+        starts = {}
+        for g in grids:
+            N = g.getSize()
+            rho, v, vstar = eng.array(N), eng.array(N), eng.array(N)
+            for q in range(a.held_out):
+                eng.synthetic_density(g, 900000 + 17 * q + g.nx, rho)
+                eng.poisson_start(g, None, rho, vstar, multigrid_cycles=60)
+                eng.hartree_from_guess(g, rho, vstar, 1e-10, 400000)
+                ref = vstar.to_host()
+                for name in ("cold", "coarse", "coarse+network", "multigrid+network"):
+                    if name == "cold":
+                        sw = eng.hartree(g, rho, v, 1e-8, 10000)[0]
+                    else:
+                        eng.poisson_start(g, net if "network" in name else None, rho, v,
+                                          multigrid_cycles=40 if name.startswith("multigrid") else 0)
+                        sw = eng.hartree_from_guess(g, rho, v, 1e-8, 10000)[0]
+                    err = float(np.max(np.abs(v.to_host() - ref)))
+                    st = starts.setdefault(f"{g.nx}^3 {name}", {"sweeps": [], "max_error": []})
+                    st["sweeps"].append(sw)
+                    st["max_error"].append(err)
+        summary = {k: {"mean_sweeps": float(np.mean(v["sweeps"])), "mean_max_error": float(np.mean(v["max_error"])),
+                       "capped": int(sum(1 for x in v["sweeps"] if x >= 10000))} for k, v in starts.items()}
+        out.update(samples=a.samples, grids=[96, 128], h=a.h, train_seconds=train_s, steps=rep["steps"],
+                   val_loss=rep["val_loss"], val_loss_coarse=rep["val_loss_coarse"],
+                   mean_target_sweeps=rep["mean_target_sweeps"], held_out_per_grid=a.held_out, starts=summary)
     elif a.mode == "rotate":
         g = cube(a.n, a.h)
         N = g.getSize()
