@@ -150,6 +150,9 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
         } else if (k == "tensor_core_ring") {
             NEED(value == 0 || value == 1, "tensor_core_ring must be 0 or 1");
             ctx->tc_ring = (int)value;
+        } else if (k == "hpsi_variant") {
+            NEED(value == 0 || value == 1, "hpsi_variant must be 0 or 1");
+            ctx->hpsi_variant = (int)value;
         } else if (k == "hpsi_bands_per_thread") {
             NEED(value == 0 || value == 1 || value == 2 || value == 4, "hpsi_bands_per_thread must be 0 (auto), 1, 2 or 4");
             ctx->hpsi_bands_per_thread = (int)value;

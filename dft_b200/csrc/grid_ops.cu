@@ -217,6 +217,89 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
     }
 }
 
+// Tiled variant ("hpsi_variant" = 1): the current plane of a 32 x 8 column tile and its one-point
+// halo sit in shared memory, the z neighbours in registers; each thread's load of the next
+// plane is issued a full step before it is used.  Same operation order as hpsi_kernel.
+template <int NB>
+__global__ void __launch_bounds__(HB_X* HB_Y) hpsi_tile_kernel(Grid g, const double* __restrict__ V,
+                                                              const double* __restrict__ psi, double* __restrict__ out,
+                                                              long long ld, int nbands, int zchunk, int nzc,
+                                                              double k0) {
+    __shared__ double tile[NB][HB_Y + 2][HB_X + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = blockIdx.x * HB_X + tx;
+    const int j = blockIdx.y * HB_Y + ty;
+    const int group = blockIdx.z / nzc;
+    const int kc = blockIdx.z - group * nzc;
+    const int b0 = group * NB;
+    const int nb = min(NB, nbands - b0);
+    const bool in = i < g.nx && j < g.ny;
+    const double* __restrict__ p = psi + (long long)b0 * ld;
+    double* __restrict__ o = out + (long long)b0 * ld;
+    const long long sxy = (long long)g.nx * g.ny;
+    const int kb = kc * zchunk;
+    const int ke = min(g.nz, kb + zchunk);
+    const long long col = (long long)j * g.nx + i;
+    long long idx = (long long)kb * sxy + col;
+    // halo duty: x- by tx == 0, x+ by the last column of the tile inside the grid, y- by ty == 0,
+    // y+ by the last row inside the grid
+    const int last_x = min(HB_X, g.nx - blockIdx.x * HB_X) - 1, last_y = min(HB_Y, g.ny - blockIdx.y * HB_Y) - 1;
+    const bool hxm = in && tx == 0 && i > 0, hxp = in && tx == last_x && i + 1 < g.nx;
+    const bool hym = in && ty == 0 && j > 0, hyp = in && ty == last_y && j + 1 < g.ny;
+    double below[NB], cur[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const bool on = in && b < nb;
+        below[b] = (on && kb > 0) ? __ldg(p + b * ld + idx - sxy) : 0.0;
+        cur[b] = on ? __ldg(p + b * ld + idx) : 0.0;
+    }
+    const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+    for (int k = kb; k < ke; ++k, idx += sxy) {
+        const bool zr = k + 1 < g.nz;
+        double above[NB], hv[NB][4];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const bool on = in && b < nb;
+            const double* q = p + b * ld + idx;
+            above[b] = (on && zr) ? __ldg(q + sxy) : 0.0;
+            hv[b][0] = (on && hxm) ? __ldg(q - 1) : 0.0;
+            hv[b][1] = (on && hxp) ? __ldg(q + 1) : 0.0;
+            hv[b][2] = (on && hym) ? __ldg(q - g.nx) : 0.0;
+            hv[b][3] = (on && hyp) ? __ldg(q + g.nx) : 0.0;
+        }
+        const double v = in ? __ldg(V + idx) : 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            tile[b][ty + 1][tx + 1] = cur[b];
+            if (hxm) tile[b][ty + 1][0] = hv[b][0];
+            if (hxp) tile[b][ty + 1][tx + 2] = hv[b][1];
+            if (hym) tile[b][0][tx + 1] = hv[b][2];
+            if (hyp) tile[b][ty + 2][tx + 1] = hv[b][3];
+        }
+        __syncthreads();
+        if (in) {
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                if (b >= nb) break;
+                double lap = __dmul_rn(k0, cur[b]);
+                if (xl) lap = __dadd_rn(lap, __dmul_rn(tile[b][ty + 1][tx], g.ix2));
+                if (xr) lap = __dadd_rn(lap, __dmul_rn(tile[b][ty + 1][tx + 2], g.ix2));
+                if (yl) lap = __dadd_rn(lap, __dmul_rn(tile[b][ty][tx + 1], g.iy2));
+                if (yr) lap = __dadd_rn(lap, __dmul_rn(tile[b][ty + 2][tx + 1], g.iy2));
+                if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below[b], g.iz2));
+                if (zr) lap = __dadd_rn(lap, __dmul_rn(above[b], g.iz2));
+                o[b * ld + idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(v, cur[b]));
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            below[b] = cur[b];
+            cur[b] = above[b];
+        }
+        __syncthreads();
+    }
+}
+
 inline int pick_zchunk(const Grid& g, long long columns_blocks, int nbands, int num_sms) {
     // enough CTAs to fill the machine a few times over, but chunks long enough to amortise
     // the two-plane warm-up of the z march
@@ -241,6 +324,7 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
     }
     nbt = std::min(nbt, std::max(1, nbands));
     nbt = nbt >= 4 ? 4 : nbt >= 2 ? 2 : 1;
+    if (ctx->hpsi_variant == 1) nbt = std::min(nbt, 2);
     const int groups = (nbands + nbt - 1) / nbt;
     const int zc = pick_zchunk(g, (long long)bx * by, groups, ctx->num_sms);
     const int nzc = (g.nz + zc - 1) / zc;
@@ -253,9 +337,16 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
         dim3 grid(bx, by, ng * nzc);
         const double* pi = psi + (long long)b0 * ld;
         double* po = hpsi + (long long)b0 * ld;
-        if (nbt == 4) hpsi_kernel<4><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
-        else if (nbt == 2) hpsi_kernel<2><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
-        else hpsi_kernel<1><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+        if (ctx->hpsi_variant == 1) {
+            if (nbt >= 2) hpsi_tile_kernel<2><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+            else hpsi_tile_kernel<1><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+        } else if (nbt == 4) {
+            hpsi_kernel<4><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+        } else if (nbt == 2) {
+            hpsi_kernel<2><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+        } else {
+            hpsi_kernel<1><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+        }
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
     }

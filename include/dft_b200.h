@@ -76,6 +76,9 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               through registers; 1 = through a 2-deep cp.async shared-memory
  *                               ring (even leading dimensions, 16-byte-aligned blocks, <= 128
  *                               columns per tile; otherwise the register path).  Same results.
+ *   "hpsi_variant":             0 (default) = the H psi kernel reads x/y neighbours through L1;
+ *                               1 = through a shared-memory plane tile (at most 2 bands per
+ *                               thread).  Results identical for every value.
  *   "grid_barrier_poll_limit":  0 = 2^24 (default): polls a block of the persistent Jacobi
  *                               launch makes at a grid barrier before it gives up; the solve then
  *                               fails with DFT_CUDA_ERROR and the context stays usable.

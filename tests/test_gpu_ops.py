@@ -31,12 +31,16 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
-@pytest.fixture(params=[0, 1, 2, 4], ids=lambda t: f"bpt{t}")
+@pytest.fixture(params=[(0, 0), (0, 1), (0, 2), (0, 4), (1, 1), (1, 2)], ids=lambda t: f"v{t[0]}bpt{t[1]}")
 def hpsi_bands_per_thread(request, engine):
-    """Every H psi launch shape: auto, 1, 2 or 4 bands marched by each thread."""
-    engine.set_tuning("hpsi_bands_per_thread", request.param)
+    """Every H psi launch shape: neighbours through L1 (variant 0) with auto, 1, 2 or 4 bands per
+    thread, and the shared-memory plane tile (variant 1) with 1 or 2."""
+    variant, bpt = request.param
+    engine.set_tuning("hpsi_variant", variant)
+    engine.set_tuning("hpsi_bands_per_thread", bpt)
     yield request.param
     engine.set_tuning("hpsi_bands_per_thread", 0)
+    engine.set_tuning("hpsi_variant", 0)
 
 
 @pytest.mark.parametrize("n,b", GRIDS)

@@ -219,7 +219,7 @@ def test_multigrid_graph_replay_identical(engine):
             engine.set_tuning("multigrid_graphs", graphs)
             v = engine.array(N)
             info = engine.poisson_start(g, None, rho, v, multigrid_cycles=6)
-            out.setdefault(graphs, []).append((v.to_host(), info["cycles"]))
+            out.setdefault(graphs, []).append((v.to_host(), info["multigrid_cycles"]))
     finally:
         engine.set_tuning("multigrid_graphs", 1)
     ref, cyc = out[0][0]
