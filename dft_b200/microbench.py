@@ -89,6 +89,9 @@ def main():
     ap.add_argument("--ring", type=int, default=0, help="tensor-core Gram through the cp.async ring (1)")
     ap.add_argument("--system", default="h2_48", help="scf mode: h2_48, h2o_128, cluster20")
     ap.add_argument("--stop-abs-de", type=float, default=0.0)
+    ap.add_argument("--stop-abs-deig", type=float, default=0.0)
+    ap.add_argument("--kerker", type=float, default=0.0, help="scf: Kerker screening q0 (bohr^-1), 0 = off")
+    ap.add_argument("--atoms", type=int, default=0, help="scf: superposed-atoms start (1)")
     ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args()
     import torch
@@ -151,8 +154,9 @@ def main():
             out["train"] = {k: rep[k] for k in ("steps", "seconds_data", "seconds_train", "val_loss",
                                                 "val_loss_coarse")}
         o = d.default_scf_options(max_iterations=a.iterations, extra_bands=w["extra_bands"], verbose=int(a.verbose),
-                                  stop_abs_de=a.stop_abs_de, poisson_start=POISSON[a.poisson], mixer=a.mixer,
-                                  adaptive_eig_tol=a.adaptive, smearing_kt=a.smearing)
+                                  stop_abs_de=a.stop_abs_de, stop_abs_deig=a.stop_abs_deig,
+                                  poisson_start=POISSON[a.poisson], mixer=a.mixer, adaptive_eig_tol=a.adaptive,
+                                  smearing_kt=a.smearing, kerker_q0=a.kerker, initial_density=a.atoms)
         if net is not None:
             o.poisson_net = net.handle
         o.eig.verbose = int(a.verbose > 2)
@@ -164,7 +168,8 @@ def main():
                    energy=r.total,
                    seconds=r.seconds, launches=eng.launches, eigenvalues=r.eigenvalues[:8],
                    history=[{k: h[k] for k in ("iteration", "energy", "energy_difference", "density_difference",
-                                               "ks_residual", "poisson_sweeps_in", "poisson_sweeps_out",
+                                               "ks_residual", "eigenvalue_difference", "poisson_sweeps_in",
+                                               "poisson_sweeps_out",
                                                "eig_iterations_alpha", "ms_hartree", "ms_xc", "ms_orbitals",
                                                "ms_density", "ms_energy", "ms_total")} for h in r.history])
     elif a.mode == "poisson":

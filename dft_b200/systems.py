@@ -7,6 +7,7 @@ cluster20    20 nuclei with Z drawn from {1, 6, 7, 8}, positions uniform in a 24
              in a 192^3 grid (h = 0.2), minimum separation 2.0 bohr, no nucleus within 1e-12 of a
              node, neutral, multiplicity 1 + (N_e mod 2), PBE96 (seeded numpy generator)
 cluster20_clear  the same draw with every nucleus at least 0.08 bohr from the nearest node
+cluster20_compact  the same seeded draw in a 14-bohr cube (more vacuum to the box faces)
 """
 from __future__ import annotations
 
@@ -70,7 +71,18 @@ def cluster_clear(**kw):
     return w
 
 
-SYSTEMS = {"h2_48": h2_48, "h2o_128": h2o_128, "cluster20": cluster, "cluster20_clear": cluster_clear}
+def cluster_compact(**kw):
+    """The 20-atom draw in a 14-bohr cube instead of 24 (same grid): 12 bohr of vacuum to every
+    face instead of 7, which keeps the box-wall states above the Fermi level."""
+    kw.setdefault("box", 14.0)
+    w = cluster(**kw)
+    w["name"] += "_compact"
+    w["desc"] += ", nuclei in a 14-bohr cube"
+    return w
+
+
+SYSTEMS = {"h2_48": h2_48, "h2o_128": h2o_128, "cluster20": cluster, "cluster20_clear": cluster_clear,
+           "cluster20_compact": cluster_compact}
 
 
 def get(name, **kw):
