@@ -157,6 +157,42 @@ namespace {
 
 constexpr int HB_X = 32, HB_Y = 8;
 
+// One thread per (i,j) column of one band, marching k over a z-chunk (32 registers, 8 blocks
+// per SM).  reference KohnShamHamiltonianMolecule.cpp:59-177: lap = k0*c (+ neighbours in the
+// order x-, x+, y-, y+, z-, z+), H psi = -0.5*lap + V*c; absent neighbours are skipped.
+__global__ void __launch_bounds__(HB_X* HB_Y) hpsi1_kernel(Grid g, const double* __restrict__ V,
+                                                          const double* __restrict__ psi, double* __restrict__ out,
+                                                          long long ld, int zchunk, int nzc, double k0) {
+    const int i = blockIdx.x * HB_X + threadIdx.x;
+    const int j = blockIdx.y * HB_Y + threadIdx.y;
+    const int band = blockIdx.z / nzc;
+    const int kc = blockIdx.z - band * nzc;
+    if (i >= g.nx || j >= g.ny) return;
+    const double* __restrict__ p = psi + (long long)band * ld;
+    double* __restrict__ o = out + (long long)band * ld;
+    const long long sxy = (long long)g.nx * g.ny;
+    const int kb = kc * zchunk;
+    const int ke = min(g.nz, kb + zchunk);
+    long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
+    double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
+    double cur = __ldg(p + idx);
+    const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+    for (int k = kb; k < ke; ++k, idx += sxy) {
+        const bool zr = k + 1 < g.nz;
+        const double above = zr ? __ldg(p + idx + sxy) : 0.0;
+        double lap = __dmul_rn(k0, cur);
+        if (xl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - 1), g.ix2));
+        if (xr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + 1), g.ix2));
+        if (yl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - g.nx), g.iy2));
+        if (yr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + g.nx), g.iy2));
+        if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below, g.iz2));
+        if (zr) lap = __dadd_rn(lap, __dmul_rn(above, g.iz2));
+        o[idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(__ldg(V + idx), cur));
+        below = cur;
+        cur = above;
+    }
+}
+
 // One thread per (i,j) column of NB bands, marching k over a z-chunk: V is read once per point
 // for all NB bands and the NB bands' loads are independent, so more of them are in flight.
 // reference KohnShamHamiltonianMolecule.cpp:59-177: lap = k0*c (+ neighbours in the order
@@ -221,7 +257,7 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi_kernel(Grid g, const double* 
 // halo sit in shared memory, the z neighbours in registers; each thread's load of the next
 // plane is issued a full step before it is used.  Same operation order as hpsi_kernel.
 template <int NB>
-__global__ void __launch_bounds__(HB_X* HB_Y) hpsi_tile_kernel(Grid g, const double* __restrict__ V,
+__global__ void __launch_bounds__(HB_X* HB_Y, 6) hpsi_tile_kernel(Grid g, const double* __restrict__ V,
                                                               const double* __restrict__ psi, double* __restrict__ out,
                                                               long long ld, int nbands, int zchunk, int nzc,
                                                               double k0) {
@@ -316,11 +352,12 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
     const double k0 = -2.0 * (g.ix2 + g.iy2 + g.iz2);
     dim3 block(HB_X, HB_Y);
     const int bx = (g.nx + HB_X - 1) / HB_X, by = (g.ny + HB_Y - 1) / HB_Y;
-    // bands per thread: the "hpsi_bands_per_thread" tuning key, else 2 for blocks of 2 or more
+    // bands per thread: the "hpsi_bands_per_thread" tuning key, else the autotuner's choice for
+    // this grid, else 1 (the 32-register single-band march keeps 8 blocks per SM resident)
     int nbt = ctx->hpsi_bands_per_thread;
     if (nbt <= 0) {
         auto t = ctx->tuned.find({(long long)g.nx, (long long)g.ny, (long long)g.nz});
-        nbt = t != ctx->tuned.end() ? t->second[0] : (nbands >= 2 ? 2 : 1);
+        nbt = t != ctx->tuned.end() ? t->second[0] : 1;
     }
     nbt = std::min(nbt, std::max(1, nbands));
     nbt = nbt >= 4 ? 4 : nbt >= 2 ? 2 : 1;
@@ -345,7 +382,7 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
         } else if (nbt == 2) {
             hpsi_kernel<2><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
         } else {
-            hpsi_kernel<1><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+            hpsi1_kernel<<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, zc, nzc, k0);
         }
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
