@@ -481,7 +481,12 @@ int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, doub
                     }
                 for (int i = 0; i < nt; ++i)
                     for (int j = 0; j < nt; ++j) Yc[(size_t)(k + i) * nt + j] = Yk[(size_t)i * nt + j];
-                rotate(ctx, g, V, ld, k + nt, Yc, nt, W, ld, 1.0, 0.0);
+                // in mixed-precision mode a wide rotation runs on the tensor cores like the Ritz
+                // rotations (the second pass restores orthonormality to the products' accuracy)
+                if (tc && k + nt >= 32 && (long long)(k + nt) * nt >= 2048)
+                    rotate_tc(ctx, g, V, ld, k + nt, Yc, nt, W, ld);
+                else
+                    rotate(ctx, g, V, ld, k + nt, Yc, nt, W, ld, 1.0, 0.0);
                 DFT_CUDA(cudaMemcpyAsync(T, W, sizeof(double) * (size_t)ld * nt, cudaMemcpyDeviceToDevice,
                                          ctx->stream));
                 continue;
