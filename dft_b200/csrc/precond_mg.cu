@@ -153,29 +153,32 @@ __global__ void pc_restrict_axis_kernel(const double* __restrict__ in, long long
     }
 }
 
-// v += trilinear interpolation of the coarse correction e, at every fine point
-__global__ void pc_prolong_add_kernel(Grid f, long long fld, Grid c, long long cld, const double* __restrict__ e,
-                                      double* __restrict__ v) {
-    const int a = blockIdx.y;
+// v += trilinear interpolation of the coarse correction e, at every fine point.  One thread per
+// fine (i, j) column: the x/y cells and weights are found once, z steps along the column.
+__global__ void __launch_bounds__(256) pc_prolong_add_kernel(Grid f, long long fld, Grid c, long long cld,
+                                                             const double* __restrict__ e, double* __restrict__ v,
+                                                             int zc, int nzc) {
+    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+    const int a = blockIdx.z / nzc, kc = blockIdx.z - a * nzc;
+    if (i >= f.nx || j >= f.ny) return;
     e += (long long)a * cld;
     v += (long long)a * fld;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < f.N; p += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(p % f.nx), j = (int)((p / f.nx) % f.ny), k = (int)(p / ((long long)f.nx * f.ny));
-        const double u[3] = {i * f.dx / c.dx, j * f.dy / c.dy, k * f.dz / c.dz};
-        const int m[3] = {c.nx, c.ny, c.nz};
-        int I[3];
-        double w[3];
-        for (int d = 0; d < 3; ++d) {
-            I[d] = min(max((int)floor(u[d]), 0), m[d] - 2);
-            w[d] = fmin(fmax(u[d] - I[d], 0.0), 1.0);
-        }
-        double acc = 0.0;
-        for (int t = 0; t < 8; ++t) {
-            const int x = t & 1, y = (t >> 1) & 1, z = t >> 2;
-            const double wt = (x ? w[0] : 1.0 - w[0]) * (y ? w[1] : 1.0 - w[1]) * (z ? w[2] : 1.0 - w[2]);
-            acc += wt * e[((long long)(I[2] + z) * c.ny + (I[1] + y)) * c.nx + (I[0] + x)];
-        }
-        v[p] += acc;
+    const double ux = i * f.dx / c.dx, uy = j * f.dy / c.dy;
+    const int Ix = min(max((int)floor(ux), 0), c.nx - 2), Iy = min(max((int)floor(uy), 0), c.ny - 2);
+    const double wx = fmin(fmax(ux - Ix, 0.0), 1.0), wy = fmin(fmax(uy - Iy, 0.0), 1.0);
+    const long long cxy = (long long)c.nx * c.ny;
+    const long long b00 = (long long)Iy * c.nx + Ix;
+    const long long fxy = (long long)f.nx * f.ny;
+    const int kb = kc * zc, ke = min(f.nz, kb + zc);
+    for (int k = kb; k < ke; ++k) {
+        const double uz = k * f.dz / c.dz;
+        const int Iz = min(max((int)floor(uz), 0), c.nz - 2);
+        const double wz = fmin(fmax(uz - Iz, 0.0), 1.0);
+        const double* e0 = e + (long long)Iz * cxy + b00;
+        const double* e1 = e0 + cxy;
+        const double p0 = (1.0 - wy) * ((1.0 - wx) * e0[0] + wx * e0[1]) + wy * ((1.0 - wx) * e0[c.nx] + wx * e0[c.nx + 1]);
+        const double p1 = (1.0 - wy) * ((1.0 - wx) * e1[0] + wx * e1[1]) + wy * ((1.0 - wx) * e1[c.nx] + wx * e1[c.nx + 1]);
+        v[(long long)k * fxy + (long long)j * f.nx + i] += (1.0 - wz) * p0 + wz * p1;
     }
 }
 
@@ -278,7 +281,10 @@ void pc_vcycle(dft_context* ctx, std::vector<PCLevel>& L, size_t i, double s, co
         l.t2, (long long)f.nz * c.g.ny * c.g.nx, c.src, c.ld, c.g.nx, c.g.ny, f.nz, 2, c.g.nz, f.dz, c.g.dz);
     count_launch(ctx, 4);
     pc_vcycle(ctx, L, i + 1, 1.0, shift, nb);
-    pc_prolong_add_kernel<<<pc_grid(ctx, f.N, nb), 256, 0, ctx->stream>>>(f, l.ld, c.g, c.ld, c.v, l.v);
+    {
+        const ColShape cs = col_shape(ctx, f, nb);
+        pc_prolong_add_kernel<<<cs.grid, cs.block, 0, ctx->stream>>>(f, l.ld, c.g, c.ld, c.v, l.v, cs.zc, cs.nzc);
+    }
     count_launch(ctx);
     pc_smooth(ctx, l, s, shift, nb, 2, false);
     DFT_LAUNCH_CHECK();
