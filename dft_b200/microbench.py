@@ -92,6 +92,8 @@ def main():
     ap.add_argument("--stop-abs-deig", type=float, default=0.0)
     ap.add_argument("--kerker", type=float, default=0.0, help="scf: Kerker screening q0 (bohr^-1), 0 = off")
     ap.add_argument("--atoms", type=int, default=0, help="scf: superposed-atoms start (1)")
+    ap.add_argument("--pulay-beta", type=float, default=0.0, help="scf: Pulay step (0 = 0.2)")
+    ap.add_argument("--pulay-depth", type=int, default=0, help="scf: Pulay history (0 = 8)")
     ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args()
     import torch
@@ -156,7 +158,8 @@ def main():
         o = d.default_scf_options(max_iterations=a.iterations, extra_bands=w["extra_bands"], verbose=int(a.verbose),
                                   stop_abs_de=a.stop_abs_de, stop_abs_deig=a.stop_abs_deig,
                                   poisson_start=POISSON[a.poisson], mixer=a.mixer, adaptive_eig_tol=a.adaptive,
-                                  smearing_kt=a.smearing, kerker_q0=a.kerker, initial_density=a.atoms)
+                                  smearing_kt=a.smearing, kerker_q0=a.kerker, initial_density=a.atoms,
+                                  pulay_beta=a.pulay_beta, pulay_depth=a.pulay_depth)
         if net is not None:
             o.poisson_net = net.handle
         o.eig.verbose = int(a.verbose > 2)
