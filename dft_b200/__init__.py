@@ -48,7 +48,8 @@ class dft_scf_opts(C.Structure):
                 ("pulay_depth", C.c_int), ("pulay_beta", C.c_double), ("adaptive_eig_tol", C.c_int),
                 ("smearing_kt", C.c_double), ("kerker_q0", C.c_double),
                 ("stop_abs_deig", C.c_double), ("log_path", C.c_char_p), ("autotune", C.c_int),
-                ("initial_density", C.c_int)]
+                ("initial_density", C.c_int),
+                ("hartree_boundary", C.c_int)]
 
 
 class dft_autotune_report(C.Structure):
@@ -139,6 +140,8 @@ _SIGS = {
     "dft_hartree_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double, C.c_long, C.POINTER(C.c_long), _D], C.c_int),
     "dft_hartree_noalloc_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double, C.c_long, C.POINTER(C.c_long), _D],
                                 C.c_int),
+    "dft_hartree_monopole_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double, C.c_long, C.POINTER(C.c_long), _D],
+                                 C.c_int),
     "dft_hartree_energy_dev": ([_P, C.POINTER(dft_grid), _P, _P, _D], C.c_int),
     "dft_xc_dev": ([_P, C.POINTER(dft_grid), C.c_int, _P, _P, _P, _P, _D], C.c_int),
     "dft_xc_evaluate_dev": ([_P, C.c_int, C.c_long, _P, _P, _P, _P, _P], C.c_int),
@@ -398,6 +401,15 @@ class Engine:
         ld = C.c_double()
         _check(load().dft_hartree_dev(self.ctx, C.byref(g), _ptr(rho), _ptr(vh), tol, max_sweeps, C.byref(sw),
                                       C.byref(ld)))
+        return sw.value, ld.value
+
+    def hartree_monopole(self, grid, rho, vh, tol=1e-8, max_sweeps=10000):
+        """Hartree potential with Q/|r| on every face (dft_scf_opts.hartree_boundary = 1)."""
+        g = grid.c()
+        sw = C.c_long()
+        ld = C.c_double()
+        _check(load().dft_hartree_monopole_dev(self.ctx, C.byref(g), _ptr(rho), _ptr(vh), tol, max_sweeps,
+                                               C.byref(sw), C.byref(ld)))
         return sw.value, ld.value
 
     def hartree_from_guess(self, grid, rho, vh, tol=1e-8, max_sweeps=10000):

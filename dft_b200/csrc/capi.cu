@@ -258,6 +258,37 @@ dft_status_t dft_hartree_noalloc_dev(dft_context* ctx, const dft_grid* g, const 
     });
 }
 
+dft_status_t dft_hartree_monopole_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
+                                      long max_sweeps, long* sweeps_out, double* last_diff_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && rho && vh, "NULL argument");
+        NEED(rho != vh, "rho and vh must not alias");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::monopole_width(G);
+        double *rp = nullptr, *vc = nullptr, *vp = nullptr;
+        auto release = [&] {
+            cudaFree(rp);
+            cudaFree(vc);
+            cudaFree(vp);
+        };
+        try {
+            DFT_CUDA(cudaMalloc(&rp, sizeof(double) * (size_t)G.N));
+            DFT_CUDA(cudaMalloc(&vc, sizeof(double) * (size_t)G.N));
+            DFT_CUDA(cudaMalloc(&vp, sizeof(double) * (size_t)G.N));
+            dftb::monopole_prepare(ctx, G, rho, rp, vc);
+            dftb::JacobiResult r = dftb::hartree(ctx, G, rp, vp, tol, max_sweeps, nullptr, true);
+            dftb::add_into(ctx, G.N, vp, vc, vh);
+            dftb::sync(ctx);
+            if (sweeps_out) *sweeps_out = r.sweeps;
+            if (last_diff_out) *last_diff_out = r.last_diff;
+        } catch (...) {
+            release();
+            throw;
+        }
+        release();
+    });
+}
+
 dft_status_t dft_hartree_energy_dev(dft_context* ctx, const dft_grid* g, const double* rho, const double* vh,
                                     double* energy_out) {
     return guard(ctx, [&] {

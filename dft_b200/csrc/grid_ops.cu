@@ -1100,6 +1100,86 @@ JacobiResult hartree(dft_context* ctx, const Grid& g, const double* rho, double*
     return {sweeps, hc->last_diff};
 }
 
+// =============================================================== monopole boundary (option)
+// The reference's face values are Q/|r| (|r| from the origin, Q the total charge), except that
+// a face whose last node lands exactly on the bound gets 0 (HartreePotentialMolecule.cpp:45-94);
+// every grid of the benchmark systems lands exactly, so their faces are all 0.  For many
+// electrons the zero faces are far from the free-space potential and bind spurious states at
+// the box walls.  The option applies Q/|r| on every face.  It is solved without touching the
+// zero-face solvers: with V_c = Q erf(|r| / (sqrt(2) s)) / |r| (which equals Q/|r| on the faces
+// to double precision for s <= face distance / 8), V_H = V' + V_c where V' has zero faces and
+// L_h V' = -4 pi rho - L_h V_c, L_h the same 7-point Laplacian: the discrete problem is exactly
+// the Dirichlet problem with V_c's face values.
+namespace {
+struct SumF {
+    const double* a;
+    __device__ void operator()(long long p, double* acc) const { acc[0] += a[p]; }
+};
+
+__device__ __forceinline__ double gauss_pot(double q, double s, double r) {
+    // q erf(r / (sqrt(2) s)) / r, its limit q sqrt(2/pi) / s at r = 0
+    if (r < 1e-10 * s) return q * 0.79788456080286535588 / s;
+    return q * erf(r * (0.70710678118654752440 / s)) / r;
+}
+
+__global__ void monopole_comp_kernel(Grid g, double q, double s, double* __restrict__ vc) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((long long)g.nx * g.ny));
+        const double x = g.xmin + i * g.dx, y = g.ymin + j * g.dy, z = g.zmin + k * g.dz;
+        vc[p] = gauss_pot(q, s, sqrt(x * x + y * y + z * z));
+    }
+}
+
+// interior: out = rho + (L_h vc) / (4 pi); faces: 0 (unused by the solvers)
+__global__ void monopole_source_kernel(Grid g, const double* __restrict__ rho, const double* __restrict__ vc,
+                                       double* __restrict__ out) {
+    const double inv4pi = 1.0 / (4.0 * xcf::PI);
+    const long long sxy = (long long)g.nx * g.ny;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / sxy);
+        if (i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz) {
+            out[p] = 0.0;
+            continue;
+        }
+        const double c = vc[p];
+        const double lap = g.ix2 * (vc[p - 1] + vc[p + 1] - 2.0 * c) + g.iy2 * (vc[p - g.nx] + vc[p + g.nx] - 2.0 * c) +
+                           g.iz2 * (vc[p - sxy] + vc[p + sxy] - 2.0 * c);
+        out[p] = rho[p] + lap * inv4pi;
+    }
+}
+
+__global__ void add_into_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
+                                double* __restrict__ o) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        o[p] = a[p] + b[p];
+}
+}  // namespace
+
+double monopole_width(const Grid& g) {
+    const double d = std::min({-g.xmin, g.xmax, -g.ymin, g.ymax, -g.zmin, g.zmax});
+    if (!(d > 4.0 * std::max({g.dx, g.dy, g.dz})))
+        fail(DFT_INVALID_ARGUMENT, "the monopole boundary needs the origin well inside the box");
+    return d / 8.0;
+}
+
+double monopole_prepare(dft_context* ctx, const Grid& g, const double* rho, double* rho_prime, double* vc) {
+    double q = 0.0;
+    reduce_to_host<1>(ctx, g.N, SumF{rho}, &q);
+    q *= g.dV;
+    const double s = monopole_width(g);
+    monopole_comp_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, q, s, vc);
+    monopole_source_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, rho, vc, rho_prime);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx, 2);
+    return q;
+}
+
+void add_into(dft_context* ctx, long long n, const double* a, const double* b, double* out) {
+    add_into_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, a, b, out);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
 // =============================================================== allocation-free Poisson
 // The Jacobi solve above takes its second iterate buffer and its control words from the
 // context's workspace, which grows with cudaMalloc.  Some callers cannot let a library

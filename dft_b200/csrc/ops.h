@@ -32,6 +32,14 @@ double* noalloc_scratch(int device);
 JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol,
                              long max_sweeps);
 
+// Monopole boundary option (grid_ops.cu): vc = Q erf(|r|/(sqrt 2 s))/|r| (Q = sum rho dV, returned)
+// and rho_prime = rho + L_h vc / (4 pi) on the interior, so that V_H = V' + vc with V' the
+// zero-face solution for rho_prime has the face values Q/|r|.  monopole_width: s for grid g.
+double monopole_prepare(dft_context* ctx, const Grid& g, const double* rho, double* rho_prime, double* vc);
+double monopole_width(const Grid& g);
+// out = a + b (plain addition)
+void add_into(dft_context* ctx, long long n, const double* a, const double* b, double* out);
+
 // rho = a + b
 void add2(dft_context* ctx, long long n, const double* a, const double* b, double* out);
 // out = (a + b) + c

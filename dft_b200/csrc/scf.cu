@@ -134,7 +134,19 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     dft_pnet* net = pstart == DFT_POISSON_COARSE ? nullptr : o.poisson_net;
     // Poisson solve of density d into v with the chosen start; `have_prev` says whether v
     // still holds this slot's potential from the previous iteration.
-    auto poisson = [&](const double* d, double* v, bool have_prev) {
+    // Monopole faces: the zero-face solve runs on (rho', V') per slot, V_H = V' + V_c.
+    const bool monopole = o.hartree_boundary == 1;
+    if (monopole) monopole_width(g);  // the origin must lie well inside the box
+    DevBuf mrho(monopole ? (size_t)N : 0), mvc(monopole ? (size_t)N : 0), mvp0(monopole ? (size_t)N : 0),
+        mvp1(monopole ? (size_t)N : 0);
+    auto poisson = [&](const double* d_in, double* v_out, bool have_prev) {
+        const double* d = d_in;
+        double* v = v_out;
+        if (monopole) {
+            monopole_prepare(ctx, g, d_in, mrho.p, mvc.p);
+            d = mrho.p;
+            v = v_out == vh.p ? mvp0.p : mvp1.p;
+        }
         const double* start = nullptr;
         if (pstart == DFT_POISSON_MULTIGRID) {
             const auto t0 = Clock::now();
@@ -159,7 +171,9 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             poisson_start(ctx, net, g, d, vstart.p, 0, nullptr);
             start = vstart.p;
         }
-        return hartree(ctx, g, d, v, o.poisson_tol, o.poisson_max_sweeps, start);
+        const JacobiResult r = hartree(ctx, g, d, v, o.poisson_tol, o.poisson_max_sweeps, start, monopole);
+        if (monopole) add_into(ctx, N, v, mvc.p, v_out);
+        return r;
     };
     DevBuf psia((size_t)bands_a * ld), psib(closed ? 0 : (size_t)bands_b * ld);
     std::vector<double> eiga(bands_a), eigb(bands_b), resa(bands_a), resb(bands_b);
@@ -186,6 +200,8 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     // superposed radial atoms (option): densities now, atomic orbitals as the first eigensolve's
     // start basis (both spins), freed after the first iteration
     const bool atoms_start = o.initial_density == 1;
+    if (o.hartree_boundary != 0 && o.hartree_boundary != 1)
+        fail(DFT_INVALID_ARGUMENT, "unknown hartree_boundary %d", o.hartree_boundary);
     int nao = 0;
     DevBuf aobuf;
     if (atoms_start) {

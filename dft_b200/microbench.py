@@ -94,6 +94,7 @@ def main():
     ap.add_argument("--atoms", type=int, default=0, help="scf: superposed-atoms start (1)")
     ap.add_argument("--pulay-beta", type=float, default=0.0, help="scf: Pulay step (0 = 0.2)")
     ap.add_argument("--pulay-depth", type=int, default=0, help="scf: Pulay history (0 = 8)")
+    ap.add_argument("--boundary", type=int, default=0, help="scf: Hartree faces, 0 reference, 1 Q/|r| (monopole)")
     ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args()
     import torch
@@ -159,7 +160,8 @@ def main():
                                   stop_abs_de=a.stop_abs_de, stop_abs_deig=a.stop_abs_deig,
                                   poisson_start=POISSON[a.poisson], mixer=a.mixer, adaptive_eig_tol=a.adaptive,
                                   smearing_kt=a.smearing, kerker_q0=a.kerker, initial_density=a.atoms,
-                                  pulay_beta=a.pulay_beta, pulay_depth=a.pulay_depth)
+                                  pulay_beta=a.pulay_beta, pulay_depth=a.pulay_depth,
+                                  hartree_boundary=a.boundary)
         if net is not None:
             o.poisson_net = net.handle
         o.eig.verbose = int(a.verbose > 2)

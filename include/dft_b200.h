@@ -151,6 +151,16 @@ dft_status_t dft_hartree_dev(dft_context* ctx, const dft_grid* g, const double* 
 dft_status_t dft_hartree_noalloc_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
                                      long max_sweeps, long* sweeps_out, double* last_diff_out);
 
+/* Hartree potential with V = Q/|r| on every face (Q = sum rho dV, |r| from the origin), the
+ * boundary of dft_scf_opts.hartree_boundary = 1: a Gaussian compensation charge of width
+ * (smallest origin-face distance)/8 carries Q, the remainder is solved by the Jacobi sweeps of
+ * dft_hartree_dev with zero faces (same tol / max_sweeps stop rule) and the compensation's
+ * potential is added back.  The origin must lie more than four spacings inside every face
+ * (DFT_INVALID_ARGUMENT otherwise).  Allocates two N-point scratch arrays per call.  No
+ * counterpart in the reference, whose faces follow dft_hartree_dev. */
+dft_status_t dft_hartree_monopole_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
+                                      long max_sweeps, long* sweeps_out, double* last_diff_out);
+
 /* calculateHartreeEnergy (reference HartreePotentialMolecule.cpp:326-379): 1/2 sum rho V dV. */
 dft_status_t dft_hartree_energy_dev(dft_context* ctx, const dft_grid* g, const double* rho, const double* vh,
                                     double* energy_out);
@@ -287,6 +297,11 @@ typedef struct {
                                 1: superposed radial atoms of the same functional (batched radial
                                 SCF, SelfConsistentField.cpp:539-786), scaled to the electron count,
                                 and their occupied atomic orbitals as the first eigensolve's start */
+    int hartree_boundary;    /* 0: the reference's face values (Q/|r| only on a face whose last node
+                                misses the bound by rounding, else 0; HartreePotentialMolecule.cpp:45-94);
+                                1: Q/|r| on every face (monopole), through a Gaussian compensation
+                                charge and the same zero-face solvers; the wall states that zero
+                                faces bind for many electrons do not form */
 } dft_scf_opts;
 
 /* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)
