@@ -406,6 +406,12 @@ def _reference_scf_worker(args):
             "iterations": o["iterations"], "energy": o["total"], "last_de": None}
 
 
+def bench_config(args, w, world):
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": args.workload, "desc": w["desc"], "grid": list(w["n"]),
+            "l2": "512 MiB write between steps", "parallelism": f"replicas{world}"}
+
+
 def run_reference_arm(args, w, rank, world):
     """The reference's own CPU code on this host's cores: one whole SCF of the workload to
     |dE| < 1e-6 per core, all cores at once (the reference is single-threaded), timed by wall
@@ -430,7 +436,7 @@ def run_reference_arm(args, w, rank, world):
     out = {"metric": METRIC, "value": val, "unit": "SCF/s", "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / cores, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": args.workload, "desc": w["desc"]},
+           "config": bench_config(args, w, args.gpus),
            "reference_scfs_timed": cores, "reference_wall_s": wall, "reference_seconds_per_scf": per,
            "reference_energy": runs[0]["energy"], "reference_iterations": runs[0]["iterations"],
            "note": "steps/warmup are not applied to the CPU arm: it times one batch of whole SCFs "
@@ -577,9 +583,8 @@ def main():
         "metric": METRIC, "value": value, "unit": "SCF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": w["desc"], "grid": list(w["n"]),
-                   "l2": "512 MiB write between steps", "parallelism": f"replicas{world}",
-                   "scf_iterations": last.iterations, "energy": last.total,
+        "config": bench_config(args, w, world),
+        "run": {"scf_iterations": last.iterations, "energy": last.total,
                    "seconds_to_1e-6": ms_per_step / 1e3,
                    "phase_ms": {k: round(sum(h[k] for h in last.history), 2)
                                 for k in ("ms_hartree", "ms_xc", "ms_orbitals", "ms_density", "ms_energy")},

@@ -113,6 +113,7 @@ dft_status_t dft_context_destroy(dft_context* ctx) {
             if (w.ptr) cudaFree(w.ptr);
         if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
         if (ctx->gram_ticket) cudaFree(ctx->gram_ticket);
+        if (ctx->dev_status) cudaFree(ctx->dev_status);
         for (auto& kv : ctx->mg_graphs) cudaGraphExecDestroy(kv.second.exec);
         cudaStreamDestroy(ctx->stream);
     });
@@ -124,6 +125,7 @@ dft_status_t dft_context_synchronize(dft_context* ctx) {
     return guard(ctx, [&] {
         NEED(ctx, "context is NULL");
         dftb::sync(ctx);
+        dftb::check_device_status(ctx, "a kernel on the context's stream");
     });
 }
 
@@ -151,10 +153,11 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
             NEED(value == 0 || value == 1, "tensor_core_ring must be 0 or 1");
             ctx->tc_ring = (int)value;
         } else if (k == "hpsi_variant") {
-            NEED(value == 0 || value == 1, "hpsi_variant must be 0 or 1");
+            NEED(value >= 0 && value <= 2, "hpsi_variant must be 0, 1 or 2");
             ctx->hpsi_variant = (int)value;
         } else if (k == "hpsi_bands_per_thread") {
-            NEED(value == 0 || value == 1 || value == 2 || value == 4, "hpsi_bands_per_thread must be 0 (auto), 1, 2 or 4");
+            NEED(value == 0 || value == 1 || value == 2 || value == 4 || value == 8,
+                 "hpsi_bands_per_thread must be 0 (auto), 1, 2, 4 or 8");
             ctx->hpsi_bands_per_thread = (int)value;
         } else {
             dftb::fail(DFT_INVALID_ARGUMENT, "unknown tuning key '%s'", key);

@@ -110,7 +110,9 @@ struct dft_context {
     int jacobi_sweeps_per_launch = 0;  // 0 = auto, 1 = one sweep per launch, 2/4/8 = temporal blocking
     int net_tensor_cores = 1;          // network convolutions on tcgen05 (1) or FP32 CUDA cores (0)
     int hpsi_bands_per_thread = 0;     // H psi bands per thread: 0 = auto, 1, 2 or 4
-    int hpsi_variant = 0;              // H psi: 0 = neighbours through L1, 1 = shared-memory plane tile
+    int hpsi_variant = 0;              // H psi: 0 = neighbours through L1, 1 = shared-memory plane tile,
+                                       // 2 = TMA plane ring (where eligible, else 0)
+    int* dev_status = nullptr;         // device word set by kernels whose bounded waits gave up
     int tc_ring = 0;                   // tensor-core Gram: cp.async ring variant (1) or register staging (0)
     long long grid_barrier_poll_limit = 0;  // persistent Jacobi barrier polls before giving up (0 = 2^24)
     // autotuner choices per grid (nx, ny, nz) -> {H psi bands per thread, Jacobi sweeps per launch},

@@ -781,6 +781,7 @@ int solve_orbitals(dft_context* ctx, const Grid& g, const double* V, int nocc, i
         if (resid_host) resid_host[b] = rn[b];
     }
     sync(ctx);
+    check_device_status(ctx, "eigensolver");
     if (!done) {
         double mx = 0.0;
         for (int b = 0; b < nocc; ++b) mx = std::max(mx, rn[b]);

@@ -9,6 +9,8 @@
 // nuclear potential, mixing) uses round-to-nearest intrinsics in the reference's operation
 // order (no FMA contraction), which makes it bit-identical to the reference.
 #include <cooperative_groups.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -336,6 +338,174 @@ __global__ void __launch_bounds__(HB_X* HB_Y, 6) hpsi_tile_kernel(Grid g, const 
     }
 }
 
+// ---------------------------------------------------------------- TMA plane ring ---------
+// "hpsi_variant" = 2.  A CTA owns a 32 x 8 column tile, a z-chunk and a run of bands, and walks
+// the planes kb-1 .. ke of each band in order.  One elected thread loads each plane tile with
+// its one-point halo (x from x0-2 so the copy starts on a 16-byte boundary: 36 x 10 doubles)
+// by cp.async.bulk.tensor into a ring of HT_S shared-memory stages, each tracked by an
+// mbarrier with the transaction count; the loads run HT_S-2 planes ahead of the compute,
+// so the copies in flight per SM do not depend on registers.  Out-of-box parts of a tile
+// (x < 0, y < 0, z = -1, z = nz, ...) are zero-filled by the copy and never used: absent
+// neighbours are skipped exactly as in hpsi1_kernel, so every value is bit-identical.  The
+// point's own column (below, current) is kept in registers; V is read from global memory
+// once per band (from L2 after the first band of the run).
+constexpr int HT_X = 32, HT_Y = 8, HT_S = 6;
+constexpr int HT_PX = HT_X + 4, HT_PY = HT_Y + 2;
+constexpr int HT_PLANE = HT_PX * HT_PY;                            // doubles in a plane tile
+constexpr int HT_STAGE = (HT_PLANE * 8 + 127) / 128 * 128 / 8;     // stage stride (128-byte aligned)
+constexpr long long HT_SPIN = 1LL << 22;                           // polls before a wait gives up
+
+__device__ __forceinline__ uint32_t ht_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool ht_wait(uint64_t* bar, uint32_t parity, long long limit) {
+    const uint32_t a = ht_smem(bar);
+    for (long long n = 0; n < limit; ++n) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(HT_X* HT_Y) hpsi_tma_kernel(const __grid_constant__ CUtensorMap tm, Grid g,
+                                                              const double* __restrict__ V, double* __restrict__ out,
+                                                              long long ld, int nbands, int nbc, int zchunk, int nzc,
+                                                              double k0, int* __restrict__ status) {
+    __shared__ __align__(128) double plane[HT_S][HT_STAGE];
+    __shared__ __align__(8) uint64_t full[HT_S];
+    __shared__ int abort_flag;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool leader = tx == 0 && ty == 0;
+    const int x0 = blockIdx.x * HT_X, y0 = blockIdx.y * HT_Y;
+    const int grp = blockIdx.z / nzc;
+    const int kc = blockIdx.z - grp * nzc;
+    const int b0 = grp * nbc;
+    const int nb = min(nbc, nbands - b0);
+    const int kb = kc * zchunk;
+    const int ke = min(g.nz, kb + zchunk);
+    const int nk = ke - kb;
+    const int L = nk + 2;  // planes kb-1 .. ke of one band
+    const int Q = nb * L;
+    if (leader) {
+        for (int s = 0; s < HT_S; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(ht_smem(&full[s])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        abort_flag = 0;
+    }
+    __syncthreads();
+    int issued = 0;
+    auto issue = [&](int p) {
+        const int b = p / L;
+        const int k = kb - 1 + (p - b * L);
+        const uint32_t bar = ht_smem(&full[p % HT_S]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(HT_PLANE * 8)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+            "%5}], [%6];" ::"r"(ht_smem(&plane[p % HT_S][0])),
+            "l"(reinterpret_cast<uint64_t>(&tm)), "r"(x0 - 2), "r"(y0 - 1), "r"(k), "r"(b0 + b), "r"(bar)
+            : "memory");
+    };
+    if (leader)
+        while (issued < Q && issued < HT_S) issue(issued++);
+    const int i = x0 + tx, j = y0 + ty;
+    const bool in = i < g.nx && j < g.ny;
+    const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+    const long long sxy = (long long)g.nx * g.ny;
+    const int c = (ty + 1) * HT_PX + tx + 2;  // the point's offset inside a plane tile
+    int waited = 0;                           // planes this thread has waited for
+    double below = 0.0, cur = 0.0;
+    const int steps = nb * nk;
+    for (int s = 0; s < steps; ++s) {
+        const int b = s / nk;
+        const int k = kb + (s - b * nk);
+        const int q = b * L + (k - kb + 1);  // the plane of this step in the sequence
+        const long long idx = (long long)k * sxy + (long long)j * g.nx + i;
+        const double v = in ? __ldg(V + idx) : 0.0;
+        bool good = true;
+        while (waited <= q + 1) {
+            good = good && ht_wait(&full[waited % HT_S], (uint32_t)((waited / HT_S) & 1), HT_SPIN);
+            ++waited;
+        }
+        if (!good) abort_flag = 1;
+        if (k == kb) {
+            below = plane[(q - 1) % HT_S][c];
+            cur = plane[q % HT_S][c];
+        }
+        const double* P = plane[q % HT_S];
+        const double above = plane[(q + 1) % HT_S][c];
+        if (in) {
+            double lap = __dmul_rn(k0, cur);
+            if (xl) lap = __dadd_rn(lap, __dmul_rn(P[c - 1], g.ix2));
+            if (xr) lap = __dadd_rn(lap, __dmul_rn(P[c + 1], g.ix2));
+            if (yl) lap = __dadd_rn(lap, __dmul_rn(P[c - HT_PX], g.iy2));
+            if (yr) lap = __dadd_rn(lap, __dmul_rn(P[c + HT_PX], g.iy2));
+            if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below, g.iz2));
+            if (k + 1 < g.nz) lap = __dadd_rn(lap, __dmul_rn(above, g.iz2));
+            out[(long long)(b0 + b) * ld + idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(v, cur));
+        }
+        below = cur;
+        cur = above;
+        __syncthreads();  // every thread is done with the planes before the next step's q - 1
+        if (abort_flag) break;
+        if (leader) {
+            int qn = Q;  // the next step's plane (all planes free after the last step)
+            if (s + 1 < steps) {
+                const int bn = (s + 1) / nk;
+                qn = bn * L + (s + 1 - bn * nk) + 1;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            while (issued < Q && issued < qn - 1 + HT_S) issue(issued++);
+        }
+    }
+    if (abort_flag && leader) {
+        atomicOr(status, 1);
+        // let the copies still in flight land before the block's shared memory is released
+        for (; waited < issued; ++waited) ht_wait(&full[waited % HT_S], (uint32_t)((waited / HT_S) & 1), HT_SPIN);
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+    });
+    return fn;
+}
+
+// The TMA ring needs 16-byte strides (nx and ld even) and a 16-byte aligned band block.
+bool hpsi_tma_eligible(const Grid& g, const double* psi, long long ld) {
+    return g.nx % 2 == 0 && ld % 2 == 0 && (reinterpret_cast<uintptr_t>(psi) & 15) == 0 && g.nx >= 3 &&
+           g.ny >= 3 && tensor_map_encoder() != nullptr;
+}
+
+// 4-D map (x, y, z, band) of nbands bands at psi, box = one plane tile with its halo.
+CUtensorMap hpsi_tensor_map(const Grid& g, const double* psi, long long ld, int nbands) {
+    CUtensorMap tm;
+    const cuuint64_t dims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz, (cuuint64_t)nbands};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.nx * 8, (cuuint64_t)g.nx * g.ny * 8, (cuuint64_t)ld * 8};
+    const cuuint32_t box[4] = {HT_PX, HT_PY, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = tensor_map_encoder()(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(psi), dims,
+                                            strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(DFT_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return tm;
+}
+
 inline int pick_zchunk(const Grid& g, long long columns_blocks, int nbands, int num_sms) {
     // enough CTAs to fill the machine a few times over, but chunks long enough to amortise
     // the two-plane warm-up of the z march
@@ -346,10 +516,51 @@ inline int pick_zchunk(const Grid& g, long long columns_blocks, int nbands, int 
 
 }  // namespace
 
+int* device_status(dft_context* ctx) {
+    if (!ctx->dev_status) {
+        DFT_CUDA(cudaMalloc(&ctx->dev_status, 256));
+        DFT_CUDA(cudaMemsetAsync(ctx->dev_status, 0, 256, ctx->stream));
+    }
+    return ctx->dev_status;
+}
+
+void check_device_status(dft_context* ctx, const char* what) {
+    if (!ctx->dev_status) return;
+    int* h = (int*)pinned(ctx, 1);
+    DFT_CUDA(cudaMemcpyAsync(h, ctx->dev_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    if (*h) {
+        DFT_CUDA(cudaMemsetAsync(ctx->dev_status, 0, sizeof(int), ctx->stream));
+        fail(DFT_CUDA_ERROR, "%s: a bounded device wait gave up (status %d)", what, *h);
+    }
+}
+
 void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const double* psi, double* hpsi, int nbands,
                        long long ld) {
     if (nbands <= 0) return;
     const double k0 = -2.0 * (g.ix2 + g.iy2 + g.iz2);
+    if (ctx->hpsi_variant == 2 && hpsi_tma_eligible(g, psi, ld)) {
+        // bands per CTA: the "hpsi_bands_per_thread" key (1, 2, 4 or 8), else 4
+        int nbc = ctx->hpsi_bands_per_thread > 0 ? ctx->hpsi_bands_per_thread : 4;
+        nbc = std::max(1, std::min(nbc, nbands));
+        const int bx = (g.nx + HT_X - 1) / HT_X, by = (g.ny + HT_Y - 1) / HT_Y;
+        const int groups = (nbands + nbc - 1) / nbc;
+        const int zc = pick_zchunk(g, (long long)bx * by, groups, ctx->num_sms);
+        const int nzc = (g.nz + zc - 1) / zc;
+        const int max_groups = std::max(1, 65535 / nzc);
+        int* st = device_status(ctx);
+        for (int g0 = 0; g0 < groups; g0 += max_groups) {
+            const int ng = std::min(max_groups, groups - g0);
+            const int b0 = g0 * nbc;
+            const int nb = std::min(nbands - b0, ng * nbc);
+            const CUtensorMap tm = hpsi_tensor_map(g, psi + (long long)b0 * ld, ld, nb);
+            hpsi_tma_kernel<<<dim3(bx, by, ng * nzc), dim3(HT_X, HT_Y), 0, ctx->stream>>>(
+                tm, g, V, hpsi + (long long)b0 * ld, ld, nb, nbc, zc, nzc, k0, st);
+            DFT_LAUNCH_CHECK();
+            count_launch(ctx);
+        }
+        return;
+    }
     dim3 block(HB_X, HB_Y);
     const int bx = (g.nx + HB_X - 1) / HB_X, by = (g.ny + HB_Y - 1) / HB_Y;
     // bands per thread: the "hpsi_bands_per_thread" tuning key, else the autotuner's choice for

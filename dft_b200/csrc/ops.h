@@ -40,6 +40,11 @@ double monopole_width(const Grid& g);
 // out = a + b (plain addition)
 void add_into(dft_context* ctx, long long n, const double* a, const double* b, double* out);
 
+// The context's device status word (allocated on first use) and its check: fails with
+// DFT_CUDA_ERROR (and clears the word) when a kernel's bounded wait gave up since the last check.
+int* device_status(dft_context* ctx);
+void check_device_status(dft_context* ctx, const char* what);
+
 // rho = a + b
 void add2(dft_context* ctx, long long n, const double* a, const double* b, double* out);
 // out = (a + b) + c

@@ -57,6 +57,9 @@ const char* dft_version(void);
 /* ---- context and device memory (no reference counterpart: the reference has no device) ---- */
 dft_status_t dft_context_create(int device, dft_context** out);
 dft_status_t dft_context_destroy(dft_context* ctx);
+/* Waits for the context's stream.  Also fails with DFT_CUDA_ERROR when a kernel launched since
+ * the last call gave up a bounded wait (the TMA H psi ring, "hpsi_variant" = 2); the context
+ * stays usable. */
 dft_status_t dft_context_synchronize(dft_context* ctx);
 /* Kernel-shape knobs.  Keys:
  *   "jacobi_sweeps_per_launch": 0 = auto (default), -2 = the whole solve in the shared memory
@@ -68,7 +71,9 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               convolutions on tcgen05, 0 = FP32 CUDA cores (results agree to
  *                               BF16 rounding, not bit for bit).
  *   "hpsi_bands_per_thread":    0 = auto (default), 1, 2 or 4 bands marched together by each
- *                               thread of the H psi kernel (results identical for every value).
+ *                               thread of the H psi kernel (8 counts as 4), or with
+ *                               "hpsi_variant" = 2 the bands (1, 2, 4, 8) each block walks
+ *                               (results identical for every value).
  *   "multigrid_graphs":         1 (default) = each Poisson multigrid cycle is captured once per
  *                               grid and buffers as a CUDA graph and replayed; 0 = launched kernel
  *                               by kernel (same results).
@@ -78,7 +83,11 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               columns per tile; otherwise the register path).  Same results.
  *   "hpsi_variant":             0 (default) = the H psi kernel reads x/y neighbours through L1;
  *                               1 = through a shared-memory plane tile (at most 2 bands per
- *                               thread).  Results identical for every value.
+ *                               thread); 2 = plane tiles with their halo loaded by TMA
+ *                               (cp.async.bulk.tensor) into a 6-stage shared-memory ring, each
+ *                               block walking hpsi_bands_per_thread bands (0 = 4) of its column
+ *                               tile; needs nx and ld even and a 16-byte-aligned psi, else 0 is
+ *                               used.  Results identical for every value.
  *   "grid_barrier_poll_limit":  0 = 2^24 (default): polls a block of the persistent Jacobi
  *                               launch makes at a grid barrier before it gives up; the solve then
  *                               fails with DFT_CUDA_ERROR and the context stays usable.

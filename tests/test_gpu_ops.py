@@ -31,16 +31,49 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
-@pytest.fixture(params=[(0, 0), (0, 1), (0, 2), (0, 4), (1, 1), (1, 2)], ids=lambda t: f"v{t[0]}bpt{t[1]}")
+@pytest.fixture(params=[(0, 0), (0, 1), (0, 2), (0, 4), (1, 1), (1, 2), (2, 0), (2, 8)],
+                ids=lambda t: f"v{t[0]}bpt{t[1]}")
 def hpsi_bands_per_thread(request, engine):
     """Every H psi launch shape: neighbours through L1 (variant 0) with auto, 1, 2 or 4 bands per
-    thread, and the shared-memory plane tile (variant 1) with 1 or 2."""
+    thread, the shared-memory plane tile (variant 1) with 1 or 2, and the TMA plane ring
+    (variant 2, 4 or 8 bands per block; an odd leading dimension falls back to variant 0)."""
     variant, bpt = request.param
     engine.set_tuning("hpsi_variant", variant)
     engine.set_tuning("hpsi_bands_per_thread", bpt)
     yield request.param
     engine.set_tuning("hpsi_bands_per_thread", 0)
     engine.set_tuning("hpsi_variant", 0)
+
+
+@pytest.mark.parametrize("n,b", [((12, 9, 8), (-3.0, 3.4, -2.5, 2.9, -2.2, 2.0)),
+                                 ((34, 17, 21), (-4.0, 4.0, -2.0, 2.0, -2.5, 2.5)),
+                                 ((6, 6, 4), (-2.0, 2.2, -1.0, 1.5, -1.7, 1.3)),
+                                 ((70, 41, 37), (-7.0, 7.0, -4.0, 4.0, -3.6, 3.6)),
+                                 ((48, 48, 48), (-7.05, 7.05) * 3)])
+@pytest.mark.parametrize("nbc", [0, 1, 2, 8])
+def test_hpsi_tma_ring_bit_exact(engine, port, n, b, nbc):
+    """The TMA plane ring (hpsi_variant 2): even nx and ld, tiles that overhang the grid in x and
+    y, several z-chunks, band runs of 1, 2, 4 (auto) and 8 with a partial last run; every value
+    bit for bit (signed zeros included) against the oracle."""
+    rng = np.random.default_rng(12)
+    N = int(np.prod(n))
+    nb_, ld = 7, N + 38
+    V = rng.standard_normal(N)
+    psi = np.zeros((nb_, ld))
+    psi[:, :N] = rng.standard_normal((nb_, N))
+    psi[2, : N // 3] = 0.0  # runs of zeros: the skipped-neighbour order decides the sign of zero
+    dV, dP, dH = engine.upload(V), engine.upload(psi), engine.array(nb_ * ld)
+    engine.set_tuning("hpsi_variant", 2)
+    engine.set_tuning("hpsi_bands_per_thread", nbc)
+    try:
+        engine.apply_hamiltonian(G(n, b), dV, dP, dH, nb_, ld)
+        engine.synchronize()
+    finally:
+        engine.set_tuning("hpsi_bands_per_thread", 0)
+        engine.set_tuning("hpsi_variant", 0)
+    H = dH.to_host((nb_, ld))
+    for k in range(nb_):
+        assert H[k, :N].tobytes() == port.apply_hamiltonian(n, b, V, psi[k, :N]).tobytes(), k
 
 
 @pytest.mark.parametrize("n,b", GRIDS)
