@@ -49,7 +49,7 @@ class dft_scf_opts(C.Structure):
                 ("smearing_kt", C.c_double), ("kerker_q0", C.c_double),
                 ("stop_abs_deig", C.c_double), ("log_path", C.c_char_p), ("autotune", C.c_int),
                 ("initial_density", C.c_int),
-                ("hartree_boundary", C.c_int)]
+                ("hartree_boundary", C.c_int), ("poisson_predict", C.c_int)]
 
 
 class dft_autotune_report(C.Structure):
@@ -90,7 +90,8 @@ class dft_scf_iteration(C.Structure):
                 ("eig_iterations_alpha", C.c_int), ("eig_iterations_beta", C.c_int),
                 ("ms_hartree", C.c_double), ("ms_xc", C.c_double), ("ms_orbitals", C.c_double),
                 ("ms_density", C.c_double), ("ms_energy", C.c_double), ("ms_total", C.c_double),
-                ("eigenvalue_difference", C.c_double)]
+                ("eigenvalue_difference", C.c_double), ("poisson_cycles_in", C.c_int),
+                ("poisson_cycles_out", C.c_int)]
 
 
 class dft_scf_result(C.Structure):

@@ -139,7 +139,9 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     if (monopole) monopole_width(g);  // the origin must lie well inside the box
     DevBuf mrho(monopole ? (size_t)N : 0), mvc(monopole ? (size_t)N : 0), mvp0(monopole ? (size_t)N : 0),
         mvp1(monopole ? (size_t)N : 0);
+    int last_cycles = 0;  // multigrid cycles of the last solve
     auto poisson = [&](const double* d_in, double* v_out, bool have_prev) {
+        last_cycles = 0;
         const double* d = d_in;
         double* v = v_out;
         if (monopole) {
@@ -161,6 +163,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
                 cyc = info.cycles;
                 res = info.residual;
             }
+            last_cycles = cyc;
             if (o.verbose > 1)
                 fprintf(stderr, "[poisson] multigrid %d cycles, next Jacobi update %.3e, %.2f ms\n", cyc, res,
                         ms_since(t0));
@@ -267,6 +270,14 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     const double pbeta = o.pulay_beta > 0.0 ? o.pulay_beta : 0.2;
     if (o.mixer != 0 && o.mixer != 1) fail(DFT_INVALID_ARGUMENT, "unknown mixer %d", o.mixer);
     DevBuf phist(o.mixer == 1 ? (size_t)2 * pdepth * ns * N : 0);
+    // Hartree start from the mixer (option): V_H is linear in the density, so the mixer's
+    // combination of the stored V_H(n_in,i) and V_H(n_out,i) - V_H(n_in,i) is a start for the
+    // next V_H(n_in) that is as close as those solves were (the unchanged stop rule ends it)
+    if (o.poisson_predict != 0 && o.poisson_predict != 1)
+        fail(DFT_INVALID_ARGUMENT, "unknown poisson_predict %d", o.poisson_predict);
+    const bool vpredict = o.poisson_predict == 1 && pstart != DFT_POISSON_COLD;
+    DevBuf vhist(vpredict && o.mixer == 1 ? (size_t)2 * pdepth * N : 0);
+    DevBuf vtmp(vpredict && o.mixer == 1 && pdepth > 8 ? (size_t)N : 0);
     // Kerker screening of the total-charge residual (option; 0 = off, the reference's mixer)
     const double kq0 = o.kerker_q0;
     if (kq0 < 0.0 || !std::isfinite(kq0)) fail(DFT_INVALID_ARGUMENT, "kerker_q0 must be >= 0");
@@ -283,6 +294,11 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         if (!closed) {
             DFT_CUDA(cudaMemcpyAsync(hin + N, db.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
             sub(ctx, N, ob.p, db.p, hres + N);
+        }
+        if (vpredict) {
+            double* vin = vhist.p + (size_t)slot * 2 * N;
+            DFT_CUDA(cudaMemcpyAsync(vin, vh.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+            sub(ctx, N, ovh.p, vh.p, vin + N);
         }
         phead = (phead + 1) % pdepth;
         pcount = std::min(pcount + 1, pdepth);
@@ -356,6 +372,29 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             kerker_update(ctx, g, ns, dst, rr, kbuf.p + (size_t)ns * N, kbuf.p + (size_t)(ns + 1) * N, kq2, pbeta);
         }
         if (closed) DFT_CUDA(cudaMemcpyAsync(db.p, da.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (vpredict) {
+            // V = sum c_i (V_in,i + beta (V_out,i - V_in,i)); with Kerker screening the step's
+            // screened part is not known and the unscreened one stands in (only a start)
+            const double* a[16];
+            double cv[16];
+            for (int i = 0; i < m; ++i) a[i] = vhist.p + (size_t)i * 2 * N;
+            if (2 * m <= 16) {
+                for (int i = 0; i < m; ++i) {
+                    a[m + i] = a[i] + N;
+                    cv[i] = cf[i];
+                    cv[m + i] = pbeta * cf[i];
+                }
+                combine(ctx, N, 2 * m, a, cv, vh.p);
+            } else {
+                combine(ctx, N, m, a, cf.data(), vh.p);
+                for (int i = 0; i < m; ++i) {
+                    a[i] += N;
+                    cv[i] = pbeta * cf[i];
+                }
+                combine(ctx, N, m, a, cv, vtmp.p);
+                add_into(ctx, N, vh.p, vtmp.p, vh.p);
+            }
+        }
     };
 
     // ---- SCF loop, constants SelfConsistentFieldMolecule.cpp:27-31 ----------------------
@@ -411,6 +450,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         sync(ctx);
         rec.ms_hartree = ms_since(t0);
         rec.poisson_sweeps_in = jin.sweeps;
+        rec.poisson_cycles_in = last_cycles;
         // v_xc (:68-90): the closed-shell shortcut reuses alpha
         t0 = Clock::now();
         xc(ctx, g, kind, da.p, db.p, vxa.p, closed ? nullptr : vxb.p, false);
@@ -456,6 +496,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         sync(ctx);
         rec.ms_density = ms_since(t0);
         rec.poisson_sweeps_out = jout.sweeps;
+        rec.poisson_cycles_out = last_cycles;
         // energies (TotalEnergyMolecule.cpp:237-333): orbitals alpha then beta in one sum
         t0 = Clock::now();
         double T = 0.0;
@@ -523,12 +564,13 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
                          "{\"iteration\":%d,\"energy\":%s,\"energy_difference\":%s,\"density_difference\":%s,"
                          "\"ks_residual\":%s,\"mixing\":%s,\"kinetic\":%s,\"external\":%s,\"hartree\":%s,"
                          "\"exchange_correlation\":%s,\"nuclear_repulsion\":%s,\"poisson_sweeps_in\":%ld,"
-                         "\"poisson_sweeps_out\":%ld,\"eig_iterations_alpha\":%d,\"eig_iterations_beta\":%d,"
-                         "\"eigenvalue_difference\":%s,\"levels_alpha\":%s,\"levels_beta\":%s,\"ms_hartree\":%s,\"ms_xc\":%s,"
+                         "\"poisson_sweeps_out\":%ld,\"poisson_cycles_in\":%d,\"poisson_cycles_out\":%d,"
+                         "\"eig_iterations_alpha\":%d,\"eig_iterations_beta\":%d,\"eigenvalue_difference\":%s,\"levels_alpha\":%s,\"levels_beta\":%s,\"ms_hartree\":%s,\"ms_xc\":%s,"
                          "\"ms_orbitals\":%s,\"ms_density\":%s,\"ms_energy\":%s,\"ms_total\":%s}\n",
                          it, jnum(E[5]).c_str(), jnum(dE).c_str(), jnum(effd).c_str(), jnum(resid).c_str(),
                          jnum(rec.mixing).c_str(), jnum(E[0]).c_str(), jnum(E[1]).c_str(), jnum(E[2]).c_str(),
-                         jnum(E[3]).c_str(), jnum(E[4]).c_str(), jin.sweeps, jout.sweeps, rec.eig_iterations_alpha,
+                         jnum(E[3]).c_str(), jnum(E[4]).c_str(), jin.sweeps, jout.sweeps, rec.poisson_cycles_in,
+                         rec.poisson_cycles_out, rec.eig_iterations_alpha,
                          rec.eig_iterations_beta, jnum(deig).c_str(), jlevels(eiga, na).c_str(),
                          jlevels(closed ? eiga : eigb, nb).c_str(), jnum(rec.ms_hartree).c_str(),
                          jnum(rec.ms_xc).c_str(), jnum(rec.ms_orbitals).c_str(), jnum(rec.ms_density).c_str(),
@@ -584,6 +626,8 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             mix(ctx, N, da.p, oa.p, imix);
             mix(ctx, N, db.p, ob.p, imix);
         }
+        if (vpredict && o.mixer == 0) mix(ctx, N, vh.p, ovh.p, imix);  // V_in + m (V_out - V_in)
+        if (vpredict && monopole) sub(ctx, N, vh.p, mvc.p, mvp0.p);   // the zero-face part's start
         prevD = effd;
         prevE = E[5];
     }

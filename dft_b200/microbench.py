@@ -95,6 +95,7 @@ def main():
     ap.add_argument("--pulay-beta", type=float, default=0.0, help="scf: Pulay step (0 = 0.2)")
     ap.add_argument("--pulay-depth", type=int, default=0, help="scf: Pulay history (0 = 8)")
     ap.add_argument("--boundary", type=int, default=0, help="scf: Hartree faces, 0 reference, 1 Q/|r| (monopole)")
+    ap.add_argument("--predict", type=int, default=0, help="scf: V_H(n_in) start from the mixer's combination (1)")
     ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args()
     import torch
@@ -161,7 +162,7 @@ def main():
                                   poisson_start=POISSON[a.poisson], mixer=a.mixer, adaptive_eig_tol=a.adaptive,
                                   smearing_kt=a.smearing, kerker_q0=a.kerker, initial_density=a.atoms,
                                   pulay_beta=a.pulay_beta, pulay_depth=a.pulay_depth,
-                                  hartree_boundary=a.boundary)
+                                  hartree_boundary=a.boundary, poisson_predict=a.predict)
         if net is not None:
             o.poisson_net = net.handle
         o.eig.verbose = int(a.verbose > 2)
@@ -174,7 +175,7 @@ def main():
                    seconds=r.seconds, launches=eng.launches, eigenvalues=r.eigenvalues[:8],
                    history=[{k: h[k] for k in ("iteration", "energy", "energy_difference", "density_difference",
                                                "ks_residual", "eigenvalue_difference", "poisson_sweeps_in",
-                                               "poisson_sweeps_out",
+                                               "poisson_sweeps_out", "poisson_cycles_in", "poisson_cycles_out",
                                                "eig_iterations_alpha", "ms_hartree", "ms_xc", "ms_orbitals",
                                                "ms_density", "ms_energy", "ms_total")} for h in r.history])
     elif a.mode == "poisson":

@@ -311,6 +311,10 @@ typedef struct {
                                 1: Q/|r| on every face (monopole), through a Gaussian compensation
                                 charge and the same zero-face solvers; the wall states that zero
                                 faces bind for many electrons do not form */
+    int poisson_predict;     /* 1: start each V_H(n_in) solve (any poisson_start but COLD) from the
+                                mixer's own combination of the stored V_H(n_in,i) and V_H(n_out,i)
+                                (V_H is linear in n), instead of the slot's previous potential (0).
+                                The stop rule is unchanged; only the cycles/sweeps to reach it drop */
 } dft_scf_opts;
 
 /* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)
@@ -322,6 +326,8 @@ typedef struct {
     int eig_iterations_alpha, eig_iterations_beta;
     double ms_hartree, ms_xc, ms_orbitals, ms_density, ms_energy, ms_total;
     double eigenvalue_difference;  /* max |change| of the occupied eigenvalues since the previous iteration */
+    int poisson_cycles_in, poisson_cycles_out;  /* multigrid cycles before the Jacobi stop rule
+                                                   (DFT_POISSON_MULTIGRID start; 0 otherwise) */
 } dft_scf_iteration;
 
 typedef struct {

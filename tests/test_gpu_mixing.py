@@ -89,3 +89,42 @@ def test_kerker_rejects_negative_q0(engine):
     with pytest.raises(dft_b200.DFTError) as ei:
         engine.scf_molecule(g, m, 0, 1, "PZ81", dft_b200.default_scf_options(kerker_q0=-1.0))
     assert ei.value.status == dft_b200.DFT_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("mixer,q0,mult", [(1, 0.0, 1), (0, 0.0, 1), (1, 0.8, 1), (1, 0.0, 2)])
+def test_poisson_predict_same_energy_fewer_cycles(engine, mixer, q0, mult):
+    """The mixer's own V_H combination as the start of each V_H(n_in) solve (poisson_predict)
+    ends at the same Jacobi stop rule: the same energy as the previous-potential start, with
+    fewer multigrid cycles for n_in after the first iterations (Pulay, linear, Pulay + Kerker,
+    open shell)."""
+    g = dft_b200.CartesianGrid(32, 32, 32, -6.2, 6.2, -6.2, 6.2, -6.2, 6.2)
+    m = dft_b200.Molecule()
+    if mult == 1:
+        m.addNucleus(1, -0.7, 0.0, 0.0)
+        m.addNucleus(1, 0.7, 0.0, 0.0)
+    else:
+        m.addNucleus(1, -1.6, 0.0, 0.0)
+        m.addNucleus(1, 0.0, 0.1, 0.0)
+        m.addNucleus(1, 1.6, 0.0, 0.0)
+    res = {}
+    for pp in (0, 1):
+        o = dft_b200.default_scf_options(stop_abs_de=1e-8, poisson_start=dft_b200.POISSON_MULTIGRID, mixer=mixer,
+                                         kerker_q0=q0, poisson_predict=pp)
+        r = engine.scf_molecule(g, m, 0, mult, "PBE96", o)
+        assert r.converged or r.energyDifference < 1e-8
+        res[pp] = (r.total, [h["poisson_cycles_in"] for h in r.history], r.eigenvalues)
+    print(mixer, q0, mult, res)
+    assert abs(res[1][0] - res[0][0]) < 1e-7
+    assert np.max(np.abs(np.subtract(res[1][2], res[0][2]))) < 1e-6
+    n = min(len(res[0][1]), len(res[1][1]))
+    assert sum(res[1][1][2:n]) < 0.7 * sum(res[0][1][2:n]), res
+
+
+def test_poisson_predict_rejects_unknown(engine):
+    g = dft_b200.CartesianGrid(12, 12, 12, -3.0, 3.0, -3.0, 3.0, -3.0, 3.0)
+    m = dft_b200.Molecule()
+    m.addNucleus(1, -0.7, 0.05, 0.0)
+    m.addNucleus(1, 0.7, 0.05, 0.0)
+    with pytest.raises(dft_b200.DFTError) as ei:
+        engine.scf_molecule(g, m, 0, 1, "PZ81", dft_b200.default_scf_options(poisson_predict=3, max_iterations=1))
+    assert ei.value.status == dft_b200.DFT_INVALID_ARGUMENT
