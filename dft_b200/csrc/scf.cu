@@ -273,9 +273,12 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     // Hartree start from the mixer (option): V_H is linear in the density, so the mixer's
     // combination of the stored V_H(n_in,i) and V_H(n_out,i) - V_H(n_in,i) is a start for the
     // next V_H(n_in) that is as close as those solves were (the unchanged stop rule ends it)
-    if (o.poisson_predict != 0 && o.poisson_predict != 1)
+    if (o.poisson_predict < 0 || o.poisson_predict > 2)
         fail(DFT_INVALID_ARGUMENT, "unknown poisson_predict %d", o.poisson_predict);
-    const bool vpredict = o.poisson_predict == 1 && pstart != DFT_POISSON_COLD;
+    const bool vpredict = o.poisson_predict >= 1 && pstart != DFT_POISSON_COLD;
+    // 2: also V_H(n_out) from V_H(n_in) + the previous iteration's V_H(n_out) - V_H(n_in)
+    const bool vpredict_out = o.poisson_predict == 2 && pstart != DFT_POISSON_COLD;
+    DevBuf vres(vpredict_out ? (size_t)N : 0);
     DevBuf vhist(vpredict && o.mixer == 1 ? (size_t)2 * pdepth * N : 0);
     DevBuf vtmp(vpredict && o.mixer == 1 && pdepth > 8 ? (size_t)N : 0);
     // Kerker screening of the total-charge residual (option; 0 = off, the reference's mixer)
@@ -492,7 +495,12 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         if (closed) DFT_CUDA(cudaMemcpyAsync(ob.p, oa.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
         else spin_density(ctx, N, psib.p, bands_b, ld, occb.data(), ob.p);
         add2(ctx, N, oa.p, ob.p, orho.p);
+        if (vpredict_out && it > 1) {
+            add_into(ctx, N, vh.p, vres.p, ovh.p);
+            if (monopole) sub(ctx, N, ovh.p, mvc.p, mvp1.p);
+        }
         JacobiResult jout = poisson(orho.p, ovh.p, it > 1);
+        if (vpredict_out) sub(ctx, N, ovh.p, vh.p, vres.p);
         sync(ctx);
         rec.ms_density = ms_since(t0);
         rec.poisson_sweeps_out = jout.sweeps;

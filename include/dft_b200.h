@@ -313,8 +313,10 @@ typedef struct {
                                 faces bind for many electrons do not form */
     int poisson_predict;     /* 1: start each V_H(n_in) solve (any poisson_start but COLD) from the
                                 mixer's own combination of the stored V_H(n_in,i) and V_H(n_out,i)
-                                (V_H is linear in n), instead of the slot's previous potential (0).
-                                The stop rule is unchanged; only the cycles/sweeps to reach it drop */
+                                (V_H is linear in n), instead of the slot's previous potential (0);
+                                2: as 1, and each V_H(n_out) solve from V_H(n_in) plus the previous
+                                iteration's V_H(n_out) - V_H(n_in).  The stop rule is unchanged;
+                                only the cycles/sweeps to reach it drop */
 } dft_scf_opts;
 
 /* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)

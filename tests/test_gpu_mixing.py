@@ -93,10 +93,10 @@ def test_kerker_rejects_negative_q0(engine):
 
 @pytest.mark.parametrize("mixer,q0,mult", [(1, 0.0, 1), (0, 0.0, 1), (1, 0.8, 1), (1, 0.0, 2)])
 def test_poisson_predict_same_energy_fewer_cycles(engine, mixer, q0, mult):
-    """The mixer's own V_H combination as the start of each V_H(n_in) solve (poisson_predict)
-    ends at the same Jacobi stop rule: the same energy as the previous-potential start, with
-    fewer multigrid cycles for n_in after the first iterations (Pulay, linear, Pulay + Kerker,
-    open shell)."""
+    """The mixer's own V_H combination as the start of each V_H(n_in) solve (poisson_predict 1,
+    and 2 with the V_H(n_out) start as well) ends at the same Jacobi stop rule: the same energy
+    as the previous-potential start, with fewer multigrid cycles for n_in after the first
+    iterations (Pulay, linear, Pulay + Kerker, open shell)."""
     g = dft_b200.CartesianGrid(32, 32, 32, -6.2, 6.2, -6.2, 6.2, -6.2, 6.2)
     m = dft_b200.Molecule()
     if mult == 1:
@@ -107,17 +107,19 @@ def test_poisson_predict_same_energy_fewer_cycles(engine, mixer, q0, mult):
         m.addNucleus(1, 0.0, 0.1, 0.0)
         m.addNucleus(1, 1.6, 0.0, 0.0)
     res = {}
-    for pp in (0, 1):
+    for pp in (0, 1, 2):
         o = dft_b200.default_scf_options(stop_abs_de=1e-8, poisson_start=dft_b200.POISSON_MULTIGRID, mixer=mixer,
                                          kerker_q0=q0, poisson_predict=pp)
         r = engine.scf_molecule(g, m, 0, mult, "PBE96", o)
         assert r.converged or r.energyDifference < 1e-8
-        res[pp] = (r.total, [h["poisson_cycles_in"] for h in r.history], r.eigenvalues)
+        res[pp] = (r.total, [h["poisson_cycles_in"] for h in r.history], r.eigenvalues,
+                   [h["poisson_cycles_out"] for h in r.history])
     print(mixer, q0, mult, res)
-    assert abs(res[1][0] - res[0][0]) < 1e-7
-    assert np.max(np.abs(np.subtract(res[1][2], res[0][2]))) < 1e-6
-    n = min(len(res[0][1]), len(res[1][1]))
-    assert sum(res[1][1][2:n]) < 0.7 * sum(res[0][1][2:n]), res
+    for pp in (1, 2):
+        assert abs(res[pp][0] - res[0][0]) < 1e-7
+        assert np.max(np.abs(np.subtract(res[pp][2], res[0][2]))) < 1e-6
+        n = min(len(res[0][1]), len(res[pp][1]))
+        assert sum(res[pp][1][2:n]) < 0.7 * sum(res[0][1][2:n]), res
 
 
 def test_poisson_predict_rejects_unknown(engine):
