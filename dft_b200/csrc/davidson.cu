@@ -251,8 +251,15 @@ struct Blocks {
 
 // Narrow Gram products (ka <= 64, kb <= KB): one launch.  Warp w of every block owns rows
 // i = w, w + 8, ... of A (RPW of them) and all kb columns; its lanes stride the points and
-// keep RPW x KB sums in registers.  Block partials go to `partial`; the last block to finish
-// (ticket) adds them in block order (deterministic) and writes dV * C.
+// keep RPW x KB sums in registers.  Block partials go to `partial`; the partials are then
+// added in two fixed-order levels inside the same launch: the last block to finish in each
+// group of GS_GROUP blocks (ticket[1 + group]) adds its group's partials, and the last group
+// to finish (ticket[0]) adds the group sums and writes dV * C.  Every thread of a reducing
+// block owns whole elements and issues its (at most GS_GROUP) loads at once, so the tail is a
+// few L2 round trips instead of one dependent chain per element.
+constexpr int GS_GROUP = 16;
+constexpr int GS_TICKETS = 256;  // ticket words: 1 + groups (blocks <= 4 x SMs)
+
 template <int RPW, int KB>
 __global__ void __launch_bounds__(256) gram_small_kernel(const double* __restrict__ A, long long lda, int ka,
                                                          const double* __restrict__ B, long long ldb, int kb,
@@ -294,21 +301,49 @@ __global__ void __launch_bounds__(256) gram_small_kernel(const double* __restric
             const int i = warp + 8 * r;
             if (lane == 0 && i < ka && j < kb) mine[i * kb + j] = v;
         }
-    // last block: sum the partials in block order
+    // level 1: the last block of this group adds the group's partials in block order
+    const int nblk = (int)gridDim.x;
+    const int ngroups = (nblk + GS_GROUP - 1) / GS_GROUP;
+    const int grp = (int)blockIdx.x / GS_GROUP;
+    const int g0 = grp * GS_GROUP;
+    const int gsz = min(GS_GROUP, nblk - g0);
+    double* gsum = partial + (long long)nblk * nel;  // [ngroups][nel]
     __shared__ bool last;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) last = atomicAdd(ticket + 1 + grp, 1u) == (unsigned)gsz - 1;
     __syncthreads();
     if (!last) return;
     __threadfence();
-    for (int e = warp; e < nel; e += 8) {
-        double v = 0.0;
-        for (int c = lane; c < (int)gridDim.x; c += 32) v += __ldcg(partial + (long long)c * nel + e);
-        v = warp_sum(v);
-        if (lane == 0) out[e] = v * scale;
+    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+        double v[GS_GROUP];
+#pragma unroll
+        for (int c = 0; c < GS_GROUP; ++c) v[c] = c < gsz ? __ldcg(partial + (long long)(g0 + c) * nel + e) : 0.0;
+        double sum = 0.0;
+#pragma unroll
+        for (int c = 0; c < GS_GROUP; ++c) sum += v[c];
+        gsum[(long long)grp * nel + e] = sum;
     }
-    if (threadIdx.x == 0) *ticket = 0;  // ready for the next call
+    if (threadIdx.x == 0) ticket[1 + grp] = 0;  // ready for the next call
+    // level 2: the last group adds the group sums in group order
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == (unsigned)ngroups - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+        double sum = 0.0;
+        for (int c0 = 0; c0 < ngroups; c0 += 8) {
+            double v[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) v[c] = c0 + c < ngroups ? __ldcg(gsum + (long long)(c0 + c) * nel + e) : 0.0;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) sum += v[c];
+        }
+        out[e] = sum * scale;
+    }
+    if (threadIdx.x == 0) *ticket = 0;
 }
 
 // C (ka x kb, host, row-major) = dV * A^T B
@@ -321,12 +356,15 @@ void gram(dft_context* ctx, const Grid& g, const double* A, long long lda, int k
     if (ka <= 64 && kb <= 16 && rpw * kbt <= 64) {
         // narrow product: one launch, the last block reduces
         const size_t nel = (size_t)ka * kb;
-        const int nblk = (int)std::max<long long>(1, std::min<long long>(4LL * ctx->num_sms, (g.N + 255) / 256));
-        double* partial = (double*)ws_get(ctx, WS_SMALL, sizeof(double) * (nel * nblk + nel) + 64);
-        double* res = partial + nel * nblk;
+        const int nblk = (int)std::max<long long>(
+            1, std::min<long long>(std::min(4LL * ctx->num_sms, (long long)(GS_TICKETS - 1) * GS_GROUP),
+                                   (g.N + 255) / 256));
+        const int ngroups = (nblk + GS_GROUP - 1) / GS_GROUP;
+        double* partial = (double*)ws_get(ctx, WS_SMALL, sizeof(double) * (nel * (nblk + ngroups) + nel) + 64);
+        double* res = partial + nel * (nblk + ngroups);
         if (!ctx->gram_ticket) {
-            DFT_CUDA(cudaMalloc(&ctx->gram_ticket, 64));
-            DFT_CUDA(cudaMemsetAsync(ctx->gram_ticket, 0, 64, ctx->stream));
+            DFT_CUDA(cudaMalloc(&ctx->gram_ticket, sizeof(unsigned int) * GS_TICKETS));
+            DFT_CUDA(cudaMemsetAsync(ctx->gram_ticket, 0, sizeof(unsigned int) * GS_TICKETS, ctx->stream));
         }
         unsigned int* tk = (unsigned int*)ctx->gram_ticket;
 #define DFT_GS(R, K)                                                                                          \

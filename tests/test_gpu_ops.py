@@ -313,3 +313,23 @@ def test_block_davidson_vs_reference_algorithm(engine, port, case, precond):
         hp = port.apply_hamiltonian(n, b, V, P[k])
         r = np.sqrt(np.sum((hp - eig[k] * P[k]) ** 2) * dV)
         assert r < 1e-7
+
+
+@pytest.mark.parametrize("n", [(6, 5, 4), (48, 48, 48), (96, 96, 97)])
+@pytest.mark.parametrize("ka,kb", [(1, 1), (5, 3), (20, 4), (64, 16), (33, 9)])
+def test_gram_narrow_fp64(engine, n, ka, kb):
+    """The one-launch narrow FP64 Gram (ka <= 64, kb <= 16; two-level in-launch reduction over
+    groups of 16 blocks, the last group partial): dV * A^T B against numpy to 1e-13, and
+    repeated calls are bitwise identical (fixed summation order, tickets reset)."""
+    g = G(n, (-4.0, 4.0) * 3)
+    N = g.getSize()
+    rng = np.random.default_rng(ka * 100 + kb)
+    A = rng.standard_normal((ka, N))
+    B = rng.standard_normal((kb, N))
+    dA, dB = engine.upload(A), engine.upload(B)
+    c1 = engine.gram(g, dA, N, ka, dB, N, kb, precision=0)
+    c2 = engine.gram(g, dA, N, ka, dB, N, kb, precision=0)
+    dV = g.getDx() * g.getDy() * g.getDz()
+    ref = (A @ B.T) * dV
+    assert np.max(np.abs(np.asarray(c1) - ref)) < 1e-14 * N * dV
+    assert np.array_equal(np.asarray(c1), np.asarray(c2))
