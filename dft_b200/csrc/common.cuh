@@ -113,6 +113,7 @@ struct dft_context {
     int hpsi_variant = 0;              // H psi: 0 = neighbours through L1, 1 = shared-memory plane tile,
                                        // 2 = TMA plane ring (where eligible, else 0)
     int* dev_status = nullptr;         // device word set by kernels whose bounded waits gave up
+    int ortho_adaptive = 1;            // FP64 orthonormalisation: skip the second pass when safe (1)
     int tc_ring = 0;                   // tensor-core Gram: cp.async ring variant (1) or register staging (0)
     long long grid_barrier_poll_limit = 0;  // persistent Jacobi barrier polls before giving up (0 = 2^24)
     // autotuner choices per grid (nx, ny, nz) -> {H psi bands per thread, Jacobi sweeps per launch},

@@ -527,6 +527,21 @@ int orthonormalise(dft_context* ctx, const Grid& g, const double* V, int k, doub
                     rotate(ctx, g, V, ld, k + nt, Yc, nt, W, ld, 1.0, 0.0);
                 DFT_CUDA(cudaMemcpyAsync(T, W, sizeof(double) * (size_t)ld * nt, cudaMemcpyDeviceToDevice,
                                          ctx->stream));
+                // In FP64 one pass suffices when the block was far from dependent: the loss of
+                // orthogonality of projected Cholesky QR is about eps * r * kappa(S), with
+                // r = max_i (T^T T)_ii / S_ii (the cancellation of the projection) and
+                // kappa(S) <= trace(S) ||L^-T||_F^2.  Below 1e-12 the second pass is skipped.
+                if (!tc && pass == 0 && ctx->ortho_adaptive) {
+                    double r = 1.0, tr = 0.0, yf = 0.0;
+                    for (int i = 0; i < nt; ++i) {
+                        const double sii = S[(size_t)i * nt + i];
+                        r = std::max(r, M[(size_t)(k + i) * nt + i] / sii);
+                        tr += sii;
+                    }
+                    for (double v : Yk) yf += v * v;
+                    const double est = 2.2204460492503131e-16 * 16.0 * r * tr * yf;
+                    if (std::isfinite(est) && est < 1e-12) break;
+                }
                 continue;
             }
             // nearly dependent: project with the C already at hand, then the explicit path below

@@ -96,11 +96,15 @@ def main():
     ap.add_argument("--pulay-depth", type=int, default=0, help="scf: Pulay history (0 = 8)")
     ap.add_argument("--boundary", type=int, default=0, help="scf: Hartree faces, 0 reference, 1 Q/|r| (monopole)")
     ap.add_argument("--predict", type=int, default=0, help="scf: V_H(n_in) start from the mixer's combination (1)")
+    ap.add_argument("--tuning", default="", help="context tuning keys, e.g. orthonormalise_adaptive=0,hpsi_variant=2")
     ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args()
     import torch
 
     eng = d.Engine(0)
+    for kv in filter(None, a.tuning.split(",")):
+        key, val = kv.split("=")
+        eng.set_tuning(key.strip(), int(val))
     eng.set_tuning("jacobi_sweeps_per_launch", a.spl)
     eng.set_tuning("network_tensor_cores", a.tc)
     eng.set_tuning("hpsi_bands_per_thread", a.bpt)

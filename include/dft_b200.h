@@ -91,6 +91,10 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *   "grid_barrier_poll_limit":  0 = 2^24 (default): polls a block of the persistent Jacobi
  *                               launch makes at a grid barrier before it gives up; the solve then
  *                               fails with DFT_CUDA_ERROR and the context stays usable.
+ *   "orthonormalise_adaptive":  1 (default) = the FP64 orthonormalisation of new eigensolver
+ *                               directions stops after one projected Cholesky QR pass when its
+ *                               estimated loss of orthogonality (eps * cancellation * condition
+ *                               bound) is below 1e-12; 0 = always two passes.
  *   "radial_pivot_exponent":    -14 (default): a pivot of the radial inverse iteration's Thomas
  *                               factorisation below 10^value in magnitude is singular; the run's
  *                               status becomes DFT_SINGULAR (reference NumericalMethods.cpp:105-122). */
