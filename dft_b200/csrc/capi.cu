@@ -155,6 +155,9 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
         } else if (k == "hpsi_variant") {
             NEED(value >= 0 && value <= 2, "hpsi_variant must be 0, 1 or 2");
             ctx->hpsi_variant = (int)value;
+        } else if (k == "tensor_core_tma") {
+            NEED(value == 0 || value == 1, "tensor_core_tma must be 0 or 1");
+            ctx->tc_tma = (int)value;
         } else if (k == "orthonormalise_adaptive") {
             NEED(value == 0 || value == 1, "orthonormalise_adaptive must be 0 or 1");
             ctx->ortho_adaptive = (int)value;

@@ -115,6 +115,7 @@ struct dft_context {
     int* dev_status = nullptr;         // device word set by kernels whose bounded waits gave up
     int ortho_adaptive = 1;            // FP64 orthonormalisation: skip the second pass when safe (1)
     int tc_ring = 0;                   // tensor-core Gram: cp.async ring variant (1) or register staging (0)
+    int tc_tma = 0;                    // tensor-core Gram: TMA-fed FP64 ring (1; before tc_ring)
     long long grid_barrier_poll_limit = 0;  // persistent Jacobi barrier polls before giving up (0 = 2^24)
     // autotuner choices per grid (nx, ny, nz) -> {H psi bands per thread, Jacobi sweeps per launch},
     // used where the corresponding knob is 0 (auto)

@@ -584,6 +584,190 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NC));
 }
 
+// TMA variant of the Gram tile (tuning key "tensor_core_tma"): one elected thread loads each
+// 16-point K slice of the A tile (128 rows) and the B tile (NC rows) with cp.async.bulk.tensor
+// (2-D maps over [rows, points], 128-byte swizzle, rows past ka/kb and points past n
+// zero-filled) into a ring of S FP64 stages tracked by mbarriers with transaction counts, so
+// S - 1 slices are in flight per block and no registers hold them; the warps then split each
+// slice from shared memory into the TF32 hi/lo planes of one of two operand stages (the same
+// K-major core-matrix layout and MMAs as gram_tc_kernel, K = 16 per slice).  With the swizzle,
+// a warp's reads of 8 rows x 4 points of a slice and its 128-byte core-matrix stores are both
+// free of bank conflicts.  Needs even leading dimensions and 16-byte-aligned A and B.
+constexpr int TT_KT = 16;  // points per slice: one 128-byte swizzle row of FP64 per band
+
+template <int NC>
+struct TmaCfg {
+    static constexpr int S = NC <= 128 ? 4 : 2;     // FP64 ring stages
+    static constexpr int A_BYTES = TC_M * TT_KT * 8;  // FP64 A slice = A hi + lo planes
+    static constexpr int B_BYTES = NC * TT_KT * 8;
+    static constexpr int STAGE = A_BYTES + B_BYTES;
+    static constexpr size_t SMEM = (size_t)STAGE * (S + 2) + 1024;
+};
+
+template <int NC>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    gram_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int ka, int kb,
+                    long long n, long long chunk, double* __restrict__ partial, int* __restrict__ error) {
+    using Cfg = TmaCfg<NC>;
+    constexpr int S = Cfg::S;
+    extern __shared__ uint8_t smraw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t mmab[2];
+    constexpr int NW = TC_THREADS / 32;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TC_M, n0 = blockIdx.y * NC;
+    const int mrows = min(TC_M, ka - m0), nrows = min(NC, kb - n0);
+    const long long p0 = (long long)blockIdx.z * chunk, p1 = min(n, p0 + chunk);
+    const int nslices = p1 > p0 ? (int)((p1 - p0 + TT_KT - 1) / TT_KT) : 0;
+    uint8_t* fp64 = sm;                         // S stages: A slice then B slice, row-major, swizzled
+    uint8_t* opnd = sm + (size_t)S * Cfg::STAGE;  // 2 stages: A hi, A lo, B hi, B lo
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(NC));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int q = 0; q < S; ++q) mbar_init(&full[q], 1);
+        mbar_init(&mmab[0], 1);
+        mbar_init(&mmab[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = idesc_tf32(NC);
+    int issued = 0;
+    auto issue = [&](int q) {  // slice q into FP64 stage q % S (thread 0)
+        uint8_t* st = fp64 + (size_t)(q % S) * Cfg::STAGE;
+        const uint32_t bar = smem_u32(&full[q % S]);
+        const int x = (int)(p0 + (long long)q * TT_KT);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(Cfg::STAGE) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+            "[%4];" ::"r"(smem_u32(st)),
+            "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(x), "r"(m0), "r"(bar)
+            : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+            "[%4];" ::"r"(smem_u32(st + Cfg::A_BYTES)),
+            "l"(reinterpret_cast<uint64_t>(&tmB)), "r"(x), "r"(n0), "r"(bar)
+            : "memory");
+    };
+    if (tid == 0)
+        for (; issued < nslices && issued < S; ++issued) issue(issued);
+    bool ok = true;
+    int waited_full = 0;  // slices whose TMA this thread has waited for
+    int s = 0;
+    // element (row, k) of a swizzled FP64 slice: 16-byte chunk k/2 of row `row` is stored at
+    // chunk (k/2) ^ (row % 8) (128-byte swizzle)
+    auto fp_at = [](const uint8_t* base, int row, int k) {
+        return *(const double*)(base + row * 128 + ((((k >> 1) ^ (row & 7)) << 4) | ((k & 1) << 3)));
+    };
+    for (; s < nslices; ++s) {
+        const int fs = s % S, os = s & 1;
+        if (s >= 2 && !mbar_wait(&mmab[os], (uint32_t)(((s - 2) >> 1) & 1))) ok = false;
+        if (ok && !mbar_wait(&full[fs], (uint32_t)((s / S) & 1))) ok = false;
+        if (ok) waited_full = s + 1;
+        if (!__syncthreads_and(ok)) break;
+        const uint8_t* fa = fp64 + (size_t)fs * Cfg::STAGE;
+        const uint8_t* fb = fa + Cfg::A_BYTES;
+        uint32_t* ahi = (uint32_t*)(opnd + (size_t)os * Cfg::STAGE);
+        uint32_t* alo = ahi + TC_M * TT_KT;
+        uint32_t* bhi = alo + TC_M * TT_KT;
+        uint32_t* blo = bhi + NC * TT_KT;
+        // core matrix cm = kc * (R/8) + rg holds rows 8 rg .. +7, points 4 kc .. +3; lane l
+        // owns row 8 rg + l/4, point 4 kc + l%4, i.e. word 32 cm + l
+#pragma unroll
+        for (int i = 0; i < (TC_M * TT_KT / 32) / NW; ++i) {
+            const int cm = warp + i * NW, kc = cm / (TC_M / 8), rg = cm % (TC_M / 8);
+            const double x = fp_at(fa, rg * 8 + (lane >> 2), kc * 4 + (lane & 3));
+            const uint32_t h = to_tf32((float)x);
+            ahi[cm * 32 + lane] = h;
+            alo[cm * 32 + lane] = to_tf32((float)(x - (double)__uint_as_float(h)));
+        }
+#pragma unroll
+        for (int i = 0; i < (NC * TT_KT / 32) / NW; ++i) {
+            const int cm = warp + i * NW, kc = cm / (NC / 8), rg = cm % (NC / 8);
+            const double x = fp_at(fb, rg * 8 + (lane >> 2), kc * 4 + (lane & 3));
+            const uint32_t h = to_tf32((float)x);
+            bhi[cm * 32 + lane] = h;
+            blo[cm * 32 + lane] = to_tf32((float)(x - (double)__uint_as_float(h)));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            constexpr uint32_t lbo_a = (TC_M / 8) * 128, lbo_b = (uint32_t)(NC / 8) * 128, sbo = 128;
+            const uint32_t sa_hi = smem_u32(ahi), sa_lo = smem_u32(alo), sb_hi = smem_u32(bhi), sb_lo = smem_u32(blo);
+#pragma unroll
+            for (int kk = 0; kk < TT_KT / 8; ++kk) {
+                const uint32_t oa = kk * 2 * lbo_a, ob = kk * 2 * lbo_b;
+                const uint64_t dah = smem_desc(sa_hi + oa, lbo_a, sbo), dal = smem_desc(sa_lo + oa, lbo_a, sbo);
+                const uint64_t dbh = smem_desc(sb_hi + ob, lbo_b, sbo), dbl = smem_desc(sb_lo + ob, lbo_b, sbo);
+                const uint32_t first = (s == 0 && kk == 0) ? 0u : 1u;
+                mma_tf32(tmem, dah, dbh, idesc, first);
+                mma_tf32(tmem, dah, dbl, idesc, 1u);
+                mma_tf32(tmem, dal, dbh, idesc, 1u);
+            }
+            mma_commit(&mmab[os]);
+            // every thread has split FP64 stage fs (barrier above): refill it with slice s + S
+            if (issued < nslices) issue(issued++);
+        }
+    }
+    // drain: the last two slices' MMAs, then (after a give-up) the TMA loads still in flight
+    for (int q = max(0, s - 2); q < s; ++q)
+        if (!mbar_wait(&mmab[q & 1], (uint32_t)((q >> 1) & 1))) ok = false;
+    if (tid == 0)
+        for (int q = waited_full; q < issued; ++q) mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
+    ok = __syncthreads_and(ok);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    double* out = partial + (long long)blockIdx.z * ka * kb;
+    if (!ok) {
+        if (tid == 0) atomicExch(error, 1);
+    } else if (nslices > 0) {
+        const int q4 = warp & 3, half = warp >> 2;
+        const int row = q4 * 32 + lane;
+        constexpr int CH = NC / (NW / 4);
+        for (int c0 = half * CH; c0 < half * CH + CH; c0 += 8) {
+            uint32_t v[8];
+            const uint32_t addr = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7])
+                         : "r"(addr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < mrows)
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (c0 + q < nrows) out[(long long)(m0 + row) * kb + (n0 + c0 + q)] = (double)__uint_as_float(v[q]);
+        }
+    } else {
+        for (int e = tid; e < mrows * nrows; e += TC_THREADS)
+            out[(long long)(m0 + e / nrows) * kb + (n0 + e % nrows)] = 0.0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NC));
+}
+
+// 2-D map over rows x points of a band block (row stride ld doubles), box 16 points x rows
+CUtensorMap band_tensor_map(const double* base, long long ld, long long n, int rows, int box_rows) {
+    CUtensorMap tm;
+    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+    const cuuint32_t box[2] = {TT_KT, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = tensor_map_encoder()(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims,
+                                            strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(DFT_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return tm;
+}
+
 }  // namespace
 
 // C (ka x kb, host, row-major) = dV * A^T B on the tensor cores (TF32 hi+lo split).
@@ -617,10 +801,51 @@ void gram_tc(dft_context* ctx, const Grid& g, const double* A, long long lda, in
         attr = true;
     }
     DFT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+    const bool tma = ctx->tc_tma && lda % 2 == 0 && ldb % 2 == 0 && ((uintptr_t)A & 15) == 0 &&
+                     ((uintptr_t)B & 15) == 0 && tensor_map_encoder() != nullptr;
+    if (tma) {
+        // tiles of exactly ncols columns (the B box); rows past kb are zero-filled by the copy
+        static bool tattr = false;
+        if (!tattr) {
+            DFT_CUDA(cudaFuncSetAttribute(gram_tma_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)TmaCfg<32>::SMEM));
+            DFT_CUDA(cudaFuncSetAttribute(gram_tma_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)TmaCfg<64>::SMEM));
+            DFT_CUDA(cudaFuncSetAttribute(gram_tma_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)TmaCfg<128>::SMEM));
+            DFT_CUDA(cudaFuncSetAttribute(gram_tma_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)TmaCfg<256>::SMEM));
+            tattr = true;
+        }
+        const int nt2 = (kb + ncols - 1) / ncols;
+        const CUtensorMap tmA = band_tensor_map(A, lda, g.N, ka, TC_M);
+        const CUtensorMap tmB = band_tensor_map(B, ldb, g.N, kb, ncols);
+        const dim3 grid2(mtiles, nt2, (unsigned)nch);
+        switch (ncols) {
+            case 32:
+                gram_tma_kernel<32><<<grid2, TC_THREADS, TmaCfg<32>::SMEM, ctx->stream>>>(tmA, tmB, ka, kb, g.N, chunk,
+                                                                                         partial, err);
+                break;
+            case 64:
+                gram_tma_kernel<64><<<grid2, TC_THREADS, TmaCfg<64>::SMEM, ctx->stream>>>(tmA, tmB, ka, kb, g.N, chunk,
+                                                                                         partial, err);
+                break;
+            case 128:
+                gram_tma_kernel<128><<<grid2, TC_THREADS, TmaCfg<128>::SMEM, ctx->stream>>>(tmA, tmB, ka, kb, g.N,
+                                                                                           chunk, partial, err);
+                break;
+            default:
+                gram_tma_kernel<256><<<grid2, TC_THREADS, TmaCfg<256>::SMEM, ctx->stream>>>(tmA, tmB, ka, kb, g.N,
+                                                                                           chunk, partial, err);
+                break;
+        }
+    }
     const dim3 grid(mtiles, ntiles, (unsigned)nch);
     const bool ring = ctx->tc_ring && ncols <= 128 && lda % 2 == 0 && ldb % 2 == 0 &&
                       ((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0;
-    if (ring) {
+    if (tma) {
+        // launched above
+    } else if (ring) {
         static bool rattr = false;
         if (!rattr) {
             DFT_CUDA(cudaFuncSetAttribute(gram_tc_ring_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -9,8 +9,6 @@
 // nuclear potential, mixing) uses round-to-nearest intrinsics in the reference's operation
 // order (no FMA contraction), which makes it bit-identical to the reference.
 #include <cooperative_groups.h>
-#include <cuda.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -152,6 +150,21 @@ void mix(dft_context* ctx, long long n, double* d, const double* o, double m) {
     mix_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, d, o, m);
     DFT_LAUNCH_CHECK();
     count_launch(ctx);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+    });
+    return fn;
 }
 
 // =============================================================== H psi ===============
@@ -469,20 +482,6 @@ __global__ void __launch_bounds__(HT_X* HT_Y) hpsi_tma_kernel(const __grid_const
         // let the copies still in flight land before the block's shared memory is released
         for (; waited < issued; ++waited) ht_wait(&full[waited % HT_S], (uint32_t)((waited / HT_S) & 1), HT_SPIN);
     }
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* f = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
-    });
-    return fn;
 }
 
 // The TMA ring needs 16-byte strides (nx and ld even) and a 16-byte aligned band block.

@@ -4,12 +4,18 @@
 // host scalar, in which case it synchronises.
 #pragma once
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <array>
 #include <vector>
 
 #include "common.cuh"
 
 namespace dftb {
+
+// cuTensorMapEncodeTiled (driver entry point looked up once; nullptr when unavailable)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 // H psi over a band block (bit-identical to the reference per band).
 void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const double* psi, double* hpsi, int nbands,

@@ -81,6 +81,12 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               through registers; 1 = through a 2-deep cp.async shared-memory
  *                               ring (even leading dimensions, 16-byte-aligned blocks, <= 128
  *                               columns per tile; otherwise the register path).  Same results.
+ *   "tensor_core_tma":          0 (default) = as "tensor_core_ring" says; 1 = the tensor-core Gram
+ *                               product loads 16-point FP64 slices with TMA (cp.async.bulk.tensor,
+ *                               128-byte swizzle) into a 4-stage mbarrier ring (2 stages for
+ *                               256-column tiles) and splits them from shared memory (even
+ *                               leading dimensions, 16-byte-aligned blocks; otherwise the other
+ *                               paths).  Same accuracy class (TF32 hi+lo, FP32 accumulation).
  *   "hpsi_variant":             0 (default) = the H psi kernel reads x/y neighbours through L1;
  *                               1 = through a shared-memory plane tile (at most 2 bands per
  *                               thread); 2 = plane tiles with their halo loaded by TMA

@@ -14,13 +14,16 @@ from oracle.bindings import PZ81  # noqa: F401
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=[0, 1], ids=["regs", "ring"])
+@pytest.fixture(params=[(0, 0), (1, 0), (0, 1)], ids=["regs", "ring", "tma"])
 def tc_ring(request, engine):
-    """Both staging variants of the tensor-core Gram product (register prefetch, cp.async ring);
-    shapes the ring does not take (odd leading dimension, > 128 columns) fall back."""
-    engine.set_tuning("tensor_core_ring", request.param)
+    """The staging variants of the tensor-core Gram product (register prefetch, cp.async ring,
+    TMA ring); shapes a variant does not take (odd leading dimension, > 128 columns for the
+    cp.async ring) fall back."""
+    engine.set_tuning("tensor_core_ring", request.param[0])
+    engine.set_tuning("tensor_core_tma", request.param[1])
     yield request.param
     engine.set_tuning("tensor_core_ring", 0)
+    engine.set_tuning("tensor_core_tma", 0)
 
 
 @pytest.mark.parametrize("ka,kb,n", [(12, 12, (40, 40, 40)), (50, 70, (64, 48, 33)), (130, 300, (32, 32, 40)),
@@ -75,8 +78,9 @@ def test_rotation_tensor_cores_vs_fp64(engine, k, m, n):
 
 
 def test_gram_ring_padded_rows_odd_points(engine):
-    """Odd point count with an even leading dimension: the ring's last 16-byte chunk carries one
-    point and a NaN in the padding, which must not be read."""
+    """Odd point count with an even leading dimension: the cp.async ring's last 16-byte chunk
+    carries one point and a NaN in the padding, which must not be read; the TMA map ends at the
+    last point (the copy zero-fills past it)."""
     n = (33, 29, 41)
     g = dft_b200.CartesianGrid(*n, -3.0, 3.0, -2.0, 2.5, -1.5, 1.7)
     N = g.getSize()
@@ -89,10 +93,11 @@ def test_gram_ring_padded_rows_odd_points(engine):
     B[:, :N] = rng.standard_normal((24, N))
     dA, dB = engine.upload(A), engine.upload(B)
     c64 = engine.gram(g, dA, ld, 20, dB, ld, 24, precision=0)
-    try:
-        engine.set_tuning("tensor_core_ring", 1)
-        ctc = engine.gram(g, dA, ld, 20, dB, ld, 24, precision=1)
-    finally:
-        engine.set_tuning("tensor_core_ring", 0)
-    assert np.all(np.isfinite(ctc))
-    assert np.max(np.abs(ctc - c64)) < 1e-5 * np.max(np.abs(c64))
+    for key in ("tensor_core_ring", "tensor_core_tma"):
+        try:
+            engine.set_tuning(key, 1)
+            ctc = engine.gram(g, dA, ld, 20, dB, ld, 24, precision=1)
+        finally:
+            engine.set_tuning(key, 0)
+        assert np.all(np.isfinite(ctc)), key
+        assert np.max(np.abs(ctc - c64)) < 1e-5 * np.max(np.abs(c64)), key
