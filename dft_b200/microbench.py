@@ -97,6 +97,7 @@ def main():
     ap.add_argument("--boundary", type=int, default=0, help="scf: Hartree faces, 0 reference, 1 Q/|r| (monopole)")
     ap.add_argument("--predict", type=int, default=0, help="scf: V_H(n_in) start from the mixer's combination (1)")
     ap.add_argument("--tuning", default="", help="context tuning keys, e.g. orthonormalise_adaptive=0,hpsi_variant=2")
+    ap.add_argument("--system-args", default="{}", help='scf: JSON keyword arguments of the system, e.g. {"nmol": 7}')
     ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args()
     import torch
@@ -151,7 +152,7 @@ def main():
                    gbs=32.0 * N / (ms * 1e-3) / 1e9)
     elif a.mode == "scf":
         from dft_b200 import systems
-        w = systems.get(a.system)
+        w = systems.get(a.system, **json.loads(a.system_args))
         g = d.CartesianGrid(*w["n"], *w["bounds"])
         m = d.Molecule()
         for z, p in zip(w["Z"], w["xyz"]):

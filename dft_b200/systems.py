@@ -8,6 +8,8 @@ cluster20    20 nuclei with Z drawn from {1, 6, 7, 8}, positions uniform in a 24
              node, neutral, multiplicity 1 + (N_e mod 2), PBE96 (seeded numpy generator)
 cluster20_clear  the same draw with every nucleus at least 0.08 bohr from the nearest node
 cluster20_compact  the same seeded draw in a 14-bohr cube (more vacuum to the box faces)
+water        (H2O)_n: n rigid waters, random orientations, O uniform in a 24-bohr cube, O-O >= 5 bohr,
+             192^3 grid (h = 0.2), closed shell, PBE96 (seeded numpy generator)
 """
 from __future__ import annotations
 
@@ -81,8 +83,40 @@ def cluster_compact(**kw):
     return w
 
 
+def water_cluster(nmol=4, n=192, h=0.2, box=24.0, min_sep=5.0, seed=20261204, extra_bands=8):
+    """nmol rigid H2O molecules (O-H 1.81 bohr, HOH 104.5 deg), random orientations, O positions
+    uniform in a `box`-bohr cube centred in the n^3 grid (h), O-O distances >= min_sep; closed
+    shell (multiplicity 1), PBE96.  A bonded, closed-shell cluster: unlike a draw of free atoms,
+    its occupied manifold is separated from the empty one by the molecular gap."""
+    rng = np.random.default_rng(seed)
+    grid_n, b = _cube(n, h)
+    lo = b[0]
+    ang = math.radians(104.5 / 2)
+    local = np.array([[0.0, 0.0, 0.0], [1.81 * math.sin(ang), 0.0, 1.81 * math.cos(ang)],
+                      [-1.81 * math.sin(ang), 0.0, 1.81 * math.cos(ang)]])
+    Z, xyz, centres = [], [], []
+    while len(centres) < nmol:
+        c = rng.uniform(-0.5 * box, 0.5 * box, 3)
+        if any(np.linalg.norm(c - q) < min_sep for q in centres):
+            continue
+        q, _ = np.linalg.qr(rng.standard_normal((3, 3)))  # random orthogonal frame
+        pts = c + local @ q.T
+        f = (pts - lo) / h
+        if np.any(np.abs(f - np.round(f)) * h < 1e-12):
+            continue
+        centres.append(c)
+        for zz, p in zip((8, 1, 1), pts):
+            Z.append(zz)
+            xyz.append([float(v) for v in p])
+    ne = sum(Z)
+    return dict(name=f"water{nmol}_{n}", n=grid_n, bounds=b, Z=Z, xyz=xyz, multiplicity=1, functional="PBE96",
+                extra_bands=extra_bands,
+                desc=f"(H2O)_{nmol} cluster (random orientations, O in a {box:g}-bohr cube, seed {seed}), "
+                     f"{ne} electrons, PBE96 {n}^3 h={h}")
+
+
 SYSTEMS = {"h2_48": h2_48, "h2o_128": h2o_128, "cluster20": cluster, "cluster20_clear": cluster_clear,
-           "cluster20_compact": cluster_compact}
+           "cluster20_compact": cluster_compact, "water": water_cluster}
 
 
 def get(name, **kw):
