@@ -8,9 +8,7 @@
 // Both return {eps_xc, v_alpha, v_beta, c_alpha, c_beta} where c = d f / d(grad n_sigma) with
 // the reference's sign convention, and honour its 1e-20 density floor.  The formulas,
 // constants and branch points are the reference's (they define the functional); the
-// expression order follows it, except that the fractional powers of 1 +- z are taken from
-// one cube root each (x^(2/3) = cbrt(x)^2, x^(4/3) = x cbrt(x), x^(-1/3) = 1/cbrt(x)) instead
-// of pow, so results agree to a few ulp (device libm vs glibc).
+// expression order follows it so results agree to a few ulp (device libm vs glibc).
 #pragma once
 
 namespace dftb {
@@ -60,15 +58,13 @@ __host__ __device__ inline Result pz81(double na_in, double nb_in) {
     const double lrs = rs < 1.0 ? log(rs) : 0.0;
     const double srs = rs < 1.0 ? 0.0 : sqrt(rs);
     const double opz = 1.0 + z, omz = 1.0 - z;
-    // (1 +- z)^(1/3) once each; x^(4/3) = x cbrt(x) (z is clamped, so 1 +- z >= 0)
-    const double c13a = cbrt(opz), c13b = cbrt(omz);
-    const double p43a = opz * c13a, p43b = omz * c13b;
-    const double fden = 0.51984209978974632953;                                // 2^(4/3) - 2
+    const double p43a = pow(opz, 4.0 / 3.0), p43b = pow(omz, 4.0 / 3.0);
+    const double fden = pow(2.0, 4.0 / 3.0) - 2.0;
     const double f = (p43a + p43b - 2.0) / fden;                               // PZ81.cpp:122-149
-    const double df = 4.0 / 3.0 * (c13a - c13b) / fden;                         // :151-182
+    const double df = 4.0 / 3.0 * (pow(opz, 1.0 / 3.0) - pow(omz, 1.0 / 3.0)) / fden;  // :151-182
     const double ex = -0.7385587663820223 * cbrt(n);                             // :184-190
     const double sx = (p43a + p43b) / 2.0;                                      // :192-213
-    const double dsx = 2.0 / 3.0 * (c13a - c13b);                               // :215-237
+    const double dsx = 2.0 / 3.0 * (pow(opz, 1.0 / 3.0) - pow(omz, 1.0 / 3.0)); // :215-237
     double e0, d0, e1, d1;
     pz_corr(rs, lrs, srs, pz_unpol(), e0, d0);
     pz_corr(rs, lrs, srs, pz_pol(), e1, d1);
@@ -144,9 +140,7 @@ __host__ __device__ __forceinline__ void pbe_correlation(double na, double nb, d
     const double kf = cbrt(3.0 * PI * PI * n);
     const double rs = cbrt(3.0 / (4.0 * PI * n));
     const double opz = 1.0 + z, omz = 1.0 - z;
-    // (1 +- z)^(1/3) once each: x^(2/3) = cbrt(x)^2, x^(4/3) = x cbrt(x) (1 +- z >= 0)
-    const double c13a = cbrt(opz), c13b = cbrt(omz);
-    const double phi = 0.5 * (c13a * c13a + c13b * c13b);
+    const double phi = 0.5 * (pow(opz, TWO_THIRDS) + pow(omz, TWO_THIRDS));
     const double ks = sqrt(4.0 * kf / PI);
     const double tkp = 2.0 * ks * phi;
     const double t = tkp > 0.0 ? gm / (tkp * n) : 0.0;
@@ -157,10 +151,10 @@ __host__ __device__ __forceinline__ void pbe_correlation(double na, double nb, d
     const double ep = gcor2(0.01554535, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517, srs, epd);
     const double al = gcor2(0.0168869, 0.11125, 10.357, 3.6231, 0.88026, 0.49671, srs, ad);
     const double z4 = z * z * z * z;
-    const double f = (opz * c13a + omz * c13b - 2.0) / SPIN_GAMMA;
+    const double f = (pow(opz, FOUR_THIRDS) + pow(omz, FOUR_THIRDS) - 2.0) / SPIN_GAMMA;
     const double ec = eu * (1.0 - f * z4) + ep * f * z4 - al * f * (1.0 - z4) / SPIN_FZZ;
     const double ecrs = eud * (1.0 - f * z4) + epd * f * z4 - ad * f * (1.0 - z4) / SPIN_FZZ;
-    const double fz = FOUR_THIRDS * (c13a - c13b) / SPIN_GAMMA;
+    const double fz = FOUR_THIRDS * (pow(opz, THIRD) - pow(omz, THIRD)) / SPIN_GAMMA;
     const double ecz = 4.0 * z * z * z * f * (ep - eu + al / SPIN_FZZ) +
                        fz * (z4 * ep - z4 * eu - (1.0 - z4) * al / SPIN_FZZ);
     // H(t)
@@ -179,7 +173,7 @@ __host__ __device__ __forceinline__ void pbe_correlation(double na, double nb, d
     const double hrs = -(rs / 3.0) * hb * bec * ecrs;
     const double ht = 2.0 * BETA * phi3 * q9 / q8;
     const double comm = h + hrs - 7.0 * t2 * ht / 6.0;
-    const double gz = (1.0 / cbrt(opz + ETA) - 1.0 / cbrt(omz + ETA)) / 3.0;
+    const double gz = (pow(opz + ETA, -THIRD) - pow(omz + ETA, -THIRD)) / 3.0;
     const double bg = -3.0 * b2 * ec * fac / (BETA * phi4);
     const double hz = 3.0 * gz * h / phi + hb * (bg * gz + bec * ecz);
     const double pref = hz - gz * t2 * ht / phi;
