@@ -108,8 +108,9 @@ def test_poisson_predict_same_energy_fewer_cycles(engine, mixer, q0, mult):
         m.addNucleus(1, 1.6, 0.0, 0.0)
     res = {}
     for pp in (0, 1, 2):
-        o = dft_b200.default_scf_options(stop_abs_de=1e-8, poisson_start=dft_b200.POISSON_MULTIGRID, mixer=mixer,
-                                         kerker_q0=q0, poisson_predict=pp)
+        o = dft_b200.default_scf_options(stop_abs_de=1e-8, stop_abs_deig=1e-8,
+                                         poisson_start=dft_b200.POISSON_MULTIGRID, mixer=mixer, kerker_q0=q0,
+                                         poisson_predict=pp)
         r = engine.scf_molecule(g, m, 0, mult, "PBE96", o)
         assert r.converged or r.energyDifference < 1e-8
         res[pp] = (r.total, [h["poisson_cycles_in"] for h in r.history], r.eigenvalues,
