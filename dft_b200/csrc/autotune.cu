@@ -56,20 +56,23 @@ void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* 
     if (hit != ctx->tuned.end()) {
         r.hpsi_bands_per_thread = hit->second[0];
         r.jacobi_sweeps_per_launch = hit->second[1];
+        r.hpsi_variant = hit->second[2];
         r.cached = 1;
         if (rep) *rep = r;
         return;
     }
     // the knobs are set per variant while timing and put back afterwards
     const int keep_bpt = ctx->hpsi_bands_per_thread, keep_spl = ctx->jacobi_sweeps_per_launch;
+    const int keep_var = ctx->hpsi_variant;
     struct Restore {
         dft_context* c;
-        int b, s;
+        int b, s, v;
         ~Restore() {
             c->hpsi_bands_per_thread = b;
             c->jacobi_sweeps_per_launch = s;
+            c->hpsi_variant = v;
         }
-    } restore{ctx, keep_bpt, keep_spl};
+    } restore{ctx, keep_bpt, keep_spl, keep_var};
     Events ev;
     const long long N = g.N;
     // timing buffers: at most 16 bands (the per-band cost is what differs), zero fields (the
@@ -87,8 +90,9 @@ void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* 
     double *V = buf, *psi = buf + N, *hpsi = psi + (size_t)tb * N, *rho = hpsi + (size_t)tb * N, *vh = rho + N;
     // ---- H psi: bands per thread
     const int bpt[3] = {1, 2, 4};
-    int best_bpt = 1;
+    int best_bpt = 1, best_var = 0;
     double best = 1e300;
+    ctx->hpsi_variant = 0;
     for (int i = 0; i < 3; ++i) {
         if (bpt[i] > tb && i > 0) {
             r.hpsi_ms[i] = -1.0;
@@ -98,7 +102,23 @@ void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* 
         r.hpsi_ms[i] = time_ms(ctx, ev, 3, [&] { apply_hamiltonian(ctx, g, V, psi, hpsi, tb, N); });
         if (r.hpsi_ms[i] < best) best = r.hpsi_ms[i], best_bpt = bpt[i];
     }
+    // the TMA plane ring, bands per block (where the grid and the block allow it)
+    const int nbc[4] = {1, 2, 4, 8};
+    const bool tma_ok = hpsi_tma_eligible(g, psi, N);
+    ctx->hpsi_variant = 2;
+    for (int i = 0; i < 4; ++i) {
+        if (!tma_ok || (nbc[i] > tb && i > 0)) {
+            r.hpsi_tma_ms[i] = -1.0;
+            continue;
+        }
+        ctx->hpsi_bands_per_thread = nbc[i];
+        r.hpsi_tma_ms[i] = time_ms(ctx, ev, 3, [&] { apply_hamiltonian(ctx, g, V, psi, hpsi, tb, N); });
+        if (r.hpsi_tma_ms[i] < best) best = r.hpsi_tma_ms[i], best_bpt = nbc[i], best_var = 2;
+    }
+    check_device_status(ctx, "autotune");
+    ctx->hpsi_variant = 0;
     r.hpsi_bands_per_thread = best_bpt;
+    r.hpsi_variant = best_var;
     // ---- Jacobi: sweeps per launch; tol = 0 never stops, so each call runs exactly `sweeps`
     const int spl[6] = {-2, -1, 1, 2, 4, 8};
     const long sweeps = 64;
@@ -117,7 +137,7 @@ void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* 
     }
     r.jacobi_sweeps_per_launch = best_spl;
     sync(ctx);
-    ctx->tuned[key] = {best_bpt, best_spl};
+    ctx->tuned[key] = {best_bpt, best_spl, best_var};
     if (rep) *rep = r;
 }
 

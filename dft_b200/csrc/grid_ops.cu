@@ -484,11 +484,15 @@ __global__ void __launch_bounds__(HT_X* HT_Y) hpsi_tma_kernel(const __grid_const
     }
 }
 
+}  // namespace
+
 // The TMA ring needs 16-byte strides (nx and ld even) and a 16-byte aligned band block.
 bool hpsi_tma_eligible(const Grid& g, const double* psi, long long ld) {
     return g.nx % 2 == 0 && ld % 2 == 0 && (reinterpret_cast<uintptr_t>(psi) & 15) == 0 && g.nx >= 3 &&
            g.ny >= 3 && tensor_map_encoder() != nullptr;
 }
+
+namespace {
 
 // 4-D map (x, y, z, band) of nbands bands at psi, box = one plane tile with its halo.
 CUtensorMap hpsi_tensor_map(const Grid& g, const double* psi, long long ld, int nbands) {
@@ -538,9 +542,14 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
                        long long ld) {
     if (nbands <= 0) return;
     const double k0 = -2.0 * (g.ix2 + g.iy2 + g.iz2);
-    if (ctx->hpsi_variant == 2 && hpsi_tma_eligible(g, psi, ld)) {
-        // bands per CTA: the "hpsi_bands_per_thread" key (1, 2, 4 or 8), else 4
-        int nbc = ctx->hpsi_bands_per_thread > 0 ? ctx->hpsi_bands_per_thread : 4;
+    // variant: the "hpsi_variant" key, else the autotuner's choice for this grid
+    int variant = ctx->hpsi_variant;
+    const auto tuned = ctx->tuned.find({(long long)g.nx, (long long)g.ny, (long long)g.nz});
+    if (variant == 0 && tuned != ctx->tuned.end()) variant = tuned->second[2];
+    if (variant == 2 && hpsi_tma_eligible(g, psi, ld)) {
+        // bands per CTA: the "hpsi_bands_per_thread" key (1, 2, 4 or 8), else the tuned value, else 4
+        int nbc = ctx->hpsi_bands_per_thread > 0 ? ctx->hpsi_bands_per_thread
+                  : tuned != ctx->tuned.end() && tuned->second[2] == 2 ? tuned->second[0] : 4;
         nbc = std::max(1, std::min(nbc, nbands));
         const int bx = (g.nx + HT_X - 1) / HT_X, by = (g.ny + HT_Y - 1) / HT_Y;
         const int groups = (nbands + nbc - 1) / nbc;

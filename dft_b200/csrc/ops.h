@@ -18,6 +18,8 @@ namespace dftb {
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 // H psi over a band block (bit-identical to the reference per band).
+// hpsi_tma_eligible: whether the TMA plane-ring variant takes this grid and block.
+bool hpsi_tma_eligible(const Grid& g, const double* psi, long long ld);
 void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const double* psi, double* hpsi, int nbands,
                        long long ld);
 

@@ -107,10 +107,12 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
 dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long value);
 
 /* Autotuner (no reference counterpart): times every bit-identical launch variant of the H psi
- * kernel (1, 2, 4 bands per thread, on min(nbands, 16) bands) and of the Jacobi Poisson solve
+ * kernel (1, 2, 4 bands per thread, on min(nbands, 16) bands, and the TMA plane ring with 1, 2,
+ * 4, 8 bands per block where the grid allows it) and of the Jacobi Poisson solve
  * (sweeps per launch -2, -1, 1, 2, 4, 8; 64 sweeps) on grid g with CUDA events on the context's
  * stream and remembers the fastest of each for grid g in the context: kernels on g use it
- * wherever the "hpsi_bands_per_thread" or "jacobi_sweeps_per_launch" knob is 0 (auto), and a
+ * wherever the "hpsi_bands_per_thread" or "jacobi_sweeps_per_launch" knob is 0 (auto) (the H psi
+ * kernel variant too, while "hpsi_variant" is 0), and a
  * second call for g times nothing.  report may be NULL; a time of -1 marks a variant that does
  * not apply (e.g. a grid too large for the cluster-resident Jacobi).  Allocates
  * (2 min(nbands,16) + 3) x N doubles while it runs. */
@@ -120,6 +122,8 @@ typedef struct {
     int jacobi_sweeps_per_launch;  /* chosen */
     double jacobi_us_per_sweep[6]; /* -2, -1, 1, 2, 4, 8 */
     int cached;                    /* 1: the choice was remembered, nothing was timed */
+    int hpsi_variant;              /* chosen: 0 = the register march (hpsi_ms), 2 = the TMA ring */
+    double hpsi_tma_ms[4];         /* TMA plane ring with 1, 2, 4, 8 bands per block (-1: not eligible) */
 } dft_autotune_report;
 dft_status_t dft_autotune(dft_context* ctx, const dft_grid* g, int nbands, dft_autotune_report* report);
 /* The cudaStream_t the context launches on, as an opaque handle (for event timing). */

@@ -15,8 +15,13 @@ def test_autotune_picks_fastest_and_remembers(engine):
     r = engine.autotune(g, 6)
     print(r)
     assert not r["cached"]
-    bpt = {1: r["hpsi_ms"][0], 2: r["hpsi_ms"][1], 4: r["hpsi_ms"][2]}
-    assert r["hpsi_ms"][[1, 2, 4].index(r["hpsi_bands_per_thread"])] == min(v for v in bpt.values() if v >= 0)
+    times = [v for v in list(r["hpsi_ms"]) + list(r["hpsi_tma_ms"]) if v >= 0]
+    if r["hpsi_variant"] == 2:
+        chosen = r["hpsi_tma_ms"][[1, 2, 4, 8].index(r["hpsi_bands_per_thread"])]
+    else:
+        chosen = r["hpsi_ms"][[1, 2, 4].index(r["hpsi_bands_per_thread"])]
+    assert chosen == min(times)
+    assert all(v >= 0 for v in r["hpsi_tma_ms"][:3])  # nx = 40 is even: the TMA ring applies
     spl = dict(zip([-2, -1, 1, 2, 4, 8], r["jacobi_us_per_sweep"]))
     assert spl[r["jacobi_sweeps_per_launch"]] == min(v for v in spl.values() if v >= 0)
     assert engine.autotune(g, 6)["cached"]
