@@ -155,6 +155,13 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
         } else if (k == "hpsi_variant") {
             NEED(value >= 0 && value <= 2, "hpsi_variant must be 0, 1 or 2");
             ctx->hpsi_variant = (int)value;
+        } else if (k == "multigrid_fused_restriction" || k == "multigrid_coarsest_sor") {
+            NEED(value == 0 || value == 1, "multigrid keys take 0 or 1");
+            (k == "multigrid_fused_restriction" ? ctx->mg_fused_restrict : ctx->mg_coarsest_sor) = (int)value;
+            // captured multigrid cycles hold the old launch sequence
+            dftb::sync(ctx);
+            for (auto& kv : ctx->mg_graphs) cudaGraphExecDestroy(kv.second.exec);
+            ctx->mg_graphs.clear();
         } else if (k == "tensor_core_tma") {
             NEED(value == 0 || value == 1, "tensor_core_tma must be 0 or 1");
             ctx->tc_tma = (int)value;

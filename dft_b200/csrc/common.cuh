@@ -114,6 +114,8 @@ struct dft_context {
                                        // 2 = TMA plane ring (where eligible, else 0)
     int* dev_status = nullptr;         // device word set by kernels whose bounded waits gave up
     int ortho_adaptive = 1;            // FP64 orthonormalisation: skip the second pass when safe (1)
+    int mg_fused_restrict = 1;         // multigrid: one-pass 3-D restriction on fine grids <= 64^3 (1)
+    int mg_coarsest_sor = 1;           // multigrid: red-black SOR coarsest solve (1) or Jacobi sweeps (0)
     int tc_ring = 0;                   // tensor-core Gram: cp.async ring variant (1) or register staging (0)
     int tc_tma = 0;                    // tensor-core Gram: TMA-fed FP64 ring (1; before tc_ring)
     long long grid_barrier_poll_limit = 0;  // persistent Jacobi barrier polls before giving up (0 = 2^24)

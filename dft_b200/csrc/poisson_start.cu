@@ -193,31 +193,45 @@ double* carve(double* slab, const Grid& fine, std::vector<Level>& L) {
 
 // The same restriction in one pass (small fine grids, where the three passes are three
 // launch latencies): out(I,J,K) = prod_d (h_d/H_d) sum_k w_z sum_j w_y sum_i w_x in(i,j,k).
+// hat weights of one axis: w[t] for fine index lo + t (at most RW of them; coarse spacing
+// <= 2.5 fine spacings, which coarse_points guarantees)
+constexpr int RW = 6;
+__device__ __forceinline__ int hat_weights(int I, double h, double H, int nf, double* w) {
+    const double X = I * H;
+    const int lo = max(0, (int)ceil((X - H) / h)), hi = min(nf - 1, (int)floor((X + H) / h));
+#pragma unroll
+    for (int t = 0; t < RW; ++t) {
+        const int i = lo + t;
+        const double v = i <= hi ? 1.0 - fabs(i * h - X) / H : 0.0;
+        w[t] = v > 0.0 ? v : 0.0;
+    }
+    return lo;
+}
+
 __global__ void restrict3d_kernel(const double* __restrict__ in, double* __restrict__ out, Grid f, Grid c) {
     const double scale = (f.dx / c.dx) * (f.dy / c.dy) * (f.dz / c.dz);
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < c.N; q += (long long)gridDim.x * blockDim.x) {
         const int I = (int)(q % c.nx), J = (int)((q / c.nx) % c.ny), K = (int)(q / ((long long)c.nx * c.ny));
-        const double X = I * c.dx, Y = J * c.dy, Z = K * c.dz;
-        const int i0 = max(0, (int)ceil((X - c.dx) / f.dx)), i1 = min(f.nx - 1, (int)floor((X + c.dx) / f.dx));
-        const int j0 = max(0, (int)ceil((Y - c.dy) / f.dy)), j1 = min(f.ny - 1, (int)floor((Y + c.dy) / f.dy));
-        const int k0 = max(0, (int)ceil((Z - c.dz) / f.dz)), k1 = min(f.nz - 1, (int)floor((Z + c.dz) / f.dz));
+        double wx[RW], wy[RW], wz[RW];
+        const int i0 = hat_weights(I, f.dx, c.dx, f.nx, wx);
+        const int j0 = hat_weights(J, f.dy, c.dy, f.ny, wy);
+        const int k0 = hat_weights(K, f.dz, c.dz, f.nz, wz);
         double sz = 0.0;
-        for (int k = k0; k <= k1; ++k) {
-            const double wz = 1.0 - fabs(k * f.dz - Z) / c.dz;
-            if (wz <= 0.0) continue;
+#pragma unroll
+        for (int tk = 0; tk < RW; ++tk) {
+            if (wz[tk] == 0.0) continue;
             double sy = 0.0;
-            for (int j = j0; j <= j1; ++j) {
-                const double wy = 1.0 - fabs(j * f.dy - Y) / c.dy;
-                if (wy <= 0.0) continue;
-                const double* row = in + ((long long)k * f.ny + j) * f.nx;
+#pragma unroll
+            for (int tj = 0; tj < RW; ++tj) {
+                if (wy[tj] == 0.0) continue;
+                const double* row = in + ((long long)(k0 + tk) * f.ny + (j0 + tj)) * f.nx + i0;
                 double sx = 0.0;
-                for (int i = i0; i <= i1; ++i) {
-                    const double wx = 1.0 - fabs(i * f.dx - X) / c.dx;
-                    if (wx > 0.0) sx += wx * row[i];
-                }
-                sy += wy * sx;
+#pragma unroll
+                for (int ti = 0; ti < RW; ++ti)
+                    if (wx[ti] != 0.0) sx += wx[ti] * row[ti];
+                sy += wy[tj] * sx;
             }
-            sz += wz * sy;
+            sz += wz[tk] * sy;
         }
         out[q] = sz * scale;
     }
@@ -225,7 +239,8 @@ __global__ void restrict3d_kernel(const double* __restrict__ in, double* __restr
 
 void restrict3(dft_context* ctx, const Grid& f, const Grid& c, const double* in, double* t1, double* t2,
                double* out) {
-    if (f.N <= 64LL * 64 * 64) {
+    if (ctx->mg_fused_restrict && f.N <= 64LL * 64 * 64 && c.dx <= 2.5 * f.dx && c.dy <= 2.5 * f.dy &&
+        c.dz <= 2.5 * f.dz) {
         restrict3d_kernel<<<blocks_for(ctx, c.N), 256, 0, ctx->stream>>>(in, out, f, c);
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
@@ -363,16 +378,33 @@ __global__ void __launch_bounds__(1024) mg_coarsest_kernel(Grid g, const double*
     for (int p = threadIdx.x; p < n; p += blockDim.x) a[p] = 0.0;
     __syncthreads();
     const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
-    for (int s = 0; s < sweeps; ++s)
-        for (int colour = 0; colour < 2; ++colour) {
-            for (int p = threadIdx.x; p < n; p += blockDim.x) {
-                const int i = p % g.nx, j = (p / g.nx) % g.ny, k = p / (g.nx * g.ny);
-                if (((i + j + k) & 1) != colour || on_face(g, p)) continue;
-                const double gs = (nb_sum(g, a, p) + src[p]) / den;
-                a[p] += omega * (gs - a[p]);
-            }
+    // omega == 1: plain Jacobi sweeps (the sweep reads the previous iterate: a second array)
+    if (omega == 1.0) {
+        double* b = sm + n;
+        for (int p = threadIdx.x; p < n; p += blockDim.x) b[p] = 0.0;
+        __syncthreads();
+        for (int s = 0; s < sweeps; ++s) {
+            const double* cur = (s & 1) ? b : a;
+            double* nxt = (s & 1) ? a : b;
+            for (int p = threadIdx.x; p < n; p += blockDim.x)
+                if (!on_face(g, p)) nxt[p] = (nb_sum(g, cur, p) + src[p]) / den;
             __syncthreads();
         }
+        if (sweeps & 1)
+            for (int p = threadIdx.x; p < n; p += blockDim.x) a[p] = b[p];
+        __syncthreads();
+    } else {
+        for (int s = 0; s < sweeps; ++s)
+            for (int colour = 0; colour < 2; ++colour) {
+                for (int p = threadIdx.x; p < n; p += blockDim.x) {
+                    const int i = p % g.nx, j = (p / g.nx) % g.ny, k = p / (g.nx * g.ny);
+                    if (((i + j + k) & 1) != colour || on_face(g, p)) continue;
+                    const double gs = (nb_sum(g, a, p) + src[p]) / den;
+                    a[p] += omega * (gs - a[p]);
+                }
+                __syncthreads();
+            }
+    }
     for (int p = threadIdx.x; p < n; p += blockDim.x) e[p] = a[p];
 }
 
@@ -468,10 +500,10 @@ void mg_smooth(dft_context* ctx, MGLevel& l, double sscale, int n) {
 void vcycle(dft_context* ctx, std::vector<MGLevel>& L, size_t i, double sscale) {
     MGLevel& l = L[i];
     if (i + 1 == L.size()) {
-        const size_t sm = sizeof(double) * (size_t)l.g.N;
-        double omega;
-        int sweeps;
-        coarsest_sor(l.g, &omega, &sweeps);
+        const size_t sm = sizeof(double) * 2 * (size_t)l.g.N;
+        double omega = 1.0;
+        int sweeps = 8 * std::max({l.g.nx, l.g.ny, l.g.nz});
+        if (ctx->mg_coarsest_sor) coarsest_sor(l.g, &omega, &sweeps);
         mg_coarsest_kernel<<<1, 1024, sm, ctx->stream>>>(l.g, l.src, l.v, sweeps, omega);
         DFT_LAUNCH_CHECK();
         count_launch(ctx);
@@ -507,7 +539,7 @@ int multigrid(dft_context* ctx, const Grid& g, const double* rho, double* v, dou
     static bool attr = false;
     if (!attr) {
         DFT_CUDA(cudaFuncSetAttribute(mg_coarsest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(sizeof(double) * MG_COARSEST_MAX)));
+                                      (int)(sizeof(double) * 2 * MG_COARSEST_MAX)));
         attr = true;
     }
     // the fine level works in place on v (its faces must hold the boundary values); rho is

@@ -97,6 +97,11 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *   "grid_barrier_poll_limit":  0 = 2^24 (default): polls a block of the persistent Jacobi
  *                               launch makes at a grid barrier before it gives up; the solve then
  *                               fails with DFT_CUDA_ERROR and the context stays usable.
+ *   "multigrid_fused_restriction": 1 (default) = the Poisson multigrid restricts in one 3-D pass
+ *                               on fine grids up to 64^3 (0: three separable passes).
+ *   "multigrid_coarsest_sor":   1 (default) = the coarsest multigrid level is solved by red-black
+ *                               SOR at the optimal relaxation (0: 8 Jacobi sweeps per point of the
+ *                               longest axis).
  *   "orthonormalise_adaptive":  1 (default) = the FP64 orthonormalisation of new eigensolver
  *                               directions stops after one projected Cholesky QR pass when its
  *                               estimated loss of orthogonality (eps * cancellation * condition
