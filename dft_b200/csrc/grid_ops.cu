@@ -352,20 +352,24 @@ __global__ void __launch_bounds__(HB_X* HB_Y, 6) hpsi_tile_kernel(Grid g, const 
 }
 
 // ---------------------------------------------------------------- TMA plane ring ---------
-// "hpsi_variant" = 2.  A CTA owns a 32 x 8 column tile, a z-chunk and a run of bands, and walks
-// the planes kb-1 .. ke of each band in order.  One elected thread loads each plane tile with
-// its one-point halo (x from x0-2 so the copy starts on a 16-byte boundary: 36 x 10 doubles)
-// by cp.async.bulk.tensor into a ring of HT_S shared-memory stages, each tracked by an
-// mbarrier with the transaction count; the loads run HT_S-2 planes ahead of the compute,
-// so the copies in flight per SM do not depend on registers.  Out-of-box parts of a tile
-// (x < 0, y < 0, z = -1, z = nz, ...) are zero-filled by the copy and never used: absent
-// neighbours are skipped exactly as in hpsi1_kernel, so every value is bit-identical.  The
-// point's own column (below, current) is kept in registers; V is read from global memory
-// once per band (from L2 after the first band of the run).
-constexpr int HT_X = 32, HT_Y = 8, HT_S = 6;
+// "hpsi_variant" = 2.  Persistent, warp-specialised: a block of 8 compute warps and 1 copy warp
+// takes work items (a 32 x 8 column tile, a z-chunk, a run of bands) in turn.  The copy warp's
+// first lane walks the planes kb-1 .. ke of every band of its items and loads each plane tile
+// with its one-point halo (x from x0-2 so the copy starts on a 16-byte boundary: 36 x 10
+// doubles) by cp.async.bulk.tensor into a ring of HT_S shared-memory stages.  Each stage has a
+// "full" mbarrier (the copy's transaction count) and an "empty" one (one arrival per compute
+// warp when it is done with the plane), so no block-wide barrier paces the march and up to
+// HT_S planes per block are in flight.  Compute warp w owns tile row y0 + w (lane = x); the
+// point's own column (below, current) is kept in registers.  Out-of-grid parts of a tile are
+// zero-filled by the copy and never used: absent neighbours are skipped exactly as in
+// hpsi1_kernel, so every value is bit-identical.  V is read from global memory, once per band
+// (from L2 after the first band of the run).  Every wait is bounded; a block that gives up sets
+// the context's status word and drains its copies.
+constexpr int HT_X = 32, HT_Y = 8, HT_S = 8;
 constexpr int HT_PX = HT_X + 4, HT_PY = HT_Y + 2;
 constexpr int HT_PLANE = HT_PX * HT_PY;                            // doubles in a plane tile
 constexpr int HT_STAGE = (HT_PLANE * 8 + 127) / 128 * 128 / 8;     // stage stride (128-byte aligned)
+constexpr int HT_THREADS = (HT_Y + 1) * 32;                        // 8 compute warps + 1 copy warp
 constexpr long long HT_SPIN = 1LL << 22;                           // polls before a wait gives up
 
 __device__ __forceinline__ uint32_t ht_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -386,102 +390,144 @@ __device__ __forceinline__ bool ht_wait(uint64_t* bar, uint32_t parity, long lon
     return false;
 }
 
-__global__ void __launch_bounds__(HT_X* HT_Y) hpsi_tma_kernel(const __grid_constant__ CUtensorMap tm, Grid g,
-                                                              const double* __restrict__ V, double* __restrict__ out,
-                                                              long long ld, int nbands, int nbc, int zchunk, int nzc,
-                                                              double k0, int* __restrict__ status) {
+struct HtWork {
+    int bx, by, nzc, zchunk, nbc;
+    long long items;  // bx * by * nzc * band runs
+};
+
+struct HtItem {
+    int x0, y0, kb, ke, b0, nb;
+};
+
+__device__ __forceinline__ HtItem ht_item(const HtWork& w, const Grid& g, int nbands, long long it) {
+    const long long tiles = (long long)w.bx * w.by;
+    const int t = (int)(it % tiles);
+    const long long rest = it / tiles;
+    const int kc = (int)(rest % w.nzc);
+    const int grp = (int)(rest / w.nzc);
+    HtItem r;
+    r.x0 = (t % w.bx) * HT_X;
+    r.y0 = (t / w.bx) * HT_Y;
+    r.kb = kc * w.zchunk;
+    r.ke = min(g.nz, r.kb + w.zchunk);
+    r.b0 = grp * w.nbc;
+    r.nb = min(w.nbc, nbands - r.b0);
+    return r;
+}
+
+__global__ void __launch_bounds__(HT_THREADS, 4) hpsi_tma_kernel(const __grid_constant__ CUtensorMap tm, Grid g,
+                                                                 const double* __restrict__ V, double* __restrict__ out,
+                                                                 long long ld, int nbands, HtWork w, double k0,
+                                                                 int* __restrict__ status) {
     __shared__ __align__(128) double plane[HT_S][HT_STAGE];
     __shared__ __align__(8) uint64_t full[HT_S];
+    __shared__ __align__(8) uint64_t empty[HT_S];
     __shared__ int abort_flag;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const bool leader = tx == 0 && ty == 0;
-    const int x0 = blockIdx.x * HT_X, y0 = blockIdx.y * HT_Y;
-    const int grp = blockIdx.z / nzc;
-    const int kc = blockIdx.z - grp * nzc;
-    const int b0 = grp * nbc;
-    const int nb = min(nbc, nbands - b0);
-    const int kb = kc * zchunk;
-    const int ke = min(g.nz, kb + zchunk);
-    const int nk = ke - kb;
-    const int L = nk + 2;  // planes kb-1 .. ke of one band
-    const int Q = nb * L;
-    if (leader) {
-        for (int s = 0; s < HT_S; ++s)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < HT_S; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(ht_smem(&full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(ht_smem(&empty[s])), "r"(HT_Y));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         abort_flag = 0;
     }
     __syncthreads();
-    int issued = 0;
-    auto issue = [&](int p) {
-        const int b = p / L;
-        const int k = kb - 1 + (p - b * L);
-        const uint32_t bar = ht_smem(&full[p % HT_S]);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(HT_PLANE * 8)
-                     : "memory");
-        asm volatile(
-            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-            "%5}], [%6];" ::"r"(ht_smem(&plane[p % HT_S][0])),
-            "l"(reinterpret_cast<uint64_t>(&tm)), "r"(x0 - 2), "r"(y0 - 1), "r"(k), "r"(b0 + b), "r"(bar)
-            : "memory");
-    };
-    if (leader)
-        while (issued < Q && issued < HT_S) issue(issued++);
-    const int i = x0 + tx, j = y0 + ty;
-    const bool in = i < g.nx && j < g.ny;
-    const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
-    const long long sxy = (long long)g.nx * g.ny;
-    const int c = (ty + 1) * HT_PX + tx + 2;  // the point's offset inside a plane tile
-    int waited = 0;                           // planes this thread has waited for
-    double below = 0.0, cur = 0.0;
-    const int steps = nb * nk;
-    for (int s = 0; s < steps; ++s) {
-        const int b = s / nk;
-        const int k = kb + (s - b * nk);
-        const int q = b * L + (k - kb + 1);  // the plane of this step in the sequence
-        const long long idx = (long long)k * sxy + (long long)j * g.nx + i;
-        const double v = in ? __ldg(V + idx) : 0.0;
-        bool good = true;
-        while (waited <= q + 1) {
-            good = good && ht_wait(&full[waited % HT_S], (uint32_t)((waited / HT_S) & 1), HT_SPIN);
-            ++waited;
-        }
-        if (!good) abort_flag = 1;
-        if (k == kb) {
-            below = plane[(q - 1) % HT_S][c];
-            cur = plane[q % HT_S][c];
-        }
-        const double* P = plane[q % HT_S];
-        const double above = plane[(q + 1) % HT_S][c];
-        if (in) {
-            double lap = __dmul_rn(k0, cur);
-            if (xl) lap = __dadd_rn(lap, __dmul_rn(P[c - 1], g.ix2));
-            if (xr) lap = __dadd_rn(lap, __dmul_rn(P[c + 1], g.ix2));
-            if (yl) lap = __dadd_rn(lap, __dmul_rn(P[c - HT_PX], g.iy2));
-            if (yr) lap = __dadd_rn(lap, __dmul_rn(P[c + HT_PX], g.iy2));
-            if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below, g.iz2));
-            if (k + 1 < g.nz) lap = __dadd_rn(lap, __dmul_rn(above, g.iz2));
-            out[(long long)(b0 + b) * ld + idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(v, cur));
-        }
-        below = cur;
-        cur = above;
-        __syncthreads();  // every thread is done with the planes before the next step's q - 1
-        if (abort_flag) break;
-        if (leader) {
-            int qn = Q;  // the next step's plane (all planes free after the last step)
-            if (s + 1 < steps) {
-                const int bn = (s + 1) / nk;
-                qn = bn * L + (s + 1 - bn * nk) + 1;
+    volatile int* abort_v = &abort_flag;
+    if (warp == HT_Y) {
+        // copy warp: its first lane issues every plane of this block's items in order
+        if (lane == 0) {
+            long long P = 0;
+            bool ok = true;
+            for (long long it = blockIdx.x; it < w.items && ok; it += gridDim.x) {
+                const HtItem m = ht_item(w, g, nbands, it);
+                for (int b = 0; b < m.nb && ok; ++b)
+                    for (int k = m.kb - 1; k <= m.ke; ++k, ++P) {
+                        const int s = (int)(P % HT_S);
+                        // stage s is free once every compute warp released plane P - HT_S
+                        if (!ht_wait(&empty[s], (uint32_t)(((P / HT_S) & 1) ^ 1), HT_SPIN) || *abort_v) {
+                            ok = false;
+                            break;
+                        }
+                        const uint32_t bar = ht_smem(&full[s]);
+                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                                     "r"(HT_PLANE * 8)
+                                     : "memory");
+                        asm volatile(
+                            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], "
+                            "[%1, {%2, %3, %4, %5}], [%6];" ::"r"(ht_smem(&plane[s][0])),
+                            "l"(reinterpret_cast<uint64_t>(&tm)), "r"(m.x0 - 2), "r"(m.y0 - 1), "r"(k),
+                            "r"(m.b0 + b), "r"(bar)
+                            : "memory");
+                    }
             }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            while (issued < Q && issued < qn - 1 + HT_S) issue(issued++);
+            if (!ok) {
+                *abort_v = 1;
+                atomicOr(status, 1);
+            }
+            // the copies of the last HT_S planes may still be in flight: let them land
+            for (long long q = P > HT_S ? P - HT_S : 0; q < P; ++q)
+                ht_wait(&full[q % HT_S], (uint32_t)((q / HT_S) & 1), HT_SPIN);
         }
+    } else {
+        // compute warp: tile row y0 + warp, point x0 + lane
+        const int c = (warp + 1) * HT_PX + lane + 2;  // the point's offset inside a plane tile
+        const long long sxy = (long long)g.nx * g.ny;
+        long long P = 0;
+        bool ok = true;
+        auto release = [&](long long q) {
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(ht_smem(&empty[q % HT_S])) : "memory");
+        };
+        for (long long it = blockIdx.x; it < w.items && ok; it += gridDim.x) {
+            const HtItem m = ht_item(w, g, nbands, it);
+            const int i = m.x0 + lane, j = m.y0 + warp;
+            const bool in = i < g.nx && j < g.ny;
+            const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+            const int nk = m.ke - m.kb;
+            for (int b = 0; b < m.nb && ok; ++b) {
+                // planes P (kb - 1), P + 1 (kb), ..., P + nk + 1 (ke) of this band
+                if (!ht_wait(&full[P % HT_S], (uint32_t)((P / HT_S) & 1), HT_SPIN) ||
+                    !ht_wait(&full[(P + 1) % HT_S], (uint32_t)(((P + 1) / HT_S) & 1), HT_SPIN)) {
+                    ok = false;
+                    break;
+                }
+                double below = plane[P % HT_S][c];
+                double cur = plane[(P + 1) % HT_S][c];
+                release(P);
+                double* __restrict__ o = out + (long long)(m.b0 + b) * ld;
+                for (int k = m.kb; k < m.ke; ++k) {
+                    const long long q = P + 1 + (k - m.kb);
+                    const long long idx = (long long)k * sxy + (long long)j * g.nx + i;
+                    const double v = in ? __ldg(V + idx) : 0.0;
+                    if (!ht_wait(&full[(q + 1) % HT_S], (uint32_t)(((q + 1) / HT_S) & 1), HT_SPIN)) {
+                        ok = false;
+                        break;
+                    }
+                    const double* Pl = plane[q % HT_S];
+                    const double above = plane[(q + 1) % HT_S][c];
+                    if (in) {
+                        double lap = __dmul_rn(k0, cur);
+                        if (xl) lap = __dadd_rn(lap, __dmul_rn(Pl[c - 1], g.ix2));
+                        if (xr) lap = __dadd_rn(lap, __dmul_rn(Pl[c + 1], g.ix2));
+                        if (yl) lap = __dadd_rn(lap, __dmul_rn(Pl[c - HT_PX], g.iy2));
+                        if (yr) lap = __dadd_rn(lap, __dmul_rn(Pl[c + HT_PX], g.iy2));
+                        if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below, g.iz2));
+                        if (k + 1 < g.nz) lap = __dadd_rn(lap, __dmul_rn(above, g.iz2));
+                        o[idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(v, cur));
+                    }
+                    release(q);
+                    below = cur;
+                    cur = above;
+                }
+                if (!ok) break;
+                release(P + nk + 1);  // plane ke
+                P += nk + 2;
+            }
+        }
+        if (!ok) *abort_v = 1;
     }
-    if (abort_flag && leader) {
-        atomicOr(status, 1);
-        // let the copies still in flight land before the block's shared memory is released
-        for (; waited < issued; ++waited) ht_wait(&full[waited % HT_S], (uint32_t)((waited / HT_S) & 1), HT_SPIN);
-    }
+    __syncthreads();
 }
 
 }  // namespace
@@ -547,26 +593,32 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
     const auto tuned = ctx->tuned.find({(long long)g.nx, (long long)g.ny, (long long)g.nz});
     if (variant == 0 && tuned != ctx->tuned.end()) variant = tuned->second[2];
     if (variant == 2 && hpsi_tma_eligible(g, psi, ld)) {
-        // bands per CTA: the "hpsi_bands_per_thread" key (1, 2, 4 or 8), else the tuned value, else 4
+        // bands per item: the "hpsi_bands_per_thread" key (1, 2, 4 or 8), else the tuned value, else 4
         int nbc = ctx->hpsi_bands_per_thread > 0 ? ctx->hpsi_bands_per_thread
                   : tuned != ctx->tuned.end() && tuned->second[2] == 2 ? tuned->second[0] : 4;
         nbc = std::max(1, std::min(nbc, nbands));
-        const int bx = (g.nx + HT_X - 1) / HT_X, by = (g.ny + HT_Y - 1) / HT_Y;
-        const int groups = (nbands + nbc - 1) / nbc;
-        const int zc = pick_zchunk(g, (long long)bx * by, groups, ctx->num_sms);
-        const int nzc = (g.nz + zc - 1) / zc;
-        const int max_groups = std::max(1, 65535 / nzc);
-        int* st = device_status(ctx);
-        for (int g0 = 0; g0 < groups; g0 += max_groups) {
-            const int ng = std::min(max_groups, groups - g0);
-            const int b0 = g0 * nbc;
-            const int nb = std::min(nbands - b0, ng * nbc);
-            const CUtensorMap tm = hpsi_tensor_map(g, psi + (long long)b0 * ld, ld, nb);
-            hpsi_tma_kernel<<<dim3(bx, by, ng * nzc), dim3(HT_X, HT_Y), 0, ctx->stream>>>(
-                tm, g, V, hpsi + (long long)b0 * ld, ld, nb, nbc, zc, nzc, k0, st);
-            DFT_LAUNCH_CHECK();
-            count_launch(ctx);
+        static int per_sm = 0;
+        if (!per_sm) {
+            DFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hpsi_tma_kernel, HT_THREADS, 0));
+            per_sm = std::max(per_sm, 1);
         }
+        const long long slots = (long long)per_sm * ctx->num_sms;
+        HtWork w{};
+        w.bx = (g.nx + HT_X - 1) / HT_X;
+        w.by = (g.ny + HT_Y - 1) / HT_Y;
+        w.nbc = nbc;
+        const long long runs = (nbands + nbc - 1) / nbc;
+        // z-chunks long enough to amortise the two extra planes, short enough for ~3 items per block
+        w.zchunk = 64;
+        while (w.zchunk > 8 && (long long)w.bx * w.by * runs * ((g.nz + w.zchunk - 1) / w.zchunk) < 3 * slots)
+            w.zchunk >>= 1;
+        w.nzc = (g.nz + w.zchunk - 1) / w.zchunk;
+        w.items = (long long)w.bx * w.by * w.nzc * runs;
+        const int grid = (int)std::min<long long>(w.items, slots);
+        const CUtensorMap tm = hpsi_tensor_map(g, psi, ld, nbands);
+        hpsi_tma_kernel<<<grid, HT_THREADS, 0, ctx->stream>>>(tm, g, V, hpsi, ld, nbands, w, k0, device_status(ctx));
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
         return;
     }
     dim3 block(HB_X, HB_Y);
