@@ -127,17 +127,17 @@ def molecule(w):
 
 def scf_options(w, fast=False, net=None, extra=None):
     """plain: the reference's method in FP64 (cold-start Jacobi, FP64 eigensolver).
-    fast: multigrid cycles from the previous potential (the learned start for each density
-    slot's first solve) before the same Jacobi stop rule, the mixed-precision eigensolver
-    (tcgen05 TF32 hi+lo Gram products and rotations, FP64 finish) with its multigrid
-    preconditioner on large grids, Pulay density mixing and an eigensolver tolerance that
-    follows the density change."""
+    fast: multigrid cycles before the same Jacobi stop rule, started from the learned start
+    for each density slot's first solve and afterwards, for V_H(n_in), from the mixer's own
+    combination of the stored potentials; the mixed-precision eigensolver (tcgen05 TF32 hi+lo
+    Gram products and rotations, FP64 finish) with its multigrid preconditioner on large grids,
+    Pulay density mixing and an eigensolver tolerance that follows the density change."""
     import dft_b200
     if not fast:
         return dft_b200.default_scf_options(stop_abs_de=1e-6, stop_abs_deig=STOP_DEIG, extra_bands=w["extra_bands"])
     kw = dict(stop_abs_de=1e-6, stop_abs_deig=STOP_DEIG, extra_bands=w["extra_bands"],
               poisson_start=dft_b200.POISSON_MULTIGRID,
-              eig_mixed_precision=1, eig_preconditioner=-2, mixer=1, adaptive_eig_tol=1)
+              eig_mixed_precision=1, eig_preconditioner=-2, mixer=1, adaptive_eig_tol=1, poisson_predict=1)
     kw.update(w.get("fast_options", {}))
     kw.update(extra or {})
     o = dft_b200.default_scf_options(**kw)
@@ -267,7 +267,8 @@ def ablation(eng, torch, stream, flush, w, net, reps=1):
     """Time-to-|dE|<1e-6 of one workload as the methods are switched on one at a time: multigrid
     Poisson cycles (coarse-grid start) with the FP64 eigensolver and its multigrid
     preconditioner, then + the learned start, + the mixed-precision (tcgen05) eigensolver, then
-    + Pulay mixing and the adaptive eigensolver tolerance (the headline's fast configuration;
+    + Pulay mixing and the adaptive eigensolver tolerance, then + the V_H(n_in) start from the
+    mixer's combination of stored potentials (the headline's fast configuration;
     Kerker screening and the superposed-atoms start, made for large clusters, are left out: on
     small molecules they cost SCF iterations).
     One untimed solve, then `reps` timed ones (L2 flushed before each); per configuration the
@@ -280,7 +281,8 @@ def ablation(eng, torch, stream, flush, w, net, reps=1):
                 eig_preconditioner=-2)
     steps = [("multigrid", {}), ("+network", {"poisson_net": net.handle}),
              ("+mixed_precision", {"eig_mixed_precision": 1}),
-             ("+pulay_adaptive", {"mixer": 1, "adaptive_eig_tol": 1})]
+             ("+pulay_adaptive", {"mixer": 1, "adaptive_eig_tol": 1}),
+             ("+hartree_start_from_mixer", {"poisson_predict": 1})]
     out, kw = {}, dict(base)
     for name, extra in steps:
         kw.update(extra)
