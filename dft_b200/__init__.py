@@ -55,7 +55,8 @@ class dft_scf_opts(C.Structure):
 class dft_autotune_report(C.Structure):
     _fields_ = [("hpsi_bands_per_thread", C.c_int), ("hpsi_ms", C.c_double * 3),
                 ("jacobi_sweeps_per_launch", C.c_int), ("jacobi_us_per_sweep", C.c_double * 6),
-                ("cached", C.c_int), ("hpsi_variant", C.c_int), ("hpsi_tma_ms", C.c_double * 4)]
+                ("cached", C.c_int), ("hpsi_variant", C.c_int), ("hpsi_tma_ms", C.c_double * 4),
+                ("hpsi_prefetch_ms", C.c_double)]
 
 
 # dft_poisson_start
@@ -381,7 +382,8 @@ class Engine:
         return {"hpsi_bands_per_thread": r.hpsi_bands_per_thread, "hpsi_ms": list(r.hpsi_ms),
                 "jacobi_sweeps_per_launch": r.jacobi_sweeps_per_launch,
                 "jacobi_us_per_sweep": list(r.jacobi_us_per_sweep), "cached": bool(r.cached),
-                "hpsi_variant": r.hpsi_variant, "hpsi_tma_ms": list(r.hpsi_tma_ms)}
+                "hpsi_variant": r.hpsi_variant, "hpsi_tma_ms": list(r.hpsi_tma_ms),
+                "hpsi_prefetch_ms": r.hpsi_prefetch_ms}
 
     def counter(self, name: str) -> int:
         return load().dft_context_counter(self.ctx, name.encode())

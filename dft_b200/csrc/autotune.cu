@@ -116,6 +116,11 @@ void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* 
         if (r.hpsi_tma_ms[i] < best) best = r.hpsi_tma_ms[i], best_bpt = nbc[i], best_var = 2;
     }
     check_device_status(ctx, "autotune");
+    // the prefetching single-band march
+    ctx->hpsi_variant = 3;
+    ctx->hpsi_bands_per_thread = 1;
+    r.hpsi_prefetch_ms = time_ms(ctx, ev, 3, [&] { apply_hamiltonian(ctx, g, V, psi, hpsi, tb, N); });
+    if (r.hpsi_prefetch_ms < best) best = r.hpsi_prefetch_ms, best_bpt = 1, best_var = 3;
     ctx->hpsi_variant = 0;
     r.hpsi_bands_per_thread = best_bpt;
     r.hpsi_variant = best_var;

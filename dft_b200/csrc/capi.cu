@@ -153,7 +153,7 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
             NEED(value == 0 || value == 1, "tensor_core_ring must be 0 or 1");
             ctx->tc_ring = (int)value;
         } else if (k == "hpsi_variant") {
-            NEED(value >= 0 && value <= 2, "hpsi_variant must be 0, 1 or 2");
+            NEED(value >= 0 && value <= 3, "hpsi_variant must be 0, 1, 2 or 3");
             ctx->hpsi_variant = (int)value;
         } else if (k == "multigrid_fused_restriction" || k == "multigrid_coarsest_sor") {
             NEED(value == 0 || value == 1, "multigrid keys take 0 or 1");

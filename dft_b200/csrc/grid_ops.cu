@@ -208,6 +208,48 @@ __global__ void __launch_bounds__(HB_X* HB_Y) hpsi1_kernel(Grid g, const double*
     }
 }
 
+// hpsi1_kernel with the next plane's loads issued one step ahead ("hpsi_variant" = 3): while
+// plane k is computed, psi at k + 2 and V at k + 1 are already in flight, so each thread keeps
+// two steps of HBM loads outstanding instead of one.  Same operations in the same order.
+__global__ void __launch_bounds__(HB_X* HB_Y, 8) hpsi1p_kernel(Grid g, const double* __restrict__ V,
+                                                           const double* __restrict__ psi, double* __restrict__ out,
+                                                           long long ld, int zchunk, int nzc, double k0) {
+    const int i = blockIdx.x * HB_X + threadIdx.x;
+    const int j = blockIdx.y * HB_Y + threadIdx.y;
+    const int band = blockIdx.z / nzc;
+    const int kc = blockIdx.z - band * nzc;
+    if (i >= g.nx || j >= g.ny) return;
+    const double* __restrict__ p = psi + (long long)band * ld;
+    double* __restrict__ o = out + (long long)band * ld;
+    const long long sxy = (long long)g.nx * g.ny;
+    const int kb = kc * zchunk;
+    const int ke = min(g.nz, kb + zchunk);
+    long long idx = (long long)kb * sxy + (long long)j * g.nx + i;
+    double below = kb > 0 ? __ldg(p + idx - sxy) : 0.0;
+    double cur = __ldg(p + idx);
+    double above = kb + 1 < g.nz ? __ldg(p + idx + sxy) : 0.0;
+    double v = __ldg(V + idx);
+    const bool xl = i > 0, xr = i + 1 < g.nx, yl = j > 0, yr = j + 1 < g.ny;
+    for (int k = kb; k < ke; ++k, idx += sxy) {
+        const bool zr = k + 1 < g.nz;
+        const bool more = k + 1 < ke;  // the next step exists: prefetch its loads
+        const double above2 = (more && k + 2 < g.nz) ? __ldg(p + idx + 2 * sxy) : 0.0;
+        const double vnext = more ? __ldg(V + idx + sxy) : 0.0;
+        double lap = __dmul_rn(k0, cur);
+        if (xl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - 1), g.ix2));
+        if (xr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + 1), g.ix2));
+        if (yl) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx - g.nx), g.iy2));
+        if (yr) lap = __dadd_rn(lap, __dmul_rn(__ldg(p + idx + g.nx), g.iy2));
+        if (k > 0) lap = __dadd_rn(lap, __dmul_rn(below, g.iz2));
+        if (zr) lap = __dadd_rn(lap, __dmul_rn(above, g.iz2));
+        o[idx] = __dadd_rn(__dmul_rn(-0.5, lap), __dmul_rn(v, cur));
+        below = cur;
+        cur = above;
+        above = above2;
+        v = vnext;
+    }
+}
+
 // One thread per (i,j) column of NB bands, marching k over a z-chunk: V is read once per point
 // for all NB bands and the NB bands' loads are independent, so more of them are in flight.
 // reference KohnShamHamiltonianMolecule.cpp:59-177: lap = k0*c (+ neighbours in the order
@@ -633,6 +675,7 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
     nbt = std::min(nbt, std::max(1, nbands));
     nbt = nbt >= 4 ? 4 : nbt >= 2 ? 2 : 1;
     if (ctx->hpsi_variant == 1) nbt = std::min(nbt, 2);
+    if (variant == 3) nbt = 1;  // the prefetching march is single-band
     const int groups = (nbands + nbt - 1) / nbt;
     const int zc = pick_zchunk(g, (long long)bx * by, groups, ctx->num_sms);
     const int nzc = (g.nz + zc - 1) / zc;
@@ -652,6 +695,8 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
             hpsi_kernel<4><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
         } else if (nbt == 2) {
             hpsi_kernel<2><<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, nb, zc, nzc, k0);
+        } else if (variant == 3) {
+            hpsi1p_kernel<<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, zc, nzc, k0);
         } else {
             hpsi1_kernel<<<grid, block, 0, ctx->stream>>>(g, V, pi, po, ld, zc, nzc, k0);
         }

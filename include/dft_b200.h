@@ -93,7 +93,8 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *                               (cp.async.bulk.tensor) into a 6-stage shared-memory ring, each
  *                               block walking hpsi_bands_per_thread bands (0 = 4) of its column
  *                               tile; needs nx and ld even and a 16-byte-aligned psi, else 0 is
- *                               used.  Results identical for every value.
+ *                               used; 3 = the single-band march of 0 with the next plane's loads
+ *                               issued one step ahead.  Results identical for every value.
  *   "grid_barrier_poll_limit":  0 = 2^24 (default): polls a block of the persistent Jacobi
  *                               launch makes at a grid barrier before it gives up; the solve then
  *                               fails with DFT_CUDA_ERROR and the context stays usable.
@@ -127,8 +128,10 @@ typedef struct {
     int jacobi_sweeps_per_launch;  /* chosen */
     double jacobi_us_per_sweep[6]; /* -2, -1, 1, 2, 4, 8 */
     int cached;                    /* 1: the choice was remembered, nothing was timed */
-    int hpsi_variant;              /* chosen: 0 = the register march (hpsi_ms), 2 = the TMA ring */
+    int hpsi_variant;              /* chosen: 0 = the register march (hpsi_ms), 2 = the TMA ring,
+                                      3 = the prefetching single-band march */
     double hpsi_tma_ms[4];         /* TMA plane ring with 1, 2, 4, 8 bands per block (-1: not eligible) */
+    double hpsi_prefetch_ms;       /* the prefetching single-band march */
 } dft_autotune_report;
 dft_status_t dft_autotune(dft_context* ctx, const dft_grid* g, int nbands, dft_autotune_report* report);
 /* The cudaStream_t the context launches on, as an opaque handle (for event timing). */

@@ -31,12 +31,13 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
-@pytest.fixture(params=[(0, 0), (0, 1), (0, 2), (0, 4), (1, 1), (1, 2), (2, 0), (2, 8)],
+@pytest.fixture(params=[(0, 0), (0, 1), (0, 2), (0, 4), (1, 1), (1, 2), (2, 0), (2, 8), (3, 0)],
                 ids=lambda t: f"v{t[0]}bpt{t[1]}")
 def hpsi_bands_per_thread(request, engine):
     """Every H psi launch shape: neighbours through L1 (variant 0) with auto, 1, 2 or 4 bands per
     thread, the shared-memory plane tile (variant 1) with 1 or 2, and the TMA plane ring
-    (variant 2, 4 or 8 bands per block; an odd leading dimension falls back to variant 0)."""
+    (variant 2, 4 or 8 bands per block; an odd leading dimension falls back to variant 0) and the
+    prefetching single-band march (variant 3)."""
     variant, bpt = request.param
     engine.set_tuning("hpsi_variant", variant)
     engine.set_tuning("hpsi_bands_per_thread", bpt)
