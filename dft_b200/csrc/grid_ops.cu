@@ -1490,6 +1490,21 @@ double monopole_prepare(dft_context* ctx, const Grid& g, const double* rho, doub
     return q;
 }
 
+namespace {
+__global__ void zero_faces_kernel(Grid g, double* __restrict__ v) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((long long)g.nx * g.ny));
+        if (i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz) v[p] = 0.0;
+    }
+}
+}  // namespace
+
+void zero_faces(dft_context* ctx, const Grid& g, double* v) {
+    zero_faces_kernel<<<ew_blocks(ctx, g.N), 256, 0, ctx->stream>>>(g, v);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
 void add_into(dft_context* ctx, long long n, const double* a, const double* b, double* out) {
     add_into_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, a, b, out);
     DFT_LAUNCH_CHECK();

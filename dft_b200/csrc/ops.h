@@ -45,6 +45,8 @@ JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho,
 // zero-face solution for rho_prime has the face values Q/|r|.  monopole_width: s for grid g.
 double monopole_prepare(dft_context* ctx, const Grid& g, const double* rho, double* rho_prime, double* vc);
 double monopole_width(const Grid& g);
+// v = 0 on the six faces of g (the zero-face solvers' boundary)
+void zero_faces(dft_context* ctx, const Grid& g, double* v);
 // out = a + b (plain addition)
 void add_into(dft_context* ctx, long long n, const double* a, const double* b, double* out);
 

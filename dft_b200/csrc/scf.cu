@@ -156,6 +156,10 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             double res = 0.0;
             if (have_prev) {
                 DFT_CUDA(cudaMemcpyAsync(vstart.p, v, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+                // the multigrid keeps the start's faces; the zero-face part of the monopole
+                // boundary must start from exactly zero faces (a start combined from potentials
+                // of slightly different total charge carries face values of order dQ/|r|)
+                if (monopole) zero_faces(ctx, g, vstart.p);
                 cyc = multigrid(ctx, g, d, vstart.p, 0.5 * o.poisson_tol, 40, &res);
             } else {
                 PoissonGuessInfo info;
