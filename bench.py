@@ -6,7 +6,8 @@ A step is one full SCF solve of the workload, from the nuclei to |dE| < 1e-6 Ha 
 occupied eigenvalue changed by less than 1e-7 Ha in the last iteration (the metric's
 converged SCF; the reference's own three-criterion stop is exercised by the parity tests).
 The headline configuration is the fast one: multigrid Poisson starts (the learned start for
-each density slot's first solve), the mixed-precision eigensolver with its multigrid
+each density slot's first solve, then the mixer's combination of the stored potentials for
+V_H(n_in)), the mixed-precision eigensolver with its multigrid
 preconditioner, Pulay mixing and an eigensolver tolerance that follows the density change.
 The plain FP64 method (the reference's algorithm: cold-start Jacobi, FP64 eigensolver, linear
 mixing) is timed in the same run with the same stop rule, and an FP64 run of the plain method
