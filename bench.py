@@ -644,7 +644,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": bench_config(args, w, world),
-        "run": {"scf_iterations": last.iterations, "energy": last.total,
+        "run": {"step_ms": [round(x, 3) for x in ms], "scf_iterations": last.iterations, "energy": last.total,
                    "seconds_to_1e-6": ms_per_step / 1e3,
                    "phase_ms": {k: round(sum(h[k] for h in last.history), 2)
                                 for k in ("ms_hartree", "ms_xc", "ms_orbitals", "ms_density", "ms_energy")},

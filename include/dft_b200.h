@@ -306,8 +306,8 @@ typedef struct {
     /* Density mixing and eigensolver tolerance (no counterpart in the reference; the defaults
      * 0 keep its linear mixer, SelfConsistentFieldMolecule.cpp:447-484, and its fixed tolerance). */
     int mixer;               /* 0: linear with the adaptive factor; 1: Pulay (DIIS) on n_out - n_in */
-    int pulay_depth;         /* history length for the Pulay mixer (0 = 8) */
-    double pulay_beta;       /* step along the extrapolated residual (0 = 0.2) */
+    int pulay_depth;         /* history length for the Pulay mixer (0 = 16, at most 16) */
+    double pulay_beta;       /* step along the extrapolated residual (0 = 0.5) */
     int adaptive_eig_tol;    /* 1: eigensolver tolerance max(eig.tol, min(1e-3, 0.1 * previous dRho)) */
     double smearing_kt;      /* > 0: Fermi-Dirac occupations at this temperature (Ha) over the extra
                                 bands instead of the reference's integer aufbau (0) */
