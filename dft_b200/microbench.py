@@ -177,7 +177,8 @@ def main():
         out.update(system=a.system, poisson=a.poisson, mixed=a.mixed, precond=a.precond, iterations=r.iterations,
                    converged=r.converged,
                    energy=r.total,
-                   seconds=r.seconds, launches=eng.launches, eigenvalues=r.eigenvalues[:8],
+                   seconds=r.seconds, launches=eng.launches,
+                   tensor_core_products=eng.counter("tensor_core_products"), eigenvalues=r.eigenvalues[:8],
                    history=[{k: h[k] for k in ("iteration", "energy", "energy_difference", "density_difference",
                                                "ks_residual", "eigenvalue_difference", "poisson_sweeps_in",
                                                "poisson_sweeps_out", "poisson_cycles_in", "poisson_cycles_out",
