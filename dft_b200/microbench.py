@@ -92,8 +92,8 @@ def main():
     ap.add_argument("--stop-abs-deig", type=float, default=0.0)
     ap.add_argument("--kerker", type=float, default=0.0, help="scf: Kerker screening q0 (bohr^-1), 0 = off")
     ap.add_argument("--atoms", type=int, default=0, help="scf: superposed-atoms start (1)")
-    ap.add_argument("--pulay-beta", type=float, default=0.0, help="scf: Pulay step (0 = 0.2)")
-    ap.add_argument("--pulay-depth", type=int, default=0, help="scf: Pulay history (0 = 8)")
+    ap.add_argument("--pulay-beta", type=float, default=0.0, help="scf: Pulay step (0 = 0.5)")
+    ap.add_argument("--pulay-depth", type=int, default=0, help="scf: Pulay history (0 = 16)")
     ap.add_argument("--boundary", type=int, default=0, help="scf: Hartree faces, 0 reference, 1 Q/|r| (monopole)")
     ap.add_argument("--predict", type=int, default=0, help="scf: V_H(n_in) start from the mixer's combination (1)")
     ap.add_argument("--tuning", default="", help="context tuning keys, e.g. orthonormalise_adaptive=0,hpsi_variant=2")
