@@ -71,18 +71,39 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled every 200 ms during the timed region,
+    through NVML in this process (the data `nvidia-smi --query-gpu=clocks.sm,...` reports).
+    A separate `nvidia-smi -lms 200` process made single SCF steps of this workload take
+    0.5-1 s instead of 50 ms at random on these boxes, with any query set; in-process NVML
+    polling did not.  Falls back to nvidia-smi when NVML is unavailable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", 0x8),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap", 0x4))
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.lines = []
+        self.samples = []  # (sm MHz, max MHz, reason bits) from NVML
+        self.nvml = None
+        self.stop = False
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -93,11 +114,25 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        n = self.nvml
+        while not self.stop:
+            try:
+                self.samples.append((n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM),
+                                     n.nvmlDeviceGetMaxClockInfo(self.handle, n.NVML_CLOCK_SM),
+                                     n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)))
+            except Exception:
+                pass
+            time.sleep(0.2)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop = True
+        if self.nvml is not None:
+            self.t.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -107,6 +142,15 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], None, set()
+        if self.nvml is not None:
+            for clk, cmax, bits in self.samples:
+                sm.append(float(clk))
+                mx = float(cmax)
+                for name, attr, dflt in self.REASONS:
+                    if bits & getattr(self.nvml, attr, dflt):
+                        reasons.add(name)
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                    "samples": len(sm), "source": "nvml"}
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for l in self.lines:
             c = [x.strip() for x in l.split(",")]
@@ -121,7 +165,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 def molecule(w):
