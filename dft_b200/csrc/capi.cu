@@ -114,6 +114,8 @@ dft_status_t dft_context_destroy(dft_context* ctx) {
         if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
         if (ctx->gram_ticket) cudaFree(ctx->gram_ticket);
         if (ctx->dev_status) cudaFree(ctx->dev_status);
+        for (auto& kv : ctx->buf_pool) cudaFree(kv.second);
+        ctx->buf_pool.clear();
         for (auto& kv : ctx->mg_graphs) cudaGraphExecDestroy(kv.second.exec);
         cudaStreamDestroy(ctx->stream);
     });

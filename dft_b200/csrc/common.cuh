@@ -131,6 +131,10 @@ struct dft_context {
     double* host_pinned = nullptr;  // small pinned staging area for scalars
     size_t host_pinned_bytes = 0;
     void* gram_ticket = nullptr;    // block counter of the one-launch narrow Gram product
+    // device buffers an SCF released, kept for the next SCF of the same sizes (bytes -> pointer):
+    // repeated cudaMalloc/cudaFree of the SCF state stalled single solves by up to 0.5 s
+    std::multimap<size_t, void*> buf_pool;
+    size_t buf_pool_bytes = 0;
 };
 
 namespace dftb {

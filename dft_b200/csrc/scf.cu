@@ -22,15 +22,37 @@ inline double ms_since(Clock::time_point t) {
     return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
 }
 
+// An SCF's device buffer, taken from and given back to the context's pool of released
+// buffers (exact sizes); everything stays stream-ordered on the context's one stream, so a
+// buffer handed to the next SCF is used only after this SCF's kernels.  The pool keeps at most
+// 32 GiB; beyond that a released buffer is freed.
 struct DevBuf {
+    dft_context* c = nullptr;
     double* p = nullptr;
+    size_t bytes = 0;
     DevBuf() = default;
-    explicit DevBuf(size_t n) {
-        if (n) DFT_CUDA(cudaMalloc(&p, n * sizeof(double)));
+    DevBuf(dft_context* ctx, size_t n) : c(ctx), bytes(n * sizeof(double)) {
+        if (!n) return;
+        auto it = c->buf_pool.find(bytes);
+        if (it != c->buf_pool.end()) {
+            p = (double*)it->second;
+            c->buf_pool.erase(it);
+            c->buf_pool_bytes -= bytes;
+        } else {
+            DFT_CUDA(cudaMalloc(&p, bytes));
+        }
     }
-    ~DevBuf() {
-        if (p) cudaFree(p);
+    void release() {
+        if (!p) return;
+        if (c && c->buf_pool_bytes + bytes <= (32ULL << 30)) {
+            c->buf_pool.emplace(bytes, p);
+            c->buf_pool_bytes += bytes;
+        } else {
+            cudaFree(p);
+        }
+        p = nullptr;
     }
+    ~DevBuf() { release(); }
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
 };
@@ -129,16 +151,17 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     if (pstart == DFT_POISSON_NETWORK && !o.poisson_net)
         fail(DFT_INVALID_ARGUMENT, "poisson_start DFT_POISSON_NETWORK needs poisson_net");
 
-    DevBuf vext(N), da(N), db(N), rho(N), vh(N), vxa(N), vxb(N), va(N), vb(N), oa(N), ob(N), orho(N), ovh(N);
-    DevBuf vstart(pstart >= DFT_POISSON_NETWORK ? (size_t)N : 0);
+    DevBuf vext(ctx, N), da(ctx, N), db(ctx, N), rho(ctx, N), vh(ctx, N), vxa(ctx, N), vxb(ctx, N), va(ctx, N),
+        vb(ctx, N), oa(ctx, N), ob(ctx, N), orho(ctx, N), ovh(ctx, N);
+    DevBuf vstart(ctx, pstart >= DFT_POISSON_NETWORK ? (size_t)N : 0);
     dft_pnet* net = pstart == DFT_POISSON_COARSE ? nullptr : o.poisson_net;
     // Poisson solve of density d into v with the chosen start; `have_prev` says whether v
     // still holds this slot's potential from the previous iteration.
     // Monopole faces: the zero-face solve runs on (rho', V') per slot, V_H = V' + V_c.
     const bool monopole = o.hartree_boundary == 1;
     if (monopole) monopole_width(g);  // the origin must lie well inside the box
-    DevBuf mrho(monopole ? (size_t)N : 0), mvc(monopole ? (size_t)N : 0), mvp0(monopole ? (size_t)N : 0),
-        mvp1(monopole ? (size_t)N : 0);
+    DevBuf mrho(ctx, monopole ? (size_t)N : 0), mvc(ctx, monopole ? (size_t)N : 0), mvp0(ctx, monopole ? (size_t)N : 0),
+        mvp1(ctx, monopole ? (size_t)N : 0);
     int last_cycles = 0;  // multigrid cycles of the last solve
     auto poisson = [&](const double* d_in, double* v_out, bool have_prev) {
         last_cycles = 0;
@@ -182,7 +205,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         if (monopole) add_into(ctx, N, v, mvc.p, v_out);
         return r;
     };
-    DevBuf psia((size_t)bands_a * ld), psib(closed ? 0 : (size_t)bands_b * ld);
+    DevBuf psia(ctx, (size_t)bands_a * ld), psib(ctx, closed ? 0 : (size_t)bands_b * ld);
     std::vector<double> eiga(bands_a), eigb(bands_b), resa(bands_a), resb(bands_b);
     std::vector<double> occa(bands_a, 0.0), occb(bands_b, 0.0);
     for (int i = 0; i < na; ++i) occa[i] = 1.0;  // buildSpinOccupations: one electron per orbital
@@ -216,8 +239,10 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
                                                    std::max(bands_a, bands_b) + 16LL) - 1;
         const int want = (int)std::min<long long>(atomic_orbital_count(nnuc, Z), kcap);
         if (want > 0) {
-            DevBuf tmp((size_t)want * ld);
+            DevBuf tmp(ctx, (size_t)want * ld);
             std::swap(aobuf.p, tmp.p);
+            std::swap(aobuf.c, tmp.c);
+            std::swap(aobuf.bytes, tmp.bytes);
         }
         nao = atomic_start(ctx, g, nnuc, Z, xyz, kind, na, nb, da.p, db.p, aobuf.p, ld, want);
     } else {
@@ -275,7 +300,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     const int pdepth = o.pulay_depth > 0 ? std::min(o.pulay_depth, 16) : 16;
     const double pbeta = o.pulay_beta > 0.0 ? o.pulay_beta : 0.5;
     if (o.mixer != 0 && o.mixer != 1) fail(DFT_INVALID_ARGUMENT, "unknown mixer %d", o.mixer);
-    DevBuf phist(o.mixer == 1 ? (size_t)2 * pdepth * ns * N : 0);
+    DevBuf phist(ctx, o.mixer == 1 ? (size_t)2 * pdepth * ns * N : 0);
     // Hartree start from the mixer (option): V_H is linear in the density, so the mixer's
     // combination of the stored V_H(n_in,i) and V_H(n_out,i) - V_H(n_in,i) is a start for the
     // next V_H(n_in) that is as close as those solves were (the unchanged stop rule ends it)
@@ -284,14 +309,14 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     const bool vpredict = o.poisson_predict >= 1 && pstart != DFT_POISSON_COLD;
     // 2: also V_H(n_out) from V_H(n_in) + the previous iteration's V_H(n_out) - V_H(n_in)
     const bool vpredict_out = o.poisson_predict == 2 && pstart != DFT_POISSON_COLD;
-    DevBuf vres(vpredict_out ? (size_t)N : 0);
-    DevBuf vhist(vpredict && o.mixer == 1 ? (size_t)2 * pdepth * N : 0);
-    DevBuf vtmp(vpredict && o.mixer == 1 && pdepth > 8 ? (size_t)N : 0);
+    DevBuf vres(ctx, vpredict_out ? (size_t)N : 0);
+    DevBuf vhist(ctx, vpredict && o.mixer == 1 ? (size_t)2 * pdepth * N : 0);
+    DevBuf vtmp(ctx, vpredict && o.mixer == 1 && pdepth > 8 ? (size_t)N : 0);
     // Kerker screening of the total-charge residual (option; 0 = off, the reference's mixer)
     const double kq0 = o.kerker_q0;
     if (kq0 < 0.0 || !std::isfinite(kq0)) fail(DFT_INVALID_ARGUMENT, "kerker_q0 must be >= 0");
     const double kq2 = kq0 * kq0;
-    DevBuf kbuf(kq0 > 0.0 ? (size_t)(ns + 2) * N : 0);
+    DevBuf kbuf(ctx, kq0 > 0.0 ? (size_t)(ns + 2) * N : 0);
     std::vector<double> Bp((size_t)pdepth * pdepth, 0.0);
     int pcount = 0, phead = 0;
     auto pulay_mix = [&]() {
@@ -480,11 +505,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         if (!closed)
             rec.eig_iterations_beta = solve_orbitals(ctx, g, vb.p, nconv_b, bands_b, psib.p, ld, !first_atoms,
                                                      eigb.data(), resb.data(), ek, sb, nao);
-        if (first_atoms && aobuf.p) {
-            sync(ctx);
-            cudaFree(aobuf.p);
-            aobuf.p = nullptr;
-        }
+        if (first_atoms && aobuf.p) aobuf.release();
         if (kt > 0.0) {
             nconv_a = fermi(eiga, na, occa);
             if (closed) {
