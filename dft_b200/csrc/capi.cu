@@ -116,6 +116,7 @@ dft_status_t dft_context_destroy(dft_context* ctx) {
         if (ctx->dev_status) cudaFree(ctx->dev_status);
         for (auto& kv : ctx->buf_pool) cudaFree(kv.second);
         ctx->buf_pool.clear();
+        for (auto& kv : ctx->radial_tables) cudaFree(kv.second.dens);
         for (auto& kv : ctx->mg_graphs) cudaGraphExecDestroy(kv.second.exec);
         cudaStreamDestroy(ctx->stream);
     });

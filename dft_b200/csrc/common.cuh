@@ -100,6 +100,14 @@ struct MGGraph {
     long long launches;  // kernels per replay
 };
 
+// One element's radial atom, kept for the superposed-atoms start: total density and the
+// alpha shells' radial functions on the radial grid (device), and each shell's (n, l).
+struct RadialTable {
+    double* dens = nullptr;
+    double* orbs = nullptr;
+    std::vector<std::array<int, 2>> shells;
+};
+
 struct dft_context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -135,6 +143,8 @@ struct dft_context {
     // repeated cudaMalloc/cudaFree of the SCF state stalled single solves by up to 0.5 s
     std::multimap<size_t, void*> buf_pool;
     size_t buf_pool_bytes = 0;
+    // radial atoms already solved for the superposed-atoms start: {Z, kind, points, rmax bits}
+    std::map<std::array<long long, 4>, RadialTable> radial_tables;
 };
 
 namespace dftb {

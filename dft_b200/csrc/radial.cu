@@ -593,29 +593,57 @@ int atomic_orbital_count(int nnuc, const int* Z) {
 
 void radial_atom_tables(dft_context* ctx, int nz, const int* Z, int kind, long points, double rmax, double* dens,
                         double* orbs, std::vector<std::vector<std::array<int, 2>>>& shells) {
-    std::vector<int> kinds(nz, kind);
-    std::vector<dft_atom_result> res(nz);
-    std::vector<RunSpec> specs;
-    long long per_run = 0;
-    const double* ws = run_batch(ctx, nz, Z, kinds.data(), points, rmax, res.data(), specs, per_run);
+    // elements not solved before on this context (for this functional and radial grid) are
+    // solved in one batch and kept; every element is then copied from the kept tables
+    long long rbits;
+    std::memcpy(&rbits, &rmax, sizeof(rbits));
+    auto key = [&](int z) { return std::array<long long, 4>{z, kind, points, rbits}; };
+    std::vector<int> todo;
+    for (int rr = 0; rr < nz; ++rr)
+        if (!ctx->radial_tables.count(key(Z[rr])) && std::find(todo.begin(), todo.end(), Z[rr]) == todo.end())
+            todo.push_back(Z[rr]);
+    if (!todo.empty()) {
+        const int nt = (int)todo.size();
+        std::vector<int> kinds(nt, kind);
+        std::vector<dft_atom_result> res(nt);
+        std::vector<RunSpec> specs;
+        long long per_run = 0;
+        const double* ws = run_batch(ctx, nt, todo.data(), kinds.data(), points, rmax, res.data(), specs, per_run);
+        for (int rr = 0; rr < nt; ++rr) {
+            if (res[rr].status != DFT_OK)
+                fail((dft_status_t)res[rr].status, "radial atom Z = %d failed (status %d)", todo[rr], res[rr].status);
+            RadialTable t;
+            const RunSpec& sp = specs[rr];
+            for (int q = 0; q < sp.norb; ++q)
+                if (sp.spin[q] == 0) t.shells.push_back({sp.n[q], sp.l[q]});  // every occupied alpha (n, l)
+            if ((int)t.shells.size() > RADIAL_MAX_SHELLS)
+                fail(DFT_INVALID_ARGUMENT, "atom Z = %d has more than %d shells", todo[rr], RADIAL_MAX_SHELLS);
+            DFT_CUDA(cudaMalloc(&t.dens, sizeof(double) * points * (1 + RADIAL_MAX_SHELLS)));
+            t.orbs = t.dens + points;
+            const double* base = ws + (long long)rr * per_run;
+            DFT_CUDA(cudaMemcpyAsync(t.dens, base + (long long)A_OD * points, sizeof(double) * points,
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+            int k = 0;
+            for (int q = 0; q < sp.norb; ++q) {
+                if (sp.spin[q] != 0) continue;
+                DFT_CUDA(cudaMemcpyAsync(t.orbs + (long long)k * points,
+                                         base + (long long)(A_COUNT + q * O_COUNT + O_U) * points,
+                                         sizeof(double) * points, cudaMemcpyDeviceToDevice, ctx->stream));
+                ++k;
+            }
+            ctx->radial_tables[key(todo[rr])] = std::move(t);
+        }
+    }
     shells.assign(nz, {});
     for (int rr = 0; rr < nz; ++rr) {
-        if (res[rr].status != DFT_OK)
-            fail((dft_status_t)res[rr].status, "radial atom Z = %d failed (status %d)", Z[rr], res[rr].status);
-        const double* base = ws + (long long)rr * per_run;
-        DFT_CUDA(cudaMemcpyAsync(dens + (long long)rr * points, base + (long long)A_OD * points,
-                                 sizeof(double) * points, cudaMemcpyDeviceToDevice, ctx->stream));
-        const RunSpec& sp = specs[rr];
-        for (int q = 0; q < sp.norb; ++q) {
-            if (sp.spin[q] != 0) continue;  // the alpha shells: every occupied (n, l) of the atom
-            const int k = (int)shells[rr].size();
-            if (k >= RADIAL_MAX_SHELLS) fail(DFT_INVALID_ARGUMENT, "atom Z = %d has more than %d shells", Z[rr],
-                                             RADIAL_MAX_SHELLS);
-            DFT_CUDA(cudaMemcpyAsync(orbs + ((long long)rr * RADIAL_MAX_SHELLS + k) * points,
-                                     base + (long long)(A_COUNT + q * O_COUNT + O_U) * points,
-                                     sizeof(double) * points, cudaMemcpyDeviceToDevice, ctx->stream));
-            shells[rr].push_back({sp.n[q], sp.l[q]});
-        }
+        const RadialTable& t = ctx->radial_tables.at(key(Z[rr]));
+        DFT_CUDA(cudaMemcpyAsync(dens + (long long)rr * points, t.dens, sizeof(double) * points,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+        if (!t.shells.empty())
+            DFT_CUDA(cudaMemcpyAsync(orbs + (long long)rr * RADIAL_MAX_SHELLS * points, t.orbs,
+                                     sizeof(double) * points * t.shells.size(), cudaMemcpyDeviceToDevice,
+                                     ctx->stream));
+        shells[rr] = t.shells;
     }
 }
 

@@ -233,7 +233,7 @@ typedef struct {
     int preconditioner;  /* 0: the reference's diagonal (theta - diag)^-1 (EigenvalueSolverMolecule.cpp:521-555);
                             k > 0: k damped-Jacobi smoothing steps on (T + sigma) t = r (default 4);
                             -1: one multigrid V(2,2) cycle on (T + sigma) t = r, all bands batched;
-                            -2: -1 on grids of 80^3 points or more, 4 below;
+                            -2: -1 on grids of 32^3 points or more, 4 below;
                             -3: -1 plus the learned correction of preconditioner_net, trained by
                                 dft_pnet_train_preconditioner */
     int mixed_precision; /* 1: Gram products on the tensor cores (TF32 hi+lo split, FP32 accumulation)
