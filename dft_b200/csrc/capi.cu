@@ -165,6 +165,9 @@ dft_status_t dft_context_set_tuning(dft_context* ctx, const char* key, long valu
             dftb::sync(ctx);
             for (auto& kv : ctx->mg_graphs) cudaGraphExecDestroy(kv.second.exec);
             ctx->mg_graphs.clear();
+        } else if (k == "hpsi_zchunk") {
+            NEED(value >= 0 && value <= 65536, "hpsi_zchunk must be 0 (auto) or a plane count");
+            ctx->hpsi_zchunk = (int)value;
         } else if (k == "tensor_core_tma") {
             NEED(value == 0 || value == 1, "tensor_core_tma must be 0 or 1");
             ctx->tc_tma = (int)value;

@@ -121,6 +121,7 @@ struct dft_context {
     int hpsi_variant = 0;              // H psi: 0 = neighbours through L1, 1 = shared-memory plane tile,
                                        // 2 = TMA plane ring (where eligible, else 0)
     int* dev_status = nullptr;         // device word set by kernels whose bounded waits gave up
+    int hpsi_zchunk = 0;               // H psi march length per block (0 = auto)
     int ortho_adaptive = 1;            // FP64 orthonormalisation: skip the second pass when safe (1)
     int mg_fused_restrict = 1;         // multigrid: one-pass 3-D restriction on fine grids <= 64^3 (1)
     int mg_coarsest_sor = 1;           // multigrid: red-black SOR coarsest solve (1) or Jacobi sweeps (0)

@@ -98,6 +98,8 @@ dft_status_t dft_context_synchronize(dft_context* ctx);
  *   "grid_barrier_poll_limit":  0 = 2^24 (default): polls a block of the persistent Jacobi
  *                               launch makes at a grid barrier before it gives up; the solve then
  *                               fails with DFT_CUDA_ERROR and the context stays usable.
+ *   "hpsi_zchunk":              0 = auto (default), else the number of z-planes each block of the
+ *                               register-march H psi kernels walks (same results for every value).
  *   "multigrid_fused_restriction": 1 (default) = the Poisson multigrid restricts in one 3-D pass
  *                               on fine grids up to 64^3 (0: three separable passes).
  *   "multigrid_coarsest_sor":   1 (default) = the coarsest multigrid level is solved by red-black
