@@ -56,7 +56,7 @@ class dft_autotune_report(C.Structure):
     _fields_ = [("hpsi_bands_per_thread", C.c_int), ("hpsi_ms", C.c_double * 3),
                 ("jacobi_sweeps_per_launch", C.c_int), ("jacobi_us_per_sweep", C.c_double * 6),
                 ("cached", C.c_int), ("hpsi_variant", C.c_int), ("hpsi_tma_ms", C.c_double * 4),
-                ("hpsi_prefetch_ms", C.c_double)]
+                ("hpsi_prefetch_ms", C.c_double), ("hpsi_zchunk", C.c_int), ("hpsi_zchunk_ms", C.c_double * 5)]
 
 
 # dft_poisson_start
@@ -383,7 +383,8 @@ class Engine:
                 "jacobi_sweeps_per_launch": r.jacobi_sweeps_per_launch,
                 "jacobi_us_per_sweep": list(r.jacobi_us_per_sweep), "cached": bool(r.cached),
                 "hpsi_variant": r.hpsi_variant, "hpsi_tma_ms": list(r.hpsi_tma_ms),
-                "hpsi_prefetch_ms": r.hpsi_prefetch_ms}
+                "hpsi_prefetch_ms": r.hpsi_prefetch_ms, "hpsi_zchunk": r.hpsi_zchunk,
+                "hpsi_zchunk_ms": list(r.hpsi_zchunk_ms)}
 
     def counter(self, name: str) -> int:
         return load().dft_context_counter(self.ctx, name.encode())

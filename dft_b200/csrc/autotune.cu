@@ -57,6 +57,7 @@ void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* 
         r.hpsi_bands_per_thread = hit->second[0];
         r.jacobi_sweeps_per_launch = hit->second[1];
         r.hpsi_variant = hit->second[2];
+        r.hpsi_zchunk = hit->second[3];
         r.cached = 1;
         if (rep) *rep = r;
         return;
@@ -121,6 +122,27 @@ void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* 
     ctx->hpsi_bands_per_thread = 1;
     r.hpsi_prefetch_ms = time_ms(ctx, ev, 3, [&] { apply_hamiltonian(ctx, g, V, psi, hpsi, tb, N); });
     if (r.hpsi_prefetch_ms < best) best = r.hpsi_prefetch_ms, best_bpt = 1, best_var = 3;
+    // the march length per block of the chosen register march (the auto choice is zc = 0)
+    int best_zc = 0;
+    if (best_var == 0 || best_var == 3) {
+        const int keep_zc = ctx->hpsi_zchunk;
+        ctx->hpsi_variant = best_var;
+        ctx->hpsi_bands_per_thread = best_bpt;
+        const int zcs[5] = {16, 32, 64, 96, 192};
+        for (int i = 0; i < 5; ++i) {
+            if (zcs[i] > g.nz) {
+                r.hpsi_zchunk_ms[i] = -1.0;
+                continue;
+            }
+            ctx->hpsi_zchunk = zcs[i];
+            r.hpsi_zchunk_ms[i] = time_ms(ctx, ev, 3, [&] { apply_hamiltonian(ctx, g, V, psi, hpsi, tb, N); });
+            if (r.hpsi_zchunk_ms[i] < best) best = r.hpsi_zchunk_ms[i], best_zc = zcs[i];
+        }
+        ctx->hpsi_zchunk = keep_zc;
+    } else {
+        for (double& v : r.hpsi_zchunk_ms) v = -1.0;
+    }
+    r.hpsi_zchunk = best_zc;
     ctx->hpsi_variant = 0;
     r.hpsi_bands_per_thread = best_bpt;
     r.hpsi_variant = best_var;
@@ -142,7 +164,7 @@ void autotune(dft_context* ctx, const Grid& g, int nbands, dft_autotune_report* 
     }
     r.jacobi_sweeps_per_launch = best_spl;
     sync(ctx);
-    ctx->tuned[key] = {best_bpt, best_spl, best_var};
+    ctx->tuned[key] = {best_bpt, best_spl, best_var, best_zc};
     if (rep) *rep = r;
 }
 

@@ -130,8 +130,9 @@ struct dft_context {
     long long grid_barrier_poll_limit = 0;  // persistent Jacobi barrier polls before giving up (0 = 2^24)
     // autotuner choices per grid (nx, ny, nz) -> {H psi bands per thread, Jacobi sweeps per launch},
     // used where the corresponding knob is 0 (auto)
-    // {H psi bands per thread (or per block for the TMA ring), Jacobi sweeps per launch, H psi variant}
-    std::map<std::array<long long, 3>, std::array<int, 3>> tuned;
+    // {H psi bands per thread (or per block for the TMA ring), Jacobi sweeps per launch, H psi
+    // variant, H psi z-march length (0 = auto)}
+    std::map<std::array<long long, 3>, std::array<int, 4>> tuned;
     int multigrid_graphs = 1;                 // replay captured multigrid cycles (1) or launch directly (0)
     std::map<MGGraphKey, MGGraph> mg_graphs;  // the captured cycles
     int radial_pivot_exp = -14;        // radial inverse iteration: |pivot| < 10^exp is singular

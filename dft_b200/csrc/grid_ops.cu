@@ -679,8 +679,9 @@ void apply_hamiltonian(dft_context* ctx, const Grid& g, const double* V, const d
     const int groups = (nbands + nbt - 1) / nbt;
     // z-chunk: the "hpsi_zchunk" key (points per block's march), else enough blocks to fill the
     // machine a few times over
-    const int zc = ctx->hpsi_zchunk > 0 ? std::min(ctx->hpsi_zchunk, g.nz)
-                                        : pick_zchunk(g, (long long)bx * by, groups, ctx->num_sms);
+    int zset = ctx->hpsi_zchunk;
+    if (zset == 0 && tuned != ctx->tuned.end()) zset = tuned->second[3];
+    const int zc = zset > 0 ? std::min(zset, g.nz) : pick_zchunk(g, (long long)bx * by, groups, ctx->num_sms);
     const int nzc = (g.nz + zc - 1) / zc;
     // gridDim.z limit is 65535: split the band block if needed
     const int max_groups = std::max(1, 65535 / nzc);

@@ -134,6 +134,8 @@ typedef struct {
                                       3 = the prefetching single-band march */
     double hpsi_tma_ms[4];         /* TMA plane ring with 1, 2, 4, 8 bands per block (-1: not eligible) */
     double hpsi_prefetch_ms;       /* the prefetching single-band march */
+    int hpsi_zchunk;               /* chosen z-march length per block of the register march (0 = auto) */
+    double hpsi_zchunk_ms[5];      /* the chosen register march with 16, 32, 64, 96, 192 planes per block */
 } dft_autotune_report;
 dft_status_t dft_autotune(dft_context* ctx, const dft_grid* g, int nbands, dft_autotune_report* report);
 /* The cudaStream_t the context launches on, as an opaque handle (for event timing). */

@@ -15,8 +15,11 @@ def test_autotune_picks_fastest_and_remembers(engine):
     r = engine.autotune(g, 6)
     print(r)
     assert not r["cached"]
-    times = [v for v in list(r["hpsi_ms"]) + list(r["hpsi_tma_ms"]) + [r["hpsi_prefetch_ms"]] if v >= 0]
-    if r["hpsi_variant"] == 3:
+    times = [v for v in list(r["hpsi_ms"]) + list(r["hpsi_tma_ms"]) + [r["hpsi_prefetch_ms"]]
+             + list(r["hpsi_zchunk_ms"]) if v >= 0]
+    if r["hpsi_zchunk"] > 0:
+        chosen = r["hpsi_zchunk_ms"][[16, 32, 64, 96, 192].index(r["hpsi_zchunk"])]
+    elif r["hpsi_variant"] == 3:
         chosen = r["hpsi_prefetch_ms"]
     elif r["hpsi_variant"] == 2:
         chosen = r["hpsi_tma_ms"][[1, 2, 4, 8].index(r["hpsi_bands_per_thread"])]
