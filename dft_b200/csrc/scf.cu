@@ -163,8 +163,17 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
     DevBuf mrho(ctx, monopole ? (size_t)N : 0), mvc(ctx, monopole ? (size_t)N : 0), mvp0(ctx, monopole ? (size_t)N : 0),
         mvp1(ctx, monopole ? (size_t)N : 0);
     int last_cycles = 0;  // multigrid cycles of the last solve
+    // Jacobi spectral radius of the grid: a max|dV| stop at tol leaves ~tol / (1 - rho) of error
+    const double rho_j = (g.ix2 * std::cos(3.14159265358979323846 / (g.nx - 1)) +
+                          g.iy2 * std::cos(3.14159265358979323846 / (g.ny - 1)) +
+                          g.iz2 * std::cos(3.14159265358979323846 / (g.nz - 1))) /
+                         (g.ix2 + g.iy2 + g.iz2);
+    const double fixed_scale = std::max(1.0 - rho_j, 1e-6);
+    if (o.poisson_fixed_point != 0 && o.poisson_fixed_point != 1)
+        fail(DFT_INVALID_ARGUMENT, "unknown poisson_fixed_point %d", o.poisson_fixed_point);
     auto poisson = [&](const double* d_in, double* v_out, bool have_prev, double tol = -1.0) {
-        const double ptol = tol > 0.0 ? tol : o.poisson_tol;
+        // multigrid target: half the Jacobi stop, scaled by 1 - rho with poisson_fixed_point
+        const double ptol = tol > 0.0 ? tol : o.poisson_tol * (o.poisson_fixed_point ? fixed_scale : 1.0);
         last_cycles = 0;
         const double* d = d_in;
         double* v = v_out;
@@ -202,7 +211,9 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             poisson_start(ctx, net, g, d, vstart.p, 0, nullptr);
             start = vstart.p;
         }
-        const JacobiResult r = hartree(ctx, g, d, v, ptol, o.poisson_max_sweeps, start, monopole);
+        // the Jacobi stop: the given tolerance, else the caller's (its rule is unchanged)
+        const JacobiResult r = hartree(ctx, g, d, v, tol > 0.0 ? tol : o.poisson_tol, o.poisson_max_sweeps, start,
+                                       monopole);
         if (monopole) add_into(ctx, N, v, mvc.p, v_out);
         return r;
     };
@@ -672,11 +683,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         // V_H(n_out): with multigrid starts the last V_H(n_out) is taken on to the Jacobi fixed
         // point (the max|dV| rule scaled by 1 - rho_Jacobi, a few cycles from the potential at
         // hand) before E_H and E_tot are reported.  The density is unchanged.
-        const double pi = 3.14159265358979323846;
-        const double rj = (g.ix2 * std::cos(pi / (g.nx - 1)) + g.iy2 * std::cos(pi / (g.ny - 1)) +
-                           g.iz2 * std::cos(pi / (g.nz - 1))) /
-                          (g.ix2 + g.iy2 + g.iz2);
-        poisson(orho.p, ovh.p, true, o.poisson_tol * std::max(1.0 - rj, 1e-6));
+        poisson(orho.p, ovh.p, true, o.poisson_tol * fixed_scale);
         const double eh = 0.5 * dot(ctx, N, orho.p, ovh.p) * g.dV;
         E[5] += eh - E[2];
         E[2] = eh;

@@ -343,6 +343,11 @@ typedef struct {
                                 2: as 1, and each V_H(n_out) solve from V_H(n_in) plus the previous
                                 iteration's V_H(n_out) - V_H(n_in).  The stop rule is unchanged;
                                 only the cycles/sweeps to reach it drop */
+    int poisson_fixed_point; /* 1: with DFT_POISSON_MULTIGRID the cycles of every solve go on until the
+                                next Jacobi update is below tol (1 - rho_Jacobi) / 2, so each V_H is
+                                at the Jacobi fixed point to ~tol instead of tol / (1 - rho) (the
+                                eigenvalues are first order in that error); the Jacobi stop rule
+                                that follows is unchanged.  0 (default): cycles to tol / 2 */
 } dft_scf_opts;
 
 /* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)
