@@ -508,11 +508,6 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         t0 = Clock::now();
         EigOpts ek = eo;
         if (o.adaptive_eig_tol && std::isfinite(prevD)) ek.tol = std::max(eo.tol, std::min(1e-3, 0.1 * prevD));
-        // the |dE| / eigenvalue stop may end the SCF only after orbitals solved to the full
-        // tolerance: with a looser one the iterates can settle (H2O 64^3 with tensor-core
-        // products: |dE| and the eigenvalue changes below 1e-7 while E_tot was 1.2e-6 Ha and the
-        // eigenvalues 1.8e-6 Ha from the fixed point)
-        const bool full_tol = ek.tol <= eo.tol;
         // the first iteration of the atomic start begins from the atomic orbitals (or, with
         // none, from the reference's seeds); later ones from the previous orbitals
         const bool first_atoms = atoms_start && it == 1;
@@ -657,8 +652,7 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             }
         }
         if (converged) break;
-        if (o.stop_abs_de > 0.0 && full_tol && dE < o.stop_abs_de && (o.stop_abs_deig <= 0.0 || deig < o.stop_abs_deig))
-            break;
+        if (o.stop_abs_de > 0.0 && dE < o.stop_abs_de && (o.stop_abs_deig <= 0.0 || deig < o.stop_abs_deig)) break;
         // adaptive mixing with the pre-update factor applied (:447-484)
         if (std::isfinite(prevD)) {
             if (effd > prevD * 1.05) mixing = std::max(0.10, mixing * 0.75);

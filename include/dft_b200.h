@@ -297,9 +297,7 @@ typedef struct {
     double energy_tol;       /* 1e-11 (DFTConstants.h:16) */
     double density_tol;      /* 1e-9  (DFTConstants.h:15) */
     double ks_tol;           /* 1e-7  (DFTConstants.h:17) */
-    double stop_abs_de;      /* > 0: also stop as soon as |dE| < stop_abs_de (time-to-|dE| metric),
-                                after an iteration whose eigensolve ran at the full eig.tol (with
-                                adaptive_eig_tol a looser one does not end the SCF) */
+    double stop_abs_de;      /* > 0: also stop as soon as |dE| < stop_abs_de (time-to-|dE| metric) */
     double poisson_tol;      /* 1e-8  (HartreePotentialMolecule.cpp:15) */
     long poisson_max_sweeps; /* 10000 (HartreePotentialMolecule.cpp:14) */
     int extra_bands;         /* unoccupied buffer bands per spin in the block eigensolver */
