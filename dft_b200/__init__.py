@@ -50,7 +50,7 @@ class dft_scf_opts(C.Structure):
                 ("stop_abs_deig", C.c_double), ("log_path", C.c_char_p), ("autotune", C.c_int),
                 ("initial_density", C.c_int),
                 ("hartree_boundary", C.c_int), ("poisson_predict", C.c_int),
-                ("poisson_fixed_point", C.c_int)]
+                ("poisson_fixed_point", C.c_int), ("stop_abs_drho", C.c_double)]
 
 
 class dft_autotune_report(C.Structure):

@@ -652,7 +652,9 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
             }
         }
         if (converged) break;
-        if (o.stop_abs_de > 0.0 && dE < o.stop_abs_de && (o.stop_abs_deig <= 0.0 || deig < o.stop_abs_deig)) break;
+        if (o.stop_abs_de > 0.0 && dE < o.stop_abs_de && (o.stop_abs_deig <= 0.0 || deig < o.stop_abs_deig) &&
+            (o.stop_abs_drho <= 0.0 || effd < o.stop_abs_drho))
+            break;
         // adaptive mixing with the pre-update factor applied (:447-484)
         if (std::isfinite(prevD)) {
             if (effd > prevD * 1.05) mixing = std::max(0.10, mixing * 0.75);

@@ -348,6 +348,10 @@ typedef struct {
                                 at the Jacobi fixed point to ~tol instead of tol / (1 - rho) (the
                                 eigenvalues are first order in that error); the Jacobi stop rule
                                 that follows is unchanged.  0 (default): cycles to tol / 2 */
+    double stop_abs_drho;    /* > 0: the stop_abs_de stop also needs the density difference below this.
+                                The reported energy is first order in n_out - n_in: on H2O 64^3 a Pulay
+                                plateau at dRho ~7e-7 kept |dE| and the eigenvalue changes below 1e-7
+                                while E_tot was 1.2e-6 Ha from the fixed point */
 } dft_scf_opts;
 
 /* Per-iteration record: the reference's iteration table (MolecularSCFHelpers.cpp:264-352)

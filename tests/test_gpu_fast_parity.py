@@ -3,7 +3,8 @@
 The fast configuration (multigrid Poisson starts taken to the Jacobi fixed point, the Hartree
 start from the mixer, mixed-precision eigensolver with its multigrid preconditioner, Pulay
 mixing, adaptive eigensolver tolerance, stop at
-|dE| < 1e-7 Ha with every occupied eigenvalue changed by < 1e-7 Ha, the bench's stop) must agree with the plain method run to its fixed point in FP64: the
+|dE| < 1e-7 Ha with every occupied eigenvalue changed by < 1e-7 Ha and dRho < 5e-7, the bench's
+stop) must agree with the plain method run to its fixed point in FP64: the
 reference's linear mixer and FP64 eigensolver, each Poisson solve stopped where its
 iterate is within ~1e-8 of the Jacobi fixed point (the reference's max|dV| < 1e-8 rule
 scaled by 1 - rho_Jacobi; the multigrid start only shortens the way there), SCF to
@@ -50,7 +51,8 @@ def test_fast_configuration_matches_fp64_oracle(engine, name):
                                          poisson_start=dft_b200.POISSON_MULTIGRID,
                                          poisson_tol=_tight_tol(w["n"], w["bounds"]), poisson_max_sweeps=400000,
                                          eig_preconditioner=-1)
-    fast = dft_b200.default_scf_options(stop_abs_de=1e-7, stop_abs_deig=1e-7, extra_bands=w["extra_bands"],
+    fast = dft_b200.default_scf_options(stop_abs_de=1e-7, stop_abs_deig=1e-7, stop_abs_drho=5e-7,
+                                        extra_bands=w["extra_bands"],
                                         poisson_start=dft_b200.POISSON_MULTIGRID, eig_mixed_precision=1,
                                         eig_preconditioner=-2, mixer=1, adaptive_eig_tol=1, poisson_predict=1,
                                         poisson_fixed_point=1)
