@@ -62,7 +62,12 @@ for _w in WORKLOADS.values():
 WORKLOADS["cluster20"]["fast_options"] = {"kerker_q0": 0.8, "initial_density": 1}
 # H2 48^3: the superposed-atoms start (radial atoms kept per context) saves the first
 # eigensolve in the bare V_ext: 30.5 instead of 35.5 ms per SCF
-WORKLOADS["h2_48"]["fast_options"] = {"initial_density": 1}
+WORKLOADS["h2_48"]["fast_options"] = {"initial_density": 1,
+                                      # the adaptive eigensolver tolerance follows dRho down to 1e-9
+                                      # instead of stopping at 1e-7: with the density condition of the
+                                      # stop, 13 SCF iterations instead of 20.  On (H2O)_2 192^3 the
+                                      # 1e-9 floor ended 1.2e-6 Ha from the fixed point (6e-7 with 1e-7)
+                                      "eig_tol": 1e-9}
 # the largest cluster that converges under the reference's boundary on the 192^3 grid (the
 # 20-atom draw and larger water clusters bind box-wall states there): (H2O)_2, Pulay with a
 # step of 0.5 and 16 entries of history (0.2 / 8 do not reach the stop within 100 iterations)
@@ -199,10 +204,7 @@ def scf_options(w, fast=False, net=None, extra=None):
     kw = dict(stop_abs_de=STOP_DE, stop_abs_deig=STOP_DEIG, stop_abs_drho=STOP_DRHO, extra_bands=w["extra_bands"],
               poisson_start=dft_b200.POISSON_MULTIGRID,
               eig_mixed_precision=1, eig_preconditioner=-2, mixer=1, adaptive_eig_tol=1, poisson_predict=1,
-              autotune=1,
-              # the adaptive tolerance follows dRho down to 1e-9 instead of stopping at 1e-7: with the
-              # density condition of the stop, H2 48^3 then takes 13 SCF iterations instead of 20
-              eig_tol=1e-9)
+              autotune=1)
     kw.update(w.get("fast_options", {}))
     kw.update(extra or {})
     o = dft_b200.default_scf_options(**kw)
