@@ -680,7 +680,9 @@ void scf_molecule(dft_context* ctx, const dft_grid* grid, int nnuc, const int* Z
         prevD = effd;
         prevE = E[5];
     }
-    if (pstart == DFT_POISSON_MULTIGRID && it >= 1) {
+    // (skipped when the caller's own Jacobi stop is already that tight: a target below 1e-13
+    // is rounding noise and would only run the sweep cap)
+    if (pstart == DFT_POISSON_MULTIGRID && it >= 1 && o.poisson_tol * fixed_scale >= 1e-13) {
         // The reported Hartree energy enters the total at first order in the error of
         // V_H(n_out): with multigrid starts the last V_H(n_out) is taken on to the Jacobi fixed
         // point (the max|dV| rule scaled by 1 - rho_Jacobi, a few cycles from the potential at
