@@ -146,6 +146,11 @@ _SIGS = {
     "dft_hartree_monopole_dev": ([_P, C.POINTER(dft_grid), _P, _P, C.c_double, C.c_long, C.POINTER(C.c_long), _D],
                                  C.c_int),
     "dft_hartree_energy_dev": ([_P, C.POINTER(dft_grid), _P, _P, _D], C.c_int),
+    "dft_zslab_jacobi_init_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, C.c_double, _P, _P], C.c_int),
+    "dft_zslab_jacobi_sweeps_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P,
+                                     C.c_int, _P], C.c_int),
+    "dft_zslab_hamiltonian_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, _P, _P, _P, C.c_int, C.c_long],
+                                  C.c_int),
     "dft_xc_dev": ([_P, C.POINTER(dft_grid), C.c_int, _P, _P, _P, _P, _D], C.c_int),
     "dft_xc_evaluate_dev": ([_P, C.c_int, C.c_long, _P, _P, _P, _P, _P], C.c_int),
     "dft_spin_density_dev": ([_P, C.c_long, _P, C.c_int, C.c_long, _D, _P], C.c_int),

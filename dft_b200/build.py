@@ -38,6 +38,7 @@ SOURCES = {
     "precond_mg.cu": [],
     "atomic_start.cu": [],
     "autotune.cu": [],
+    "zslab.cu": [],
     "eigh.cpp": ["-Xcompiler", "-O3"],
 }
 

@@ -280,6 +280,38 @@ dft_status_t dft_hartree_noalloc_dev(dft_context* ctx, const dft_grid* g, const 
     });
 }
 
+dft_status_t dft_zslab_jacobi_init_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, double Q,
+                                       const double* guess, double* v) {
+    return guard(ctx, [&] {
+        NEED(ctx && v, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::zslab_jacobi_init(ctx, G, z_lo, z_hi, Q, guess, v);
+        dftb::sync(ctx);
+    });
+}
+
+dft_status_t dft_zslab_jacobi_sweeps_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo,
+                                         int own_hi, const double* rho, double* v, double* tmp, int sweeps,
+                                         double* diffs) {
+    return guard(ctx, [&] {
+        NEED(ctx && rho && v && tmp && (diffs || sweeps == 0), "NULL argument");
+        NEED(v != tmp && rho != v && rho != tmp, "rho, v and tmp must be distinct");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::zslab_jacobi_sweeps(ctx, G, z_lo, z_hi, own_lo, own_hi, rho, v, tmp, sweeps, diffs);
+        dftb::sync(ctx);
+    });
+}
+
+dft_status_t dft_zslab_hamiltonian_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, const double* V,
+                                       const double* psi, double* hpsi, int nbands, long ld) {
+    return guard(ctx, [&] {
+        NEED(ctx && V && psi && hpsi, "NULL argument");
+        NEED(nbands >= 0, "nbands must be >= 0");
+        const dftb::Grid G = dftb::make_grid(g);
+        dftb::zslab_hamiltonian(ctx, G, z_lo, z_hi, V, psi, hpsi, nbands, ld);
+    });
+}
+
 dft_status_t dft_hartree_monopole_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
                                       long max_sweeps, long* sweeps_out, double* last_diff_out) {
     return guard(ctx, [&] {

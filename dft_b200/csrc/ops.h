@@ -40,6 +40,19 @@ double* noalloc_scratch(int device);
 JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho, double* vh, double tol,
                              long max_sweeps);
 
+// Z-slab decomposition (zslab.cu).  A slab holds the global planes [z_lo, z_hi) of grid g.
+// zslab_jacobi_init: the reference's face values (Q: total charge, used only on faces whose
+// last node misses the bound) and a cold or `guess` interior.  zslab_jacobi_sweeps: `sweeps`
+// Jacobi sweeps of the slab's interior planes (outermost planes fixed), result in v (tmp:
+// scratch of the slab's size), diffs[t] = max|dV| of sweep t over the owned planes
+// [own_lo, own_hi) (global indices).  zslab_hamiltonian: H psi of the slab (owned planes exact
+// with one halo plane per side).
+void zslab_jacobi_init(dft_context* ctx, const Grid& g, int z_lo, int z_hi, double Q, const double* guess, double* v);
+void zslab_jacobi_sweeps(dft_context* ctx, const Grid& g, int z_lo, int z_hi, int own_lo, int own_hi,
+                         const double* rho, double* v, double* tmp, int sweeps, double* diffs);
+void zslab_hamiltonian(dft_context* ctx, const Grid& g, int z_lo, int z_hi, const double* V, const double* psi,
+                       double* hpsi, int nbands, long long ld);
+
 // Monopole boundary option (grid_ops.cu): vc = Q erf(|r|/(sqrt 2 s))/|r| (Q = sum rho dV, returned)
 // and rho_prime = rho + L_h vc / (4 pi) on the interior, so that V_H = V' + vc with V' the
 // zero-face solution for rho_prime has the face values Q/|r|.  monopole_width: s for grid g.

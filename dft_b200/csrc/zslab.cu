@@ -1,0 +1,178 @@
+// Z-slab domain decomposition of the 3D grid: the pieces one rank runs on its own slab.
+//
+// A slab holds the global planes [z_lo, z_hi) of the x-fastest layout, i.e. its own planes
+// plus halo planes copied from the neighbouring slabs.  The host driver (dft_b200/zslab.py)
+// exchanges the halos and reduces the stop measures over ranks; nothing here waits on another
+// rank or another kernel.
+//
+// Jacobi (reference HartreePotentialMolecule.cpp:207-321): a slab with T halo planes on each
+// side can run T sweeps between exchanges.  Every sweep updates all interior planes of the
+// slab; the outermost planes stay fixed, so after s <= T sweeps the planes at distance >= s
+// from the slab's edges -- every owned plane -- hold exactly the values of the single-domain
+// solve.  The stop measure max|V' - V| is folded only over owned planes and kept per sweep, so
+// the driver can reduce it over ranks and find the sweep at which the single-domain loop stops.
+// Same arithmetic and operation order as jacobi_sweep_kernel: bit-identical values.
+//
+// H psi (reference KohnShamHamiltonianMolecule.cpp:78-177): with one halo plane per side the
+// owned planes of a slab see the same six neighbours as on the whole grid, and the grid's own
+// faces (where no neighbour exists) are slab faces too, so apply_hamiltonian on the slab's
+// plane count gives bit-identical owned planes.
+#include <algorithm>
+#include <cmath>
+
+#include "ops.h"
+#include "xc_device.cuh"
+
+namespace dftb {
+namespace {
+
+constexpr int SB_X = 32, SB_Y = 8;
+
+// Slab initial state: face values of the global grid (the reference's boundary rule,
+// HartreePotentialMolecule.cpp:37-95, as in jacobi_init_kernel) on the slab's part of the six
+// faces; the interior is 0 (cold start) or the interior of `guess` (same slab layout).
+__global__ void slab_init_kernel(Grid g, int z_lo, long long n_local, double Q, double* __restrict__ v,
+                                 const double* __restrict__ guess) {
+    const long long sxy = (long long)g.nx * g.ny;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n_local;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % g.nx);
+        const int j = (int)((p / g.nx) % g.ny);
+        const int k = z_lo + (int)(p / sxy);
+        const bool face = i == 0 || i + 1 == g.nx || j == 0 || j + 1 == g.ny || k == 0 || k + 1 == g.nz;
+        double val = 0.0;
+        if (!face && guess) val = guess[p];
+        if (face) {
+            const double x = __dadd_rn(g.xmin, __dmul_rn((double)i, g.dx));
+            const double y = __dadd_rn(g.ymin, __dmul_rn((double)j, g.dy));
+            const double z = __dadd_rn(g.zmin, __dmul_rn((double)k, g.dz));
+            const double d[6] = {fabs(x - g.xmin), fabs(x - g.xmax), fabs(y - g.ymin),
+                                 fabs(y - g.ymax), fabs(z - g.zmin), fabs(z - g.zmax)};
+            double m2 = INFINITY;
+            for (int q = 0; q < 6; ++q) m2 = fmin(m2, __dmul_rn(d[q], d[q]));
+            if (m2 > 0.0) {
+                const double r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+                if (r > 0.0) val = Q / r;
+            }
+        }
+        v[p] = val;
+    }
+}
+
+// One Jacobi sweep over the slab's interior planes 1..nzl-2 (local indices), x and y interior
+// as on the whole grid.  max|V' - V| over the local planes [own_lo, own_hi) goes into
+// *diff_bits (a non-negative double orders like its bit pattern, so atomicMax on the bits is
+// the maximum; the caller zeroes the word).
+__global__ void __launch_bounds__(SB_X* SB_Y) slab_sweep_kernel(int nx, int ny, int nzl, double ix2, double iy2,
+                                                                double iz2, double den,
+                                                                const double* __restrict__ rho,
+                                                                const double* __restrict__ cur,
+                                                                double* __restrict__ nxt, int own_lo, int own_hi,
+                                                                int zchunk, unsigned long long* diff_bits) {
+    __shared__ double sh[SB_X * SB_Y / 32];
+    const double c4pi = 4.0 * xcf::PI;
+    const int i = blockIdx.x * SB_X + threadIdx.x;
+    const int j = blockIdx.y * SB_Y + threadIdx.y;
+    double md = 0.0;
+    if (i >= 1 && i + 1 < nx && j >= 1 && j + 1 < ny) {
+        const int sxy = nx * ny;
+        const int kb = max(1, (int)blockIdx.z * zchunk);
+        const int ke = min(nzl - 1, (int)(blockIdx.z + 1) * zchunk);
+        if (kb < ke) {
+            int idx = kb * sxy + j * nx + i;
+            double below = __ldg(cur + idx - sxy);
+            double c = __ldg(cur + idx);
+#pragma unroll 4
+            for (int k = kb; k < ke; ++k, idx += sxy) {
+                const double above = __ldg(cur + idx + sxy);
+                const double sx = __dadd_rn(__ldg(cur + idx - 1), __ldg(cur + idx + 1));
+                const double sy = __dadd_rn(__ldg(cur + idx - nx), __ldg(cur + idx + nx));
+                const double sz = __dadd_rn(below, above);
+                double acc = __dadd_rn(__dmul_rn(ix2, sx), __dmul_rn(iy2, sy));
+                acc = __dadd_rn(acc, __dmul_rn(iz2, sz));
+                acc = __dadd_rn(acc, __dmul_rn(c4pi, __ldg(rho + idx)));
+                const double v = __ddiv_rn(acc, den);
+                nxt[idx] = v;
+                if (k >= own_lo && k < own_hi) md = fmax(md, fabs(v - c));
+                below = c;
+                c = above;
+            }
+        }
+    }
+    const int tid = threadIdx.y * SB_X + threadIdx.x;
+    md = warp_max(md);
+    if ((tid & 31) == 0) sh[tid >> 5] = md;
+    __syncthreads();
+    if (tid == 0) {
+        double m = sh[0];
+        for (int w = 1; w < SB_X * SB_Y / 32; ++w) m = fmax(m, sh[w]);
+        if (m > 0.0) atomicMax(diff_bits, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// The slab as a Grid: the global spacing and bounds (so every constant is the whole grid's),
+// the slab's plane count.
+Grid slab_grid(const Grid& g, int z_lo, int z_hi) {
+    Grid s = g;
+    s.nz = z_hi - z_lo;
+    s.N = (long long)g.nx * g.ny * s.nz;
+    return s;
+}
+
+void check_slab(const Grid& g, int z_lo, int z_hi) {
+    if (z_lo < 0 || z_hi > g.nz || z_hi <= z_lo) fail(DFT_INVALID_ARGUMENT, "slab planes must satisfy 0 <= z_lo < z_hi <= nz");
+}
+
+}  // namespace
+
+void zslab_jacobi_init(dft_context* ctx, const Grid& g, int z_lo, int z_hi, double Q, const double* guess, double* v) {
+    check_slab(g, z_lo, z_hi);
+    const long long n = (long long)g.nx * g.ny * (z_hi - z_lo);
+    const int blocks = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)ctx->num_sms * 8));
+    slab_init_kernel<<<blocks, 256, 0, ctx->stream>>>(g, z_lo, n, Q, v, guess);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+}
+
+void zslab_jacobi_sweeps(dft_context* ctx, const Grid& g, int z_lo, int z_hi, int own_lo, int own_hi,
+                         const double* rho, double* v, double* tmp, int sweeps, double* diffs) {
+    check_slab(g, z_lo, z_hi);
+    if (own_lo > own_hi || own_lo < z_lo || own_hi > z_hi)
+        fail(DFT_INVALID_ARGUMENT, "owned planes must lie inside the slab");
+    // an owned plane that the whole grid updates must be one the slab updates
+    if ((own_lo < own_hi) && ((own_lo < z_lo + 1 && own_lo != 0) || (own_hi > z_hi - 1 && own_hi != g.nz)))
+        fail(DFT_INVALID_ARGUMENT, "an owned interior plane lies on the slab's edge (no halo plane beyond it)");
+    if (sweeps < 0) fail(DFT_INVALID_ARGUMENT, "sweeps must be >= 0");
+    if (sweeps == 0) return;
+    const Grid s = slab_grid(g, z_lo, z_hi);
+    DFT_CUDA(cudaMemsetAsync(diffs, 0, sizeof(double) * (size_t)sweeps, ctx->stream));
+    // the fixed points (faces, outermost halo planes) must be present in both buffers
+    DFT_CUDA(cudaMemcpyAsync(tmp, v, sizeof(double) * (size_t)s.N, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (s.nx < 3 || s.ny < 3 || s.nz < 3) return;  // no interior point in the slab: every diff stays 0
+    const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
+    const int bx = (s.nx + SB_X - 1) / SB_X, by = (s.ny + SB_Y - 1) / SB_Y;
+    int zc = 32;
+    while (zc > 4 && (long long)bx * by * ((s.nz + zc - 1) / zc) < 2LL * ctx->num_sms) zc >>= 1;
+    const dim3 grid(bx, by, (s.nz + zc - 1) / zc), block(SB_X, SB_Y);
+    const int lo = own_lo - z_lo, hi = own_hi - z_lo;
+    unsigned long long* bits = reinterpret_cast<unsigned long long*>(diffs);
+    for (int t = 0; t < sweeps; ++t) {
+        const double* cur = (t & 1) ? tmp : v;
+        double* nxt = (t & 1) ? v : tmp;
+        slab_sweep_kernel<<<grid, block, 0, ctx->stream>>>(s.nx, s.ny, s.nz, g.ix2, g.iy2, g.iz2, den, rho, cur, nxt,
+                                                           lo, hi, zc, bits + t);
+    }
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx, sweeps);
+    if (sweeps & 1) DFT_CUDA(cudaMemcpyAsync(v, tmp, sizeof(double) * (size_t)s.N, cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+void zslab_hamiltonian(dft_context* ctx, const Grid& g, int z_lo, int z_hi, const double* V, const double* psi,
+                       double* hpsi, int nbands, long long ld) {
+    check_slab(g, z_lo, z_hi);
+    const Grid s = slab_grid(g, z_lo, z_hi);
+    if (ld < s.N) fail(DFT_INVALID_ARGUMENT, "ld must be >= nx*ny*(z_hi - z_lo)");
+    apply_hamiltonian(ctx, s, V, psi, hpsi, nbands, ld);
+}
+
+}  // namespace dftb

@@ -196,6 +196,37 @@ dft_status_t dft_hartree_noalloc_dev(dft_context* ctx, const dft_grid* g, const 
 dft_status_t dft_hartree_monopole_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
                                       long max_sweeps, long* sweeps_out, double* last_diff_out);
 
+/* ---- z-slab decomposition (one rank's slab; the halo exchange and the reductions over ranks
+ * are the caller's) ---------------------------------------------------------------------
+ * A slab is the global planes [z_lo, z_hi) of grid g (x fastest, (k - z_lo)*nx*ny + j*nx + i),
+ * holding the rank's own planes plus halo planes copied from its neighbours.  The reference
+ * has no decomposition; these split its functions over ranks with bit-identical results. */
+
+/* Initial state of the Jacobi solve of dft_hartree_dev on a slab (reference
+ * HartreePotentialMolecule.cpp:37-95, :152-155): the reference's face values where the slab
+ * meets a face of g, Q/|r| with Q the total charge (used only on faces whose last node misses
+ * the bound; 0 on every grid whose nodes land on the bounds), interior 0, or the interior of
+ * guess (device, same slab layout) when guess is not NULL.  v: device, nx*ny*(z_hi - z_lo). */
+dft_status_t dft_zslab_jacobi_init_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, double Q,
+                                       const double* guess, double* v);
+
+/* `sweeps` Jacobi sweeps of dft_hartree_dev's loop (reference HartreePotentialMolecule.cpp:
+ * 207-321) on a slab: every plane of the slab except its first and last is updated, so with
+ * T halo planes per side the rank's own planes are exact for up to T sweeps.  diffs (device,
+ * `sweeps` doubles): max|dV| of each sweep over the owned planes [own_lo, own_hi) (global
+ * indices; every owned plane that g's interior contains must be an inner plane of the slab).
+ * The maximum of diffs[t] over ranks is the single-domain loop's max|dV| of that sweep.
+ * rho, v, tmp: device, the slab's size; v holds the result, tmp is scratch.  Synchronises. */
+dft_status_t dft_zslab_jacobi_sweeps_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo,
+                                         int own_hi, const double* rho, double* v, double* tmp, int sweeps,
+                                         double* diffs);
+
+/* dft_apply_hamiltonian_dev on a slab (reference KohnShamHamiltonianMolecule.cpp:78-177):
+ * with one halo plane per side (none at the faces of g) the owned planes of hpsi are
+ * bit-identical to the whole-grid result.  ld >= nx*ny*(z_hi - z_lo). */
+dft_status_t dft_zslab_hamiltonian_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, const double* V,
+                                       const double* psi, double* hpsi, int nbands, long ld);
+
 /* calculateHartreeEnergy (reference HartreePotentialMolecule.cpp:326-379): 1/2 sum rho V dV. */
 dft_status_t dft_hartree_energy_dev(dft_context* ctx, const dft_grid* g, const double* rho, const double* vh,
                                     double* energy_out);

@@ -1,0 +1,85 @@
+"""Test double of dft_b200.zslab.CudaSlabOps: the slab kernels' arithmetic in numpy on CPU
+tensors, so that the z-slab driver's host logic (layouts, halo exchanges, reductions, the
+replayed stop) runs on gloo ranks without a GPU.  numpy float64 operations round to nearest
+without contraction, in the order written, which is the order of the CUDA kernels and of the
+oracle (oracle/dft_oracle.c: hpsi3, oracle_hartree_potential_ex).  Test infrastructure only."""
+import math
+
+import numpy as np
+
+
+def _spacing(grid):
+    return grid.getDx(), grid.getDy(), grid.getDz()
+
+
+class NumpySlabOps:
+    def jacobi_init(self, grid, z_lo, z_hi, Q, v, guess=None):
+        nx, ny, nz = grid.nx, grid.ny, grid.nz
+        dx, dy, dz = _spacing(grid)
+        xmin, xmax, ymin, ymax, zmin, zmax = grid.bounds
+        k = np.arange(z_lo, z_hi, dtype=np.int64)[:, None, None]
+        j = np.arange(ny, dtype=np.int64)[None, :, None]
+        i = np.arange(nx, dtype=np.int64)[None, None, :]
+        shape = (z_hi - z_lo, ny, nx)
+        x = np.broadcast_to(xmin + i.astype(np.float64) * dx, shape)
+        y = np.broadcast_to(ymin + j.astype(np.float64) * dy, shape)
+        z = np.broadcast_to(zmin + k.astype(np.float64) * dz, shape)
+        face = np.broadcast_to((i == 0) | (i == nx - 1) | (j == 0) | (j == ny - 1) | (k == 0) | (k == nz - 1),
+                               shape)
+        d = [np.abs(x - xmin), np.abs(x - xmax), np.abs(y - ymin), np.abs(y - ymax),
+             np.abs(z - zmin), np.abs(z - zmax)]
+        m2 = np.minimum.reduce([q * q for q in d])
+        r = np.sqrt(x * x + y * y + z * z)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            bval = np.where((m2 > 0.0) & (r > 0.0), Q / r, 0.0)
+        inner = guess.numpy().reshape(shape) if guess is not None else np.zeros(shape)
+        v.numpy().reshape(shape)[...] = np.where(face, bval, inner)
+
+    def jacobi_sweeps(self, grid, z_lo, z_hi, own_lo, own_hi, rho, v, tmp, sweeps, diffs):
+        nx, ny = grid.nx, grid.ny
+        nzl = z_hi - z_lo
+        dx, dy, dz = _spacing(grid)
+        ix, iy, iz = 1.0 / (dx * dx), 1.0 / (dy * dy), 1.0 / (dz * dz)
+        den = 2.0 * (ix + iy + iz)
+        c4pi = 4.0 * math.pi
+        a = v.numpy().reshape(nzl, ny, nx)
+        b = tmp.numpy().reshape(nzl, ny, nx)
+        src = c4pi * rho.numpy().reshape(nzl, ny, nx)[1:-1, 1:-1, 1:-1]
+        dv = diffs.numpy()
+        dv[:sweeps] = 0.0
+        b[...] = a
+        # owned planes that the slab updates, as rows of the interior block
+        lo, hi = max(own_lo - z_lo, 1) - 1, min(own_hi - z_lo, nzl - 1) - 1
+        cur, nxt = a, b
+        for t in range(sweeps):
+            if nx >= 3 and ny >= 3 and nzl >= 3:
+                c = cur[1:-1, 1:-1, 1:-1]
+                sx = cur[1:-1, 1:-1, :-2] + cur[1:-1, 1:-1, 2:]
+                sy = cur[1:-1, :-2, 1:-1] + cur[1:-1, 2:, 1:-1]
+                sz = cur[:-2, 1:-1, 1:-1] + cur[2:, 1:-1, 1:-1]
+                acc = ix * sx + iy * sy
+                acc = acc + iz * sz
+                acc = acc + src
+                new = acc / den
+                if hi > lo:
+                    dv[t] = np.abs(new[lo:hi] - c[lo:hi]).max()
+                nxt[1:-1, 1:-1, 1:-1] = new
+            cur, nxt = nxt, cur
+        if sweeps % 2:
+            a[...] = b
+
+    def hamiltonian(self, grid, z_lo, z_hi, V, psi, hpsi, nbands):
+        nx, ny = grid.nx, grid.ny
+        nzl = z_hi - z_lo
+        dx, dy, dz = _spacing(grid)
+        ix, iy, iz = 1.0 / (dx * dx), 1.0 / (dy * dy), 1.0 / (dz * dz)
+        P = psi.numpy().reshape(nbands, nzl, ny, nx)
+        W = V.numpy().reshape(1, nzl, ny, nx)
+        lap = (-2.0 * (ix + iy + iz)) * P
+        lap[..., 1:] = lap[..., 1:] + P[..., :-1] * ix
+        lap[..., :-1] = lap[..., :-1] + P[..., 1:] * ix
+        lap[..., 1:, :] = lap[..., 1:, :] + P[..., :-1, :] * iy
+        lap[..., :-1, :] = lap[..., :-1, :] + P[..., 1:, :] * iy
+        lap[:, 1:] = lap[:, 1:] + P[:, :-1] * iz
+        lap[:, :-1] = lap[:, :-1] + P[:, 1:] * iz
+        hpsi.numpy().reshape(nbands, nzl, ny, nx)[...] = -0.5 * lap + W * P
