@@ -147,7 +147,7 @@ _SIGS = {
                                  C.c_int),
     "dft_hartree_energy_dev": ([_P, C.POINTER(dft_grid), _P, _P, _D], C.c_int),
     "dft_zslab_jacobi_init_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, C.c_double, _P, _P], C.c_int),
-    "dft_zslab_jacobi_sweeps_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P,
+    "dft_zslab_jacobi_sweeps_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P,
                                      C.c_int, _P], C.c_int),
     "dft_zslab_hamiltonian_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, _P, _P, _P, C.c_int, C.c_long],
                                   C.c_int),

@@ -291,13 +291,14 @@ dft_status_t dft_zslab_jacobi_init_dev(dft_context* ctx, const dft_grid* g, int 
 }
 
 dft_status_t dft_zslab_jacobi_sweeps_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo,
-                                         int own_hi, const double* rho, double* v, double* tmp, int sweeps,
-                                         double* diffs) {
+                                         int own_hi, const double* rho, const double* v_in, double* v_out,
+                                         double* scratch, int sweeps, double* diffs) {
     return guard(ctx, [&] {
-        NEED(ctx && rho && v && tmp && (diffs || sweeps == 0), "NULL argument");
-        NEED(v != tmp && rho != v && rho != tmp, "rho, v and tmp must be distinct");
+        NEED(ctx && rho && v_in && v_out && scratch && (diffs || sweeps == 0), "NULL argument");
+        NEED(v_in != v_out && v_in != scratch && v_out != scratch && rho != v_in && rho != v_out && rho != scratch,
+             "rho, v_in, v_out and scratch must be distinct");
         const dftb::Grid G = dftb::make_grid(g);
-        dftb::zslab_jacobi_sweeps(ctx, G, z_lo, z_hi, own_lo, own_hi, rho, v, tmp, sweeps, diffs);
+        dftb::zslab_jacobi_sweeps(ctx, G, z_lo, z_hi, own_lo, own_hi, rho, v_in, v_out, scratch, sweeps, diffs);
         dftb::sync(ctx);
     });
 }

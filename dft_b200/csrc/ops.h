@@ -43,13 +43,14 @@ JacobiResult hartree_noalloc(dft_context* ctx, const Grid& g, const double* rho,
 // Z-slab decomposition (zslab.cu).  A slab holds the global planes [z_lo, z_hi) of grid g.
 // zslab_jacobi_init: the reference's face values (Q: total charge, used only on faces whose
 // last node misses the bound) and a cold or `guess` interior.  zslab_jacobi_sweeps: `sweeps`
-// Jacobi sweeps of the slab's interior planes (outermost planes fixed), result in v (tmp:
-// scratch of the slab's size), diffs[t] = max|dV| of sweep t over the owned planes
-// [own_lo, own_hi) (global indices).  zslab_hamiltonian: H psi of the slab (owned planes exact
-// with one halo plane per side).
+// Jacobi sweeps of the slab's interior planes (outermost planes fixed) from v_in (only read)
+// into v_out (scratch: a third buffer of the slab's size), diffs[t] = max|dV| of sweep t over
+// the owned planes [own_lo, own_hi) (global indices).  zslab_hamiltonian: H psi of the slab
+// (owned planes exact with one halo plane per side).
 void zslab_jacobi_init(dft_context* ctx, const Grid& g, int z_lo, int z_hi, double Q, const double* guess, double* v);
 void zslab_jacobi_sweeps(dft_context* ctx, const Grid& g, int z_lo, int z_hi, int own_lo, int own_hi,
-                         const double* rho, double* v, double* tmp, int sweeps, double* diffs);
+                         const double* rho, const double* v_in, double* v_out, double* scratch, int sweeps,
+                         double* diffs);
 void zslab_hamiltonian(dft_context* ctx, const Grid& g, int z_lo, int z_hi, const double* V, const double* psi,
                        double* hpsi, int nbands, long long ld);
 

@@ -11,7 +11,10 @@
 // from the slab's edges -- every owned plane -- hold exactly the values of the single-domain
 // solve.  The stop measure max|V' - V| is folded only over owned planes and kept per sweep, so
 // the driver can reduce it over ranks and find the sweep at which the single-domain loop stops.
-// Same arithmetic and operation order as jacobi_sweep_kernel: bit-identical values.
+// A block of sweeps reads its start and never writes it (the result goes to a second buffer,
+// through a third), so a block that overshoots the stop is replayed from the untouched start
+// without a snapshot copy.  Same arithmetic and operation order as jacobi_sweep_kernel:
+// bit-identical values.
 //
 // H psi (reference KohnShamHamiltonianMolecule.cpp:78-177): with one halo plane per side the
 // owned planes of a slab see the same six neighbours as on the whole grid, and the grid's own
@@ -110,6 +113,38 @@ __global__ void __launch_bounds__(SB_X* SB_Y) slab_sweep_kernel(int nx, int ny, 
     }
 }
 
+// Copies the points a sweep never writes -- the first and last plane of the slab and the x/y
+// faces of the planes between -- from src to both destinations (the shell, enumerated directly:
+// 2 nx ny + 2 nx (nzl-2) + 2 (ny-2) (nzl-2) points).  Needs nx, ny, nzl >= 3.
+__global__ void slab_shell_copy_kernel(int nx, int ny, int nzl, const double* __restrict__ src,
+                                       double* __restrict__ d0, double* __restrict__ d1) {
+    const long long sxy = (long long)nx * ny;
+    const long long nA = 2 * sxy;                          // planes 0 and nzl-1
+    const long long nB = 2LL * nx * (nzl - 2);             // rows j = 0, ny-1 of planes 1..nzl-2
+    const long long nC = 2LL * (ny - 2) * (nzl - 2);       // columns i = 0, nx-1 of rows 1..ny-2
+    const long long total = nA + nB + nC;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        long long p;
+        if (q < nA) {
+            p = q < sxy ? q : (long long)(nzl - 1) * sxy + (q - sxy);
+        } else if (q < nA + nB) {
+            const long long r = q - nA;
+            const long long k = 1 + r / (2LL * nx), rem = r % (2LL * nx);
+            const long long j = rem < nx ? 0 : ny - 1, i = rem < nx ? rem : rem - nx;
+            p = k * sxy + j * nx + i;
+        } else {
+            const long long r = q - nA - nB;
+            const long long k = 1 + r / (2LL * (ny - 2)), rem = r % (2LL * (ny - 2));
+            const long long j = 1 + (rem < ny - 2 ? rem : rem - (ny - 2)), i = rem < ny - 2 ? 0 : nx - 1;
+            p = k * sxy + j * nx + i;
+        }
+        const double v = src[p];
+        d0[p] = v;
+        d1[p] = v;
+    }
+}
+
 // The slab as a Grid: the global spacing and bounds (so every constant is the whole grid's),
 // the slab's plane count.
 Grid slab_grid(const Grid& g, int z_lo, int z_hi) {
@@ -135,7 +170,8 @@ void zslab_jacobi_init(dft_context* ctx, const Grid& g, int z_lo, int z_hi, doub
 }
 
 void zslab_jacobi_sweeps(dft_context* ctx, const Grid& g, int z_lo, int z_hi, int own_lo, int own_hi,
-                         const double* rho, double* v, double* tmp, int sweeps, double* diffs) {
+                         const double* rho, const double* v_in, double* v_out, double* scratch, int sweeps,
+                         double* diffs) {
     check_slab(g, z_lo, z_hi);
     if (own_lo > own_hi || own_lo < z_lo || own_hi > z_hi)
         fail(DFT_INVALID_ARGUMENT, "owned planes must lie inside the slab");
@@ -143,12 +179,20 @@ void zslab_jacobi_sweeps(dft_context* ctx, const Grid& g, int z_lo, int z_hi, in
     if ((own_lo < own_hi) && ((own_lo < z_lo + 1 && own_lo != 0) || (own_hi > z_hi - 1 && own_hi != g.nz)))
         fail(DFT_INVALID_ARGUMENT, "an owned interior plane lies on the slab's edge (no halo plane beyond it)");
     if (sweeps < 0) fail(DFT_INVALID_ARGUMENT, "sweeps must be >= 0");
-    if (sweeps == 0) return;
     const Grid s = slab_grid(g, z_lo, z_hi);
-    DFT_CUDA(cudaMemsetAsync(diffs, 0, sizeof(double) * (size_t)sweeps, ctx->stream));
-    // the fixed points (faces, outermost halo planes) must be present in both buffers
-    DFT_CUDA(cudaMemcpyAsync(tmp, v, sizeof(double) * (size_t)s.N, cudaMemcpyDeviceToDevice, ctx->stream));
-    if (s.nx < 3 || s.ny < 3 || s.nz < 3) return;  // no interior point in the slab: every diff stays 0
+    if (sweeps > 0) DFT_CUDA(cudaMemsetAsync(diffs, 0, sizeof(double) * (size_t)sweeps, ctx->stream));
+    if (sweeps == 0 || s.nx < 3 || s.ny < 3 || s.nz < 3) {
+        // nothing to update: the state after the sweeps is the start (every diff stays 0)
+        DFT_CUDA(cudaMemcpyAsync(v_out, v_in, sizeof(double) * (size_t)s.N, cudaMemcpyDeviceToDevice, ctx->stream));
+        return;
+    }
+    {
+        const long long shell = 2LL * s.nx * s.ny + 2LL * s.nx * (s.nz - 2) + 2LL * (s.ny - 2) * (s.nz - 2);
+        const int blocks = (int)std::min<long long>((shell + 255) / 256, (long long)ctx->num_sms * 4);
+        slab_shell_copy_kernel<<<blocks, 256, 0, ctx->stream>>>(s.nx, s.ny, s.nz, v_in, v_out, scratch);
+        DFT_LAUNCH_CHECK();
+        count_launch(ctx);
+    }
     const double den = 2.0 * (g.ix2 + g.iy2 + g.iz2);
     const int bx = (s.nx + SB_X - 1) / SB_X, by = (s.ny + SB_Y - 1) / SB_Y;
     int zc = 32;
@@ -156,15 +200,17 @@ void zslab_jacobi_sweeps(dft_context* ctx, const Grid& g, int z_lo, int z_hi, in
     const dim3 grid(bx, by, (s.nz + zc - 1) / zc), block(SB_X, SB_Y);
     const int lo = own_lo - z_lo, hi = own_hi - z_lo;
     unsigned long long* bits = reinterpret_cast<unsigned long long*>(diffs);
+    // sweep t writes v_out when sweeps - 1 - t is even, so the last one lands there; v_in is
+    // only read
+    const double* cur = v_in;
     for (int t = 0; t < sweeps; ++t) {
-        const double* cur = (t & 1) ? tmp : v;
-        double* nxt = (t & 1) ? v : tmp;
+        double* nxt = ((sweeps - 1 - t) & 1) ? scratch : v_out;
         slab_sweep_kernel<<<grid, block, 0, ctx->stream>>>(s.nx, s.ny, s.nz, g.ix2, g.iy2, g.iz2, den, rho, cur, nxt,
                                                            lo, hi, zc, bits + t);
+        cur = nxt;
     }
     DFT_LAUNCH_CHECK();
     count_launch(ctx, sweeps);
-    if (sweeps & 1) DFT_CUDA(cudaMemcpyAsync(v, tmp, sizeof(double) * (size_t)s.N, cudaMemcpyDeviceToDevice, ctx->stream));
 }
 
 void zslab_hamiltonian(dft_context* ctx, const Grid& g, int z_lo, int z_hi, const double* V, const double* psi,

@@ -10,6 +10,7 @@
     python -m dft_b200.microbench train --n 96 --tc 1                 # network training step
     python -m dft_b200.microbench rotate --n 64 --ka 128 --kb 64 --precision 1   # tcgen05 rotation
     python -m dft_b200.microbench scf --system h2o_128 --poisson multigrid --mixed 1 --stop-abs-de 1e-6
+    python -m dft_b200.microbench zslab --n 192 --sweeps 2000 --slabs 1,2,4 --halo 8   # z-slab Jacobi, one GPU
 
 Each mode prints one JSON line with the time and the achieved bandwidth for the
 operator's algorithmic bytes.  Used for roofline numbers and as the command under ncu.
@@ -60,7 +61,7 @@ def cube(n, h):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("mode", choices=["hpsi", "jacobi", "xc", "scf", "radial", "gram", "poisson", "train", "rotate",
-                                     "c4"])
+                                     "c4", "zslab"])
     ap.add_argument("--samples", type=int, default=512, help="c4: training densities")
     ap.add_argument("--held-out", type=int, default=6, help="c4: held-out densities per grid")
     ap.add_argument("--tc", type=int, default=1, help="network convolutions on the tensor cores (1) or CUDA cores (0)")
@@ -98,6 +99,8 @@ def main():
     ap.add_argument("--predict", type=int, default=0, help="scf: V_H(n_in) start from the mixer's combination (1)")
     ap.add_argument("--tuning", default="", help="context tuning keys, e.g. orthonormalise_adaptive=0,hpsi_variant=2")
     ap.add_argument("--system-args", default="{}", help='scf: JSON keyword arguments of the system, e.g. {"nmol": 7}')
+    ap.add_argument("--slabs", default="1,2,4", help="zslab: slab counts (all slabs held by this process)")
+    ap.add_argument("--halo", type=int, default=8, help="zslab: halo planes per side (sweeps per exchange)")
     ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args()
     import torch
@@ -138,6 +141,39 @@ def main():
         interior = (a.n - 2) ** 3
         out.update(n=a.n, spl=a.spl, sweeps=res["s"], ms=ms, us_per_sweep=1e3 * ms / res["s"],
                    gbs=24.0 * interior * res["s"] / (ms * 1e-3) / 1e9)
+    elif a.mode == "zslab":
+        # wall time: the slab driver is host-synchronous (one exchange and one reduction per block)
+        import time
+
+        from .zslab import CudaSlabOps, LocalSlabs, SlabLayout, hartree_zslab
+        g = cube(a.n, a.h)
+        N = g.getSize()
+        x = np.linspace(-1, 1, a.n)
+        X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+        rho_h = np.exp(-8 * (X ** 2 + Y ** 2 + Z ** 2)).ravel()
+        rho, vh = eng.upload(rho_h), eng.array(N)
+        eng.hartree(g, rho, vh, 1e-8, min(a.sweeps, 64))
+        t0 = time.perf_counter()
+        s_ref, _ = eng.hartree(g, rho, vh, 1e-8, a.sweeps)
+        whole_ms = 1e3 * (time.perf_counter() - t0)
+        ref = vh.to_host()
+        field = torch.from_numpy(rho_h).cuda()
+        ops = CudaSlabOps(eng)
+        rows = []
+        for R in [int(v) for v in a.slabs.split(",")]:
+            lay = SlabLayout(g.shape, R, a.halo)
+            sl = {r: lay.scatter(field, r) for r in range(R)}
+            hartree_zslab(LocalSlabs(R), lay, g, sl, ops, 1e-8, min(a.sweeps, 4 * lay.halo))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            v, s, _ = hartree_zslab(LocalSlabs(R), lay, g, sl, ops, 1e-8, a.sweeps)
+            torch.cuda.synchronize()
+            ms = 1e3 * (time.perf_counter() - t0)
+            same = bool(s == s_ref and lay.gather(v).cpu().numpy().tobytes() == ref.tobytes())
+            rows.append({"slabs": R, "halo": lay.halo, "sweeps": s, "ms": ms, "us_per_sweep": 1e3 * ms / s,
+                         "identical_to_whole_grid": same})
+            del v, sl
+        out.update(n=a.n, sweeps=s_ref, whole_ms=whole_ms, whole_us_per_sweep=1e3 * whole_ms / s_ref, slabs=rows)
     elif a.mode == "xc":
         g = cube(a.n, a.h)
         N = g.getSize()

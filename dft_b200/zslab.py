@@ -214,14 +214,16 @@ class CudaSlabOps:
                                                   C.c_void_p(v.data_ptr())))
 
     def jacobi_sweeps(self, grid, z_lo: int, z_hi: int, own_lo: int, own_hi: int, rho: torch.Tensor,
-                      v: torch.Tensor, tmp: torch.Tensor, sweeps: int, diffs: torch.Tensor) -> None:
+                      v_in: torch.Tensor, v_out: torch.Tensor, scratch: torch.Tensor, sweeps: int,
+                      diffs: torch.Tensor) -> None:
         from . import _check
-        self._ready(v)
+        self._ready(v_in)
         g = grid.c()
         _check(self.lib.dft_zslab_jacobi_sweeps_dev(self.engine.ctx, C.byref(g), int(z_lo), int(z_hi), int(own_lo),
                                                     int(own_hi), C.c_void_p(rho.data_ptr()),
-                                                    C.c_void_p(v.data_ptr()), C.c_void_p(tmp.data_ptr()),
-                                                    int(sweeps), C.c_void_p(diffs.data_ptr())))
+                                                    C.c_void_p(v_in.data_ptr()), C.c_void_p(v_out.data_ptr()),
+                                                    C.c_void_p(scratch.data_ptr()), int(sweeps),
+                                                    C.c_void_p(diffs.data_ptr())))
 
     def hamiltonian(self, grid, z_lo: int, z_hi: int, V: torch.Tensor, psi: torch.Tensor, hpsi: torch.Tensor,
                     nbands: int) -> None:
@@ -269,7 +271,8 @@ def hartree_zslab(comm, layout: SlabLayout, grid, rho: Dict[int, torch.Tensor], 
             rows = layout.owned_rows(r)
             part[r] = rho[r][rows.start * n:rows.stop * n].sum().reshape(1)
         Q = float(comm.allreduce_sum(part).item()) * (grid.getDx() * grid.getDy() * grid.getDz())
-    v, tmp, snap, diffs = {}, {}, {}, {}
+    # three buffers per slab: the block's start (read only), the block's result, and scratch
+    v, out, scratch, diffs = {}, {}, {}, {}
     for r in comm.ranks:
         lo, hi = layout.extent(r)
         v[r] = torch.empty(layout.points(r), dtype=torch.float64, device=rho[r].device)
@@ -280,8 +283,8 @@ def hartree_zslab(comm, layout: SlabLayout, grid, rho: Dict[int, torch.Tensor], 
         return v, 1, 0.0
     T = layout.halo
     for r in comm.ranks:
-        tmp[r] = torch.empty_like(v[r])
-        snap[r] = torch.empty_like(v[r])
+        out[r] = torch.empty_like(v[r])
+        scratch[r] = torch.empty_like(v[r])
         diffs[r] = torch.zeros(T, dtype=torch.float64, device=v[r].device)
     done = 0
     while True:
@@ -290,24 +293,23 @@ def hartree_zslab(comm, layout: SlabLayout, grid, rho: Dict[int, torch.Tensor], 
         for r in comm.ranks:
             lo, hi = layout.extent(r)
             a, b = layout.own[r]
-            snap[r].copy_(v[r])
-            ops.jacobi_sweeps(grid, lo, hi, a, b, rho[r], v[r], tmp[r], nb, diffs[r])
+            ops.jacobi_sweeps(grid, lo, hi, a, b, rho[r], v[r], out[r], scratch[r], nb, diffs[r])
         d = comm.allreduce_max({r: diffs[r][:nb] for r in comm.ranks}).cpu().tolist()
         stop = None
         for s in range(nb):
             if d[s] < tol or done + s + 1 >= max_sweeps:
                 stop = s + 1
                 break
-        if stop is None:
-            done += nb
-            continue
-        if stop < nb:
+        if stop is not None and stop < nb:
+            # the block passed the stop: rerun its first `stop` sweeps from the untouched start
             for r in comm.ranks:
                 lo, hi = layout.extent(r)
                 a, b = layout.own[r]
-                v[r].copy_(snap[r])
-                ops.jacobi_sweeps(grid, lo, hi, a, b, rho[r], v[r], tmp[r], stop, diffs[r])
-        return v, done + stop, d[stop - 1]
+                ops.jacobi_sweeps(grid, lo, hi, a, b, rho[r], v[r], out[r], scratch[r], stop, diffs[r])
+        v, out = out, v
+        if stop is not None:
+            return v, done + stop, d[stop - 1]
+        done += nb
 
 
 def hamiltonian_zslab(comm, layout: SlabLayout, grid, V: Dict[int, torch.Tensor], psi: Dict[int, torch.Tensor],

@@ -211,15 +211,17 @@ dft_status_t dft_zslab_jacobi_init_dev(dft_context* ctx, const dft_grid* g, int 
                                        const double* guess, double* v);
 
 /* `sweeps` Jacobi sweeps of dft_hartree_dev's loop (reference HartreePotentialMolecule.cpp:
- * 207-321) on a slab: every plane of the slab except its first and last is updated, so with
- * T halo planes per side the rank's own planes are exact for up to T sweeps.  diffs (device,
- * `sweeps` doubles): max|dV| of each sweep over the owned planes [own_lo, own_hi) (global
- * indices; every owned plane that g's interior contains must be an inner plane of the slab).
- * The maximum of diffs[t] over ranks is the single-domain loop's max|dV| of that sweep.
- * rho, v, tmp: device, the slab's size; v holds the result, tmp is scratch.  Synchronises. */
+ * 207-321) on a slab, from v_in into v_out: every plane of the slab except its first and last
+ * is updated, so with T halo planes per side the rank's own planes are exact for up to T
+ * sweeps.  v_in is only read, so a block of sweeps that passed the stop can be rerun from it.
+ * diffs (device, `sweeps` doubles): max|dV| of each sweep over the owned planes
+ * [own_lo, own_hi) (global indices; every owned plane that g's interior contains must be an
+ * inner plane of the slab).  The maximum of diffs[t] over ranks is the single-domain loop's
+ * max|dV| of that sweep.  rho, v_in, v_out, scratch: distinct device buffers of the slab's
+ * size.  Synchronises. */
 dft_status_t dft_zslab_jacobi_sweeps_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo,
-                                         int own_hi, const double* rho, double* v, double* tmp, int sweeps,
-                                         double* diffs);
+                                         int own_hi, const double* rho, const double* v_in, double* v_out,
+                                         double* scratch, int sweeps, double* diffs);
 
 /* dft_apply_hamiltonian_dev on a slab (reference KohnShamHamiltonianMolecule.cpp:78-177):
  * with one halo plane per side (none at the faces of g) the owned planes of hpsi are

@@ -104,13 +104,13 @@ def test_slab_arguments_rejected(engine):
     ops = CudaSlabOps(engine)
     g = CartesianGrid(*N, *B)
     npl = N[0] * N[1]
-    t = {k: torch.zeros(10 * npl, dtype=torch.float64, device="cuda") for k in ("rho", "v", "tmp")}
+    t = {k: torch.zeros(10 * npl, dtype=torch.float64, device="cuda") for k in ("rho", "v", "w", "tmp")}
     d = torch.zeros(4, dtype=torch.float64, device="cuda")
     with pytest.raises(DFTError):  # owned plane 5 is the slab's first plane (no halo beyond it)
-        ops.jacobi_sweeps(g, 5, 15, 5, 10, t["rho"], t["v"], t["tmp"], 4, d)
+        ops.jacobi_sweeps(g, 5, 15, 5, 10, t["rho"], t["v"], t["w"], t["tmp"], 4, d)
     with pytest.raises(DFTError):  # slab past the grid
-        ops.jacobi_sweeps(g, 35, 45, 36, 44, t["rho"], t["v"], t["tmp"], 4, d)
-    with pytest.raises(DFTError):  # v and tmp alias
-        ops.jacobi_sweeps(g, 5, 15, 6, 14, t["rho"], t["v"], t["v"], 4, d)
+        ops.jacobi_sweeps(g, 35, 45, 36, 44, t["rho"], t["v"], t["w"], t["tmp"], 4, d)
+    with pytest.raises(DFTError):  # result and scratch alias
+        ops.jacobi_sweeps(g, 5, 15, 6, 14, t["rho"], t["v"], t["w"], t["w"], 4, d)
     with pytest.raises(DFTError):
         ops.hamiltonian(g, 10, 5, t["v"], t["rho"], t["tmp"], 1)

@@ -35,22 +35,22 @@ class NumpySlabOps:
         inner = guess.numpy().reshape(shape) if guess is not None else np.zeros(shape)
         v.numpy().reshape(shape)[...] = np.where(face, bval, inner)
 
-    def jacobi_sweeps(self, grid, z_lo, z_hi, own_lo, own_hi, rho, v, tmp, sweeps, diffs):
+    def jacobi_sweeps(self, grid, z_lo, z_hi, own_lo, own_hi, rho, v_in, v_out, scratch, sweeps, diffs):
         nx, ny = grid.nx, grid.ny
         nzl = z_hi - z_lo
         dx, dy, dz = _spacing(grid)
         ix, iy, iz = 1.0 / (dx * dx), 1.0 / (dy * dy), 1.0 / (dz * dz)
         den = 2.0 * (ix + iy + iz)
         c4pi = 4.0 * math.pi
-        a = v.numpy().reshape(nzl, ny, nx)
-        b = tmp.numpy().reshape(nzl, ny, nx)
+        a = v_in.numpy().reshape(nzl, ny, nx)
+        o = v_out.numpy().reshape(nzl, ny, nx)
         src = c4pi * rho.numpy().reshape(nzl, ny, nx)[1:-1, 1:-1, 1:-1]
         dv = diffs.numpy()
         dv[:sweeps] = 0.0
-        b[...] = a
+        o[...] = a
         # owned planes that the slab updates, as rows of the interior block
         lo, hi = max(own_lo - z_lo, 1) - 1, min(own_hi - z_lo, nzl - 1) - 1
-        cur, nxt = a, b
+        cur = a.copy()
         for t in range(sweeps):
             if nx >= 3 and ny >= 3 and nzl >= 3:
                 c = cur[1:-1, 1:-1, 1:-1]
@@ -63,10 +63,11 @@ class NumpySlabOps:
                 new = acc / den
                 if hi > lo:
                     dv[t] = np.abs(new[lo:hi] - c[lo:hi]).max()
+                nxt = cur.copy()
                 nxt[1:-1, 1:-1, 1:-1] = new
-            cur, nxt = nxt, cur
-        if sweeps % 2:
-            a[...] = b
+                cur = nxt
+        o[...] = cur
+        scratch.numpy()[...] = np.nan  # the caller must not rely on it
 
     def hamiltonian(self, grid, z_lo, z_hi, V, psi, hpsi, nbands):
         nx, ny = grid.nx, grid.ny
