@@ -151,6 +151,10 @@ _SIGS = {
                                      C.c_int, _P], C.c_int),
     "dft_zslab_hamiltonian_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, _P, _P, _P, C.c_int, C.c_long],
                                   C.c_int),
+    "dft_zslab_xc_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _D],
+                         C.c_int),
+    "dft_zslab_gram_dev": ([_P, C.POINTER(dft_grid), C.c_int, C.c_int, C.c_int, C.c_int, _P, C.c_long, C.c_int, _P,
+                           C.c_long, C.c_int, C.c_int, _D], C.c_int),
     "dft_xc_dev": ([_P, C.POINTER(dft_grid), C.c_int, _P, _P, _P, _P, _D], C.c_int),
     "dft_xc_evaluate_dev": ([_P, C.c_int, C.c_long, _P, _P, _P, _P, _P], C.c_int),
     "dft_spin_density_dev": ([_P, C.c_long, _P, C.c_int, C.c_long, _D, _P], C.c_int),

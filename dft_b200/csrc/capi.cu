@@ -313,6 +313,31 @@ dft_status_t dft_zslab_hamiltonian_dev(dft_context* ctx, const dft_grid* g, int 
     });
 }
 
+dft_status_t dft_zslab_xc_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo, int own_hi,
+                              dft_xc_kind kind, const double* na, const double* nb, double* va, double* vb,
+                              double* exc_out) {
+    return guard(ctx, [&] {
+        NEED(ctx && na && nb, "NULL argument");
+        const dftb::Grid G = dftb::make_grid(g);
+        const double e = dftb::zslab_xc(ctx, G, z_lo, z_hi, own_lo, own_hi, (int)kind, na, nb, va, vb);
+        dftb::sync(ctx);
+        if (exc_out) *exc_out = e;
+    });
+}
+
+dft_status_t dft_zslab_gram_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo, int own_hi,
+                                const double* A, long lda, int ka, const double* B, long ldb, int kb, int precision,
+                                double* C_host) {
+    return guard(ctx, [&] {
+        NEED(ctx && A && B && C_host, "NULL argument");
+        NEED(ka > 0 && kb > 0, "bad sizes");
+        const dftb::Grid G = dftb::make_grid(g);
+        std::vector<double> C;
+        dftb::zslab_gram(ctx, G, z_lo, z_hi, own_lo, own_hi, A, lda, ka, B, ldb, kb, precision, C);
+        std::copy(C.begin(), C.end(), C_host);
+    });
+}
+
 dft_status_t dft_hartree_monopole_dev(dft_context* ctx, const dft_grid* g, const double* rho, double* vh, double tol,
                                       long max_sweeps, long* sweeps_out, double* last_diff_out) {
     return guard(ctx, [&] {

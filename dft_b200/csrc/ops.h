@@ -53,6 +53,13 @@ void zslab_jacobi_sweeps(dft_context* ctx, const Grid& g, int z_lo, int z_hi, in
                          double* diffs);
 void zslab_hamiltonian(dft_context* ctx, const Grid& g, int z_lo, int z_hi, const double* V, const double* psi,
                        double* hpsi, int nbands, long long ld);
+// XC potentials of the slab (owned planes exact with two halo planes per side; va/vb may be
+// NULL) and the owned planes' part of E_xc (returned; synchronises).
+double zslab_xc(dft_context* ctx, const Grid& g, int z_lo, int z_hi, int own_lo, int own_hi, int kind,
+                const double* na, const double* nb, double* va, double* vb);
+// dV A^T B over the owned planes of a slab (the rank's part of the Gram product; ka x kb row-major)
+void zslab_gram(dft_context* ctx, const Grid& g, int z_lo, int z_hi, int own_lo, int own_hi, const double* A,
+                long long lda, int ka, const double* B, long long ldb, int kb, int precision, std::vector<double>& C);
 
 // Monopole boundary option (grid_ops.cu): vc = Q erf(|r|/(sqrt 2 s))/|r| (Q = sum rho dV, returned)
 // and rho_prime = rho + L_h vc / (4 pi) on the interior, so that V_H = V' + vc with V' the

@@ -20,11 +20,19 @@
 // owned planes of a slab see the same six neighbours as on the whole grid, and the grid's own
 // faces (where no neighbour exists) are slab faces too, so apply_hamiltonian on the slab's
 // plane count gives bit-identical owned planes.
+//
+// XC (reference ExchangeCorrelationMolecule.cpp:576-842): the potential at a plane needs the
+// gradient coefficients one plane away, which need the densities two planes away, so with two
+// halo planes per side the XC kernels on the slab give bit-identical owned planes.  The energy
+// is summed over the owned planes only; ranks add their parts.
+//
+// Gram products: the sum over points splits into per-rank sums over owned planes.
 #include <algorithm>
 #include <cmath>
 
 #include "ops.h"
 #include "xc_device.cuh"
+#include "xc_grad.cuh"
 
 namespace dftb {
 namespace {
@@ -145,6 +153,35 @@ __global__ void slab_shell_copy_kernel(int nx, int ny, int nzl, const double* __
     }
 }
 
+// Sum of n eps dV over the points [p_lo, p_hi) of a slab (one partial per block), gradients
+// from the whole slab as in xc_point_kernel.
+template <int KIND>
+__global__ void __launch_bounds__(256) slab_xc_energy_kernel(Grid s, long long p_lo, long long p_hi,
+                                                             const double* __restrict__ na,
+                                                             const double* __restrict__ nb,
+                                                             double* __restrict__ partial) {
+    __shared__ double sh[8];
+    double e = 0.0;
+    for (long long p = p_lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < p_hi;
+         p += (long long)gridDim.x * blockDim.x) {
+        const double a = na[p], b = nb[p];
+        const double n = a + b;
+        if (n > xcf::RHO_FLOOR) {
+            const int i = (int)(p % s.nx);
+            const int j = (int)((p / s.nx) % s.ny);
+            const int k = (int)(p / ((long long)s.nx * s.ny));
+            double ga = 0.0, gb = 0.0;
+            if (KIND == 1) {
+                ga = gradmag(s, na, p, i, j, k);
+                gb = gradmag(s, nb, p, i, j, k);
+            }
+            e += n * xcf::evaluate<KIND>(a, b, ga, gb).eps * s.dV;
+        }
+    }
+    e = block_sum(e, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = e;
+}
+
 // The slab as a Grid: the global spacing and bounds (so every constant is the whole grid's),
 // the slab's plane count.
 Grid slab_grid(const Grid& g, int z_lo, int z_hi) {
@@ -219,6 +256,49 @@ void zslab_hamiltonian(dft_context* ctx, const Grid& g, int z_lo, int z_hi, cons
     const Grid s = slab_grid(g, z_lo, z_hi);
     if (ld < s.N) fail(DFT_INVALID_ARGUMENT, "ld must be >= nx*ny*(z_hi - z_lo)");
     apply_hamiltonian(ctx, s, V, psi, hpsi, nbands, ld);
+}
+
+double zslab_xc(dft_context* ctx, const Grid& g, int z_lo, int z_hi, int own_lo, int own_hi, int kind,
+                const double* na, const double* nb, double* va, double* vb) {
+    check_slab(g, z_lo, z_hi);
+    if (own_lo > own_hi || own_lo < z_lo || own_hi > z_hi)
+        fail(DFT_INVALID_ARGUMENT, "owned planes must lie inside the slab");
+    // two planes beyond the owned ones on each side, unless the slab ends at a face of g
+    if (own_lo < own_hi && ((z_lo > 0 && own_lo - z_lo < 2) || (z_hi < g.nz && z_hi - own_hi < 2)))
+        fail(DFT_INVALID_ARGUMENT, "XC on a slab needs two halo planes beyond the owned planes");
+    if (kind != DFT_XC_PZ81 && kind != DFT_XC_PBE96) fail(DFT_INVALID_ARGUMENT, "unknown functional kind %d", kind);
+    const Grid s = slab_grid(g, z_lo, z_hi);
+    if (va || vb) xc(ctx, s, kind, na, nb, va, vb, false);
+    const long long sxy = (long long)s.nx * s.ny;
+    const long long p_lo = (long long)(own_lo - z_lo) * sxy, p_hi = (long long)(own_hi - z_lo) * sxy;
+    if (p_hi <= p_lo) return 0.0;
+    const int nbk = (int)std::max<long long>(1, std::min<long long>((p_hi - p_lo + 255) / 256, (long long)ctx->num_sms * 8));
+    double* partial = (double*)ws_get(ctx, WS_REDUCE, sizeof(double) * (size_t)nbk);
+    if (kind == DFT_XC_PBE96)
+        slab_xc_energy_kernel<1><<<nbk, 256, 0, ctx->stream>>>(s, p_lo, p_hi, na, nb, partial);
+    else
+        slab_xc_energy_kernel<0><<<nbk, 256, 0, ctx->stream>>>(s, p_lo, p_hi, na, nb, partial);
+    DFT_LAUNCH_CHECK();
+    count_launch(ctx);
+    double* h = pinned(ctx, (size_t)nbk);
+    DFT_CUDA(cudaMemcpyAsync(h, partial, sizeof(double) * (size_t)nbk, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    double e = 0.0;
+    for (int b = 0; b < nbk; ++b) e += h[b];
+    return e;
+}
+
+void zslab_gram(dft_context* ctx, const Grid& g, int z_lo, int z_hi, int own_lo, int own_hi, const double* A,
+                long long lda, int ka, const double* B, long long ldb, int kb, int precision, std::vector<double>& C) {
+    check_slab(g, z_lo, z_hi);
+    if (own_lo >= own_hi || own_lo < z_lo || own_hi > z_hi)
+        fail(DFT_INVALID_ARGUMENT, "owned planes must be a non-empty range inside the slab");
+    const long long slab_n = (long long)g.nx * g.ny * (z_hi - z_lo);
+    if (lda < slab_n || ldb < slab_n) fail(DFT_INVALID_ARGUMENT, "lda and ldb must be >= nx*ny*(z_hi - z_lo)");
+    const Grid own = slab_grid(g, own_lo, own_hi);
+    const long long off = (long long)(own_lo - z_lo) * g.nx * g.ny;
+    if (precision == 1) gram_tc(ctx, own, A + off, lda, ka, B + off, ldb, kb, C);
+    else gram_fp64(ctx, own, A + off, lda, ka, B + off, ldb, kb, C);
 }
 
 }  // namespace dftb

@@ -18,8 +18,13 @@ on the CPU); every halo plane lands in the receiving rank's own memory before a 
 it.  `LocalSlabs` holds all ranks' slabs in one process and exchanges by copies, which runs
 the same decomposition on one device.
 
+* XC (ExchangeCorrelationMolecule.cpp:576-842): two halo planes per side; potentials
+  bit-identical on the owned planes, E_xc summed over ranks.
+* Gram products (the block eigensolver's dV A^T B): per-rank products over the owned planes,
+  summed over ranks.
+
 The compute goes through `CudaSlabOps` (the slab kernels of libdft_b200); the driver takes
-any object with the same three methods.
+any object with the same methods.
 """
 from __future__ import annotations
 
@@ -237,6 +242,32 @@ class CudaSlabOps:
         self.engine.synchronize()
 
 
+    def xc(self, grid, z_lo: int, z_hi: int, own_lo: int, own_hi: int, kind: int, na: torch.Tensor,
+           nb: torch.Tensor, va: Optional[torch.Tensor], vb: Optional[torch.Tensor]) -> float:
+        from . import _check
+        self._ready(na)
+        g = grid.c()
+        e = C.c_double()
+        ptr = lambda t: C.c_void_p(t.data_ptr() if t is not None else None)  # noqa: E731
+        _check(self.lib.dft_zslab_xc_dev(self.engine.ctx, C.byref(g), int(z_lo), int(z_hi), int(own_lo), int(own_hi),
+                                         int(kind), ptr(na), ptr(nb), ptr(va), ptr(vb), C.byref(e)))
+        return e.value
+
+    def gram(self, grid, z_lo: int, z_hi: int, own_lo: int, own_hi: int, A: torch.Tensor, ka: int, B: torch.Tensor,
+             kb: int, precision: int = 0) -> torch.Tensor:
+        import numpy as np
+
+        from . import _check
+        self._ready(A)
+        g = grid.c()
+        out = np.zeros((ka, kb))
+        _check(self.lib.dft_zslab_gram_dev(self.engine.ctx, C.byref(g), int(z_lo), int(z_hi), int(own_lo),
+                                           int(own_hi), C.c_void_p(A.data_ptr()), C.c_long(A.shape[-1]), int(ka),
+                                           C.c_void_p(B.data_ptr()), C.c_long(B.shape[-1]), int(kb), int(precision),
+                                           out.ctypes.data_as(C.POINTER(C.c_double))))
+        return torch.from_numpy(out).to(A.device)
+
+
 def _faces_exact(grid) -> bool:
     """Whether every face's last node lands exactly on its bound (the reference's face values
     are then all zero and the total charge is unused)."""
@@ -327,3 +358,44 @@ def hamiltonian_zslab(comm, layout: SlabLayout, grid, V: Dict[int, torch.Tensor]
         out[r] = torch.empty_like(psi[r])
         ops.hamiltonian(grid, lo, hi, V[r], psi[r], out[r], nbands)
     return out
+
+
+def xc_zslab(comm, layout: SlabLayout, grid, kind: int, na: Dict[int, torch.Tensor], nb: Dict[int, torch.Tensor],
+             ops, potentials: bool = True):
+    """`calculateMolecularSpinExchangeCorrelationPotential` for both spins and
+    `calculateMolecularExchangeCorrelationEnergy` (ExchangeCorrelationMolecule.cpp:576-842)
+    over z-slabs: returns ({rank: v_alpha}, {rank: v_beta}, E_xc), the potentials' owned planes
+    bit-identical to the whole grid's, E_xc the sum of the ranks' parts (a different summation
+    order).  The layout needs two halo planes (every rank owns at least two planes); the halo
+    planes of na and nb are overwritten by the exchange."""
+    if (layout.nx, layout.ny, layout.nz) != (grid.nx, grid.ny, grid.nz) or layout.world != comm.world:
+        raise ValueError("layout does not match the grid or the number of ranks")
+    if comm.world > 1:
+        if layout.halo < 2:
+            raise ValueError("XC on slabs needs two halo planes per side")
+        comm.exchange(layout, na, 2)
+        comm.exchange(layout, nb, 2)
+    va, vb, part = {}, {}, {}
+    for r in comm.ranks:
+        lo, hi = layout.extent(r)
+        a, b = layout.own[r]
+        va[r] = torch.empty_like(na[r]) if potentials else None
+        vb[r] = torch.empty_like(nb[r]) if potentials else None
+        e = ops.xc(grid, lo, hi, a, b, kind, na[r], nb[r], va[r], vb[r])
+        part[r] = torch.tensor([e], dtype=torch.float64, device=na[r].device)
+    return va, vb, float(comm.allreduce_sum(part).item())
+
+
+def gram_zslab(comm, layout: SlabLayout, grid, A: Dict[int, torch.Tensor], ka: int, B: Dict[int, torch.Tensor],
+               kb: int, ops, precision: int = 0) -> torch.Tensor:
+    """The block eigensolver's Gram product dV A^T B over z-slabs: each rank's product over its
+    owned planes, summed over ranks (an all-reduce of ka x kb values).  A and B are (bands,
+    points) slabs in `layout`; their halo planes are not read."""
+    if (layout.nx, layout.ny, layout.nz) != (grid.nx, grid.ny, grid.nz) or layout.world != comm.world:
+        raise ValueError("layout does not match the grid or the number of ranks")
+    part = {}
+    for r in comm.ranks:
+        lo, hi = layout.extent(r)
+        a, b = layout.own[r]
+        part[r] = ops.gram(grid, lo, hi, a, b, A[r], ka, B[r], kb, precision)
+    return comm.allreduce_sum(part)

@@ -229,6 +229,24 @@ dft_status_t dft_zslab_jacobi_sweeps_dev(dft_context* ctx, const dft_grid* g, in
 dft_status_t dft_zslab_hamiltonian_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, const double* V,
                                        const double* psi, double* hpsi, int nbands, long ld);
 
+/* dft_xc_dev on a slab (reference ExchangeCorrelationMolecule.cpp:576-842): va/vb (device, the
+ * slab's size, either may be NULL) get the XC potentials, bit-identical to the whole-grid
+ * result on the owned planes [own_lo, own_hi) when the slab holds two planes beyond them on
+ * each side (or ends at a face of g; DFT_INVALID_ARGUMENT otherwise).  exc_out (host, may be
+ * NULL): the owned planes' part of E_xc; the ranks' parts add up to E_xc (summed in a different
+ * order than the whole grid's). */
+dft_status_t dft_zslab_xc_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo, int own_hi,
+                              dft_xc_kind kind, const double* na, const double* nb, double* va, double* vb,
+                              double* exc_out);
+
+/* The owned planes' part of dft_gram_dev's product: dV * A^T B summed over the points of the
+ * planes [own_lo, own_hi) of a slab (A: ka bands, B: kb bands, leading dimensions >= the slab's
+ * size), into C_host (ka x kb, row-major).  The ranks' parts add up to the whole grid's
+ * product. */
+dft_status_t dft_zslab_gram_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo, int own_hi,
+                                const double* A, long lda, int ka, const double* B, long ldb, int kb, int precision,
+                                double* C_host);
+
 /* calculateHartreeEnergy (reference HartreePotentialMolecule.cpp:326-379): 1/2 sum rho V dV. */
 dft_status_t dft_hartree_energy_dev(dft_context* ctx, const dft_grid* g, const double* rho, const double* vh,
                                     double* energy_out);

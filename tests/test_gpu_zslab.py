@@ -4,14 +4,16 @@ process on one GPU (LocalSlabs: halos by device copies, no kernel waits on anoth
 The potential and sweep count of 1-4 slabs equal dft_hartree_dev / the oracle bit for bit
 (HartreePotentialMolecule.cpp:99-324), from a cold and from a warm start, at the reference's
 stop and at a sweep cap; H psi of 1-4 slabs equals dft_apply_hamiltonian_dev bit for bit
-(KohnShamHamiltonianMolecule.cpp:78-177); invalid slab arguments are rejected before any
-launch."""
+(KohnShamHamiltonianMolecule.cpp:78-177); the XC potentials equal dft_xc_dev bit for bit and
+E_xc to 1e-12 (ExchangeCorrelationMolecule.cpp:576-842); the slabs' Gram parts add up to
+dft_gram_dev's product; invalid slab arguments are rejected before any launch."""
 import numpy as np
 import pytest
 import torch
 
 from dft_b200 import CartesianGrid, DFTError
-from dft_b200.zslab import CudaSlabOps, LocalSlabs, SlabLayout, hamiltonian_zslab, hartree_zslab
+from dft_b200.zslab import (CudaSlabOps, LocalSlabs, SlabLayout, gram_zslab, hamiltonian_zslab, hartree_zslab,
+                            xc_zslab)
 
 pytestmark = pytest.mark.gpu
 
@@ -100,6 +102,47 @@ def test_hamiltonian_slabs_match_whole_grid(engine, world):
     assert out.tobytes() == ref.tobytes()
 
 
+@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_xc_slabs_match_whole_grid(engine, kind, world):
+    rho = _density(N, B)
+    na, nb = 0.6 * rho, 0.4 * rho + 0.05 * np.roll(rho, 7)
+    g = CartesianGrid(*N, *B)
+    npts = rho.size
+    dva, dvb = engine.array(npts), engine.array(npts)
+    ref_e = engine.xc(g, kind, engine.upload(na), engine.upload(nb), dva, dvb)
+    lay = SlabLayout(N, world, 2)
+    A = {r: lay.scatter(torch.from_numpy(na).cuda(), r) for r in range(world)}
+    Bs = {r: lay.scatter(torch.from_numpy(nb).cuda(), r) for r in range(world)}
+    for r in range(world):  # halo planes come from the exchange
+        rows = lay.owned_rows(r)
+        for t in (A[r], Bs[r]):
+            view = t.view(-1, lay.plane_points)
+            view[:rows.start] = float("nan")
+            view[rows.stop:] = float("nan")
+    va, vb, exc = xc_zslab(LocalSlabs(world), lay, g, kind, A, Bs, CudaSlabOps(engine))
+    assert lay.gather(va).cpu().numpy().tobytes() == dva.to_host().tobytes()
+    assert lay.gather(vb).cpu().numpy().tobytes() == dvb.to_host().tobytes()
+    assert abs(exc - ref_e) <= 1e-12 * abs(ref_e)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gram_slabs_sum_to_whole_grid(engine, precision):
+    rng = np.random.default_rng(5)
+    npts = int(np.prod(N))
+    ka, kb = 40, 24
+    A, Bm = rng.standard_normal((ka, npts)), rng.standard_normal((kb, npts))
+    g = CartesianGrid(*N, *B)
+    ref = engine.gram(g, engine.upload(A), npts, ka, engine.upload(Bm), npts, kb, 0)
+    lay = SlabLayout(N, 3, 1)
+    At, Bt = torch.from_numpy(A).cuda(), torch.from_numpy(Bm).cuda()
+    As = {r: lay.scatter(At, r) for r in range(3)}
+    Bs = {r: lay.scatter(Bt, r) for r in range(3)}
+    c = gram_zslab(LocalSlabs(3), lay, g, As, ka, Bs, kb, CudaSlabOps(engine), precision).cpu().numpy()
+    tol = 1e-12 if precision == 0 else 1e-5
+    assert np.max(np.abs(c - ref)) <= tol * np.max(np.abs(ref))
+
+
 def test_slab_arguments_rejected(engine):
     ops = CudaSlabOps(engine)
     g = CartesianGrid(*N, *B)
@@ -114,3 +157,7 @@ def test_slab_arguments_rejected(engine):
         ops.jacobi_sweeps(g, 5, 15, 6, 14, t["rho"], t["v"], t["w"], t["w"], 4, d)
     with pytest.raises(DFTError):
         ops.hamiltonian(g, 10, 5, t["v"], t["rho"], t["tmp"], 1)
+    with pytest.raises(DFTError):  # one plane beyond the owned ones: XC needs two
+        ops.xc(g, 5, 15, 6, 14, 1, t["rho"], t["v"], t["w"], t["tmp"])
+    with pytest.raises(DFTError):  # empty owned range
+        ops.gram(g, 5, 15, 8, 8, t["v"], 1, t["w"], 1)

@@ -6,8 +6,10 @@
   halo widths that put the stop inside a block and at its end, and at the sweep cap;
 * `hamiltonian_zslab` gives the oracle's H psi bit for bit (hpsi3,
   KohnShamHamiltonianMolecule.cpp:78-177);
-* two gloo ranks (ProcessGroupSlabs: batched point-to-point halos, MAX all-reduce) give the
-  same results as one process."""
+* `xc_zslab` gives the oracle's XC potentials of both spins and E_xc (to rounding: the oracle
+  runs on the slab as its own grid), `gram_zslab` the whole grid's Gram product;
+* two gloo ranks (ProcessGroupSlabs: batched point-to-point halos, MAX and SUM all-reduces)
+  give the same results as one process."""
 import ctypes as C
 import os
 import socket
@@ -18,7 +20,8 @@ import torch
 import torch.multiprocessing as mp
 
 from dft_b200 import CartesianGrid
-from dft_b200.zslab import LocalSlabs, SlabLayout, hamiltonian_zslab, hartree_zslab, owned_planes
+from dft_b200.zslab import (LocalSlabs, SlabLayout, gram_zslab, hamiltonian_zslab, hartree_zslab, owned_planes,
+                            xc_zslab)
 
 from tests.zslab_numpy import NumpySlabOps
 
@@ -133,6 +136,57 @@ def test_hamiltonian_slabs_bit_identical(port, world):
         assert out[k].tobytes() == port.apply_hamiltonian(N, B, V, psi[k]).tobytes(), k
 
 
+def _spin_densities(n=N, b=B):
+    rho = _density(n, b)
+    x = np.linspace(b[0], b[1], n[0])
+    Z, Y, X = np.meshgrid(np.linspace(b[4], b[5], n[2]), np.linspace(b[2], b[3], n[1]), x, indexing="ij")
+    return 0.6 * rho, 0.4 * rho + 0.05 * np.exp(-((X - 1.5) ** 2 + Y ** 2 + Z ** 2)).ravel()
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_xc_slabs_match_oracle(port, kind, world):
+    na, nb = _spin_densities()
+    g = CartesianGrid(*N, *B)
+    lay = SlabLayout(N, world, 2)
+    A = {r: lay.scatter(torch.from_numpy(na), r) for r in range(world)}
+    Bs = {r: lay.scatter(torch.from_numpy(nb), r) for r in range(world)}
+    va, vb, exc = xc_zslab(LocalSlabs(world), lay, g, kind, A, Bs, NumpySlabOps(port))
+    for v, spin in ((lay.gather(va).numpy(), 0), (lay.gather(vb).numpy(), 1)):
+        ref = port.xc_potential(kind, N, B, na, nb, spin)
+        assert np.max(np.abs(v - ref)) <= 1e-12 * np.max(np.abs(ref)), spin
+    ref_e = port.xc_energy(kind, N, B, na, nb)
+    assert abs(exc - ref_e) <= 1e-12 * abs(ref_e)
+
+
+def test_xc_needs_two_halo_planes():
+    g = CartesianGrid(*N, *B)
+    lay = SlabLayout(N, 3, 1)
+    t = {r: torch.zeros(lay.points(r), dtype=torch.float64) for r in range(3)}
+    with pytest.raises(ValueError):
+        xc_zslab(LocalSlabs(3), lay, g, 1, t, dict(t), NumpySlabOps())
+
+
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_gram_slabs_sum_to_whole_grid(world):
+    rng = np.random.default_rng(3)
+    npts = int(np.prod(N))
+    A, Bm = rng.standard_normal((5, npts)), rng.standard_normal((3, npts))
+    g = CartesianGrid(*N, *B)
+    lay = SlabLayout(N, world, 1)
+    As = {r: lay.scatter(torch.from_numpy(A), r) for r in range(world)}
+    Bs = {r: lay.scatter(torch.from_numpy(Bm), r) for r in range(world)}
+    for r in range(world):  # halo planes are not read
+        rows = lay.owned_rows(r)
+        for t in (As[r], Bs[r]):
+            view = t.view(t.shape[0], -1, lay.plane_points)
+            view[:, :rows.start] = np.nan
+            view[:, rows.stop:] = np.nan
+    c = gram_zslab(LocalSlabs(world), lay, g, As, 5, Bs, 3, NumpySlabOps()).numpy()
+    ref = (A @ Bm.T) * (g.getDx() * g.getDy() * g.getDz())
+    assert np.max(np.abs(c - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -164,8 +218,15 @@ def _rank_main(rank, world, port_no, out_dir):
         h = hamiltonian_zslab(comm, lay1, g, {rank: lay1.scatter(V, rank)}, {rank: lay1.scatter(psi, rank)}, 2, Ops())
         rows = lay1.owned_rows(rank)
         np.save(os.path.join(out_dir, f"h{rank}.npy"), h[rank][:, rows.start * n:rows.stop * n].numpy())
+        na, nb = (torch.from_numpy(x) for x in _spin_densities())
+        lay2 = SlabLayout(N, world, 2)
+        va, vb, exc = xc_zslab(comm, lay2, g, 1, {rank: lay2.scatter(na, rank)}, {rank: lay2.scatter(nb, rank)}, Ops())
+        rows = lay2.owned_rows(rank)
+        np.save(os.path.join(out_dir, f"x{rank}.npy"), va[rank][rows.start * n:rows.stop * n].numpy())
+        c = gram_zslab(comm, lay1, g, {rank: lay1.scatter(psi, rank)}, 2, {rank: lay1.scatter(psi, rank)}, 2, Ops())
+        np.save(os.path.join(out_dir, f"c{rank}.npy"), c.numpy())
         with open(os.path.join(out_dir, f"s{rank}.txt"), "w") as f:
-            f.write(f"{sweeps} {last!r}")
+            f.write(f"{sweeps} {last!r} {exc!r}")
     finally:
         dist.destroy_process_group()
 
@@ -177,12 +238,25 @@ def test_gloo_two_ranks(port, tmp_path):
     ref, sw, ld = _oracle_hartree(port, N, B, rho)
     v = np.concatenate([np.load(tmp_path / f"v{r}.npy") for r in range(world)])
     assert v.tobytes() == ref.tobytes()
+    na, nb = _spin_densities()
+    ref_e = port.xc_energy(1, N, B, na, nb)
+    excs = []
     for r in range(world):
-        s, last = open(tmp_path / f"s{r}.txt").read().split()
+        s, last, exc = open(tmp_path / f"s{r}.txt").read().split()
         assert int(s) == sw and float(last) == ld
+        excs.append(float(exc))
+    assert excs[0] == excs[1] and abs(excs[0] - ref_e) <= 1e-12 * abs(ref_e)
+    va = np.concatenate([np.load(tmp_path / f"x{r}.npy") for r in range(world)])
+    ref_v = port.xc_potential(1, N, B, na, nb, 0)
+    assert np.max(np.abs(va - ref_v)) <= 1e-12 * np.max(np.abs(ref_v))
     rng = np.random.default_rng(7)
     V = rng.standard_normal(int(np.prod(N)))
     psi = rng.standard_normal((2, int(np.prod(N))))
     h = np.concatenate([np.load(tmp_path / f"h{r}.npy") for r in range(world)], axis=1)
     for k in range(2):
         assert h[k].tobytes() == port.apply_hamiltonian(N, B, V, psi[k]).tobytes()
+    c0, c1 = np.load(tmp_path / "c0.npy"), np.load(tmp_path / "c1.npy")
+    g = CartesianGrid(*N, *B)
+    ref_c = (psi @ psi.T) * (g.getDx() * g.getDy() * g.getDz())
+    assert c0.tobytes() == c1.tobytes()
+    assert np.max(np.abs(c0 - ref_c)) <= 1e-12 * np.max(np.abs(ref_c))

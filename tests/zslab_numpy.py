@@ -13,6 +13,15 @@ def _spacing(grid):
 
 
 class NumpySlabOps:
+    def __init__(self, port=None):
+        self.port = port
+
+    def _port(self):
+        if self.port is None:
+            from oracle.bindings import Port
+            self.port = Port()
+        return self.port
+
     def jacobi_init(self, grid, z_lo, z_hi, Q, v, guess=None):
         nx, ny, nz = grid.nx, grid.ny, grid.nz
         dx, dy, dz = _spacing(grid)
@@ -84,3 +93,53 @@ class NumpySlabOps:
         lap[:, 1:] = lap[:, 1:] + P[:, :-1] * iz
         lap[:, :-1] = lap[:, :-1] + P[:, 1:] * iz
         hpsi.numpy().reshape(nbands, nzl, ny, nx)[...] = -0.5 * lap + W * P
+
+    # ---- XC and Gram: the oracle's functional on the slab, numpy reductions ----------------
+    def xc(self, grid, z_lo, z_hi, own_lo, own_hi, kind, na, nb, va, vb):
+        port = self._port()
+        nx, ny = grid.nx, grid.ny
+        nzl = z_hi - z_lo
+        dx, dy, dz = _spacing(grid)
+        xmin, xmax, ymin, ymax, zmin, _ = grid.bounds
+        a, b = na.numpy(), nb.numpy()
+        # the slab as its own grid: the same spacing up to rounding of its bounds
+        sb = (xmin, xmax, ymin, ymax, zmin + z_lo * dz, zmin + (z_hi - 1) * dz)
+        if va is not None:
+            va.numpy()[...] = port.xc_potential(kind, (nx, ny, nzl), sb, a, b, 0)
+        if vb is not None:
+            vb.numpy()[...] = port.xc_potential(kind, (nx, ny, nzl), sb, a, b, 1)
+
+        def gradmag(f):
+            f3 = f.reshape(nzl, ny, nx)
+            out = []
+            for axis, h in ((2, dx), (1, dy), (0, dz)):
+                g = np.empty_like(f3)
+                sl = [slice(None)] * 3
+
+                def at(s):
+                    q = list(sl)
+                    q[axis] = s
+                    return tuple(q)
+                g[at(slice(1, -1))] = (f3[at(slice(2, None))] - f3[at(slice(None, -2))]) / (2.0 * h)
+                g[at(0)] = (f3[at(1)] - f3[at(0)]) / h
+                g[at(-1)] = (f3[at(-1)] - f3[at(-2)]) / h
+                out.append(g)
+            return np.sqrt(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]).ravel()
+
+        n_xy = nx * ny
+        lo, hi = (own_lo - z_lo) * n_xy, (own_hi - z_lo) * n_xy
+        ga, gb = gradmag(a)[lo:hi], gradmag(b)[lo:hi]
+        oa, ob = a[lo:hi], b[lo:hi]
+        eps = port.xc_evaluate(kind, oa, ob, ga, gb)[:, 0]
+        n = oa + ob
+        keep = n > 1.0e-20
+        return float(np.sum(n[keep] * eps[keep]) * (dx * dy * dz))
+
+    def gram(self, grid, z_lo, z_hi, own_lo, own_hi, A, ka, B, kb, precision=0):
+        import torch
+        n_xy = grid.nx * grid.ny
+        lo, hi = (own_lo - z_lo) * n_xy, (own_hi - z_lo) * n_xy
+        a = A.numpy().reshape(ka, -1)[:, lo:hi]
+        b = B.numpy().reshape(kb, -1)[:, lo:hi]
+        dx, dy, dz = _spacing(grid)
+        return torch.from_numpy((a @ b.T) * (dx * dy * dz))
