@@ -105,6 +105,12 @@ class SlabLayout:
         return torch.cat(parts, dim=-1)
 
 
+def _check_width(layout: SlabLayout, width: int) -> None:
+    if layout.world > 1 and not 1 <= width <= layout.halo:
+        raise ValueError(f"a halo exchange of {width} planes needs a layout with at least that many halo planes "
+                         f"(this one has {layout.halo})")
+
+
 def _rows(t: torch.Tensor, n: int) -> torch.Tensor:
     """(bands, planes, nx*ny) view of a slab field (one band when the field is flat)."""
     return t.view(-1, t.shape[-1] // n, n)
@@ -119,6 +125,7 @@ class LocalSlabs:
         self.ranks = list(range(self.world))
 
     def exchange(self, layout: SlabLayout, fields: Dict[int, torch.Tensor], width: int) -> None:
+        _check_width(layout, width)
         n = layout.plane_points
         for r in self.ranks:
             lo, _ = layout.extent(r)
@@ -158,6 +165,7 @@ class ProcessGroupSlabs:
         return r if self.group is None else dist.get_global_rank(self.group, r)
 
     def exchange(self, layout: SlabLayout, fields: Dict[int, torch.Tensor], width: int) -> None:
+        _check_width(layout, width)
         r = self.rank
         n = layout.plane_points
         lo, _ = layout.extent(r)

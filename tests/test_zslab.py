@@ -79,6 +79,13 @@ def test_layout_halo_capped_by_smallest_run():
     assert lay.owned_rows(1) == slice(2, 5)
 
 
+def test_exchange_wider_than_halo_rejected():
+    lay = SlabLayout(N, 3, 1)
+    t = {r: torch.zeros(lay.points(r), dtype=torch.float64) for r in range(3)}
+    with pytest.raises(ValueError):
+        LocalSlabs(3).exchange(lay, t, 2)
+
+
 def test_hartree_single_slab_is_the_oracle(port):
     rho = _density()
     ref, sw, ld = _oracle_hartree(port, N, B, rho)
@@ -104,6 +111,31 @@ def test_hartree_cap_and_zero_sweeps():
     assert three.tobytes() == one.tobytes()
     z, s0, _ = _solve_local(3, 4, rho, max_sweeps=0)
     assert s0 == 0 and not z.any()
+
+
+def test_hartree_one_plane_per_rank(port):
+    # nz ranks: halo 1, an exchange every sweep; the first and last rank own only a face
+    n, b = (9, 8, 6), (-2.0, 2.0, -1.75, 1.75, -1.25, 1.25)
+    rho = _density(n, b)
+    ref, sw, ld = _oracle_hartree(port, n, b, rho)
+    v, sweeps, last = _solve_local(6, 4, rho, n=n, b=b)
+    assert sweeps == sw and last == ld
+    assert v.tobytes() == ref.tobytes()
+
+
+def test_hartree_warm_start():
+    rho = _density()
+    g = CartesianGrid(*N, *B)
+    start, _, _ = _solve_local(1, 8, rho, max_sweeps=50)
+    guess = torch.from_numpy(0.9 * start)
+    out = {}
+    for world in (1, 3):
+        lay = SlabLayout(N, world, 6)
+        slabs = {r: lay.scatter(torch.from_numpy(rho), r) for r in range(world)}
+        gs = {r: lay.scatter(guess, r) for r in range(world)}
+        v, sweeps, last = hartree_zslab(LocalSlabs(world), lay, g, slabs, NumpySlabOps(), 1e-8, 10000, gs)
+        out[world] = (lay.gather(v).numpy().tobytes(), sweeps, last)
+    assert out[1] == out[3]
 
 
 def test_hartree_faces_off_the_nodes_close():
