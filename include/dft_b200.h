@@ -206,7 +206,8 @@ dft_status_t dft_hartree_monopole_dev(dft_context* ctx, const dft_grid* g, const
  * HartreePotentialMolecule.cpp:37-95, :152-155): the reference's face values where the slab
  * meets a face of g, Q/|r| with Q the total charge (used only on faces whose last node misses
  * the bound; 0 on every grid whose nodes land on the bounds), interior 0, or the interior of
- * guess (device, same slab layout) when guess is not NULL.  v: device, nx*ny*(z_hi - z_lo). */
+ * guess (device, same slab layout) when guess is not NULL.  v: device, nx*ny*(z_hi - z_lo).
+ * Synchronises. */
 dft_status_t dft_zslab_jacobi_init_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, double Q,
                                        const double* guess, double* v);
 
@@ -234,7 +235,7 @@ dft_status_t dft_zslab_hamiltonian_dev(dft_context* ctx, const dft_grid* g, int 
  * result on the owned planes [own_lo, own_hi) when the slab holds two planes beyond them on
  * each side (or ends at a face of g; DFT_INVALID_ARGUMENT otherwise).  exc_out (host, may be
  * NULL): the owned planes' part of E_xc; the ranks' parts add up to E_xc (summed in a different
- * order than the whole grid's). */
+ * order than the whole grid's).  Synchronises. */
 dft_status_t dft_zslab_xc_dev(dft_context* ctx, const dft_grid* g, int z_lo, int z_hi, int own_lo, int own_hi,
                               dft_xc_kind kind, const double* na, const double* nb, double* va, double* vb,
                               double* exc_out);
