@@ -293,3 +293,35 @@ def test_gloo_ranks(port, tmp_path, world):
     ref_c = (psi @ psi.T) * (g.getDx() * g.getDy() * g.getDz())
     assert all(c.tobytes() == cs[0].tobytes() for c in cs)
     assert np.max(np.abs(cs[0] - ref_c)) <= 1e-12 * np.max(np.abs(ref_c))
+
+
+def _rank_leaves(rank, world, port_no, out_dir):
+    import datetime
+    import sys
+    import time
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    from tests.zslab_numpy import NumpySlabOps as Ops
+    from dft_b200.zslab import ProcessGroupSlabs
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port_no))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    if rank == 1:
+        return  # leaves between steps, before the solve's first exchange
+    t0 = time.time()
+    try:
+        g = CartesianGrid(*N, *B)
+        lay = SlabLayout(N, world, 4)
+        hartree_zslab(ProcessGroupSlabs(), lay, g, {0: lay.scatter(torch.from_numpy(_density()), 0)}, Ops())
+        outcome = "finished"
+    except Exception as e:  # the exchange or the reduction with the missing rank fails
+        outcome = "error " + type(e).__name__
+    with open(os.path.join(out_dir, "rank0.txt"), "w") as f:
+        f.write(f"{outcome} {time.time() - t0:.1f}")
+
+
+def test_gloo_rank_leaving_ends_the_solve_with_an_error(tmp_path):
+    mp.start_processes(_rank_leaves, args=(2, _free_port(), str(tmp_path)), nprocs=2, start_method="spawn")
+    outcome, seconds = open(tmp_path / "rank0.txt").read().rsplit(" ", 1)
+    assert outcome.startswith("error"), outcome
+    assert float(seconds) < 60.0
